@@ -1,0 +1,217 @@
+"""Python mirror of the clSPARSE C API over torch device tensors.
+
+Each function here is a thin call through the C ABI (clsparse_b200._lib): the
+arguments are packed into the reference's structs (clsparseCsrMatrix,
+cldenseVector, clsparseScalar) pointing at torch CUDA storage, and a non-zero
+clsparseStatus raises ClsparseError. Names follow the reference API
+(src/include/clSPARSE.h). torch only provides device memory and the stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+
+class ClsparseError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        super().__init__(f"{what} failed with clsparseStatus {status}")
+        self.status = status
+
+
+def lib():
+    return L.load()
+
+
+def check(status: int, what: str):
+    if int(status) != L.clsparseSuccess:
+        raise ClsparseError(int(status), what)
+
+
+def setup():
+    check(lib().clsparseSetup(), "clsparseSetup")
+
+
+def teardown():
+    check(lib().clsparseTeardown(), "clsparseTeardown")
+
+
+def _dtype_prefix(t: torch.Tensor) -> str:
+    if t.dtype == torch.float64:
+        return "D"
+    if t.dtype == torch.float32:
+        return "S"
+    raise TypeError(f"unsupported value dtype {t.dtype}")
+
+
+class Control:
+    """clsparseControl bound to a CUDA stream (default: torch's current stream)."""
+
+    def __init__(self, stream: torch.cuda.Stream | None = None):
+        setup()
+        self.stream = stream if stream is not None else torch.cuda.current_stream()
+        res = lib().clsparseCreateControl(C.c_void_p(self.stream.cuda_stream))
+        check(res.status, "clsparseCreateControl")
+        self.handle = res.control
+
+    def enable_async(self, on: bool = True):
+        check(lib().clsparseEnableAsync(self.handle, 1 if on else 0), "clsparseEnableAsync")
+
+    def enable_extended_precision(self, on: bool = True):
+        check(lib().clsparseEnableExtendedPrecision(self.handle, 1 if on else 0),
+              "clsparseEnableExtendedPrecision")
+
+    def set_solver_loop_mode(self, mode: int):
+        check(lib().clsparseB200SetSolverLoopMode(self.handle, mode), "clsparseB200SetSolverLoopMode")
+
+    def release(self):
+        if self.handle:
+            check(lib().clsparseReleaseControl(self.handle), "clsparseReleaseControl")
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.release()
+
+
+def vector(t: torch.Tensor, offset: int = 0, num_values: int | None = None) -> L.cldenseVector:
+    n = t.numel() - offset if num_values is None else num_values
+    return L.cldenseVector(n, C.c_void_p(t.data_ptr()), offset)
+
+
+def scalar(t: torch.Tensor, offset: int = 0) -> L.clsparseScalar:
+    return L.clsparseScalar(C.c_void_p(t.data_ptr()), offset)
+
+
+class CsrMatrix:
+    """A clsparseCsrMatrix over torch tensors (row_ptr / col as int32 storage of
+    the uint32 indices, values float32 or float64)."""
+
+    def __init__(self, row_ptr: torch.Tensor, col: torch.Tensor, val: torch.Tensor, num_cols: int):
+        self.row_ptr, self.col, self.val = row_ptr, col, val
+        self.s = L.clsparseCsrMatrix()
+        lib().clsparseInitCsrMatrix(C.byref(self.s))
+        self.s.num_rows = row_ptr.numel() - 1
+        self.s.num_cols = num_cols
+        self.s.num_nonzeros = val.numel()
+        self.s.values = C.c_void_p(val.data_ptr()) if val.numel() else None
+        self.s.col_indices = C.c_void_p(col.data_ptr()) if col.numel() else None
+        self.s.row_pointer = C.c_void_p(row_ptr.data_ptr())
+
+    @classmethod
+    def from_numpy(cls, rp, col, val, num_cols=None, dtype=torch.float64, device="cuda"):
+        rp = np.asarray(rp, dtype=np.uint32)
+        col = np.asarray(col, dtype=np.uint32)
+        ncols = (len(rp) - 1) if num_cols is None else num_cols
+        t_rp = torch.from_numpy(rp.view(np.int32).copy()).to(device)
+        t_col = torch.from_numpy(col.view(np.int32).copy()).to(device)
+        t_val = torch.from_numpy(np.asarray(val)).to(device=device, dtype=dtype)
+        return cls(t_rp, t_col, t_val, ncols)
+
+    @property
+    def num_rows(self):
+        return self.s.num_rows
+
+    @property
+    def num_cols(self):
+        return self.s.num_cols
+
+    @property
+    def nnz(self):
+        return self.s.num_nonzeros
+
+    def meta_size(self, ctrl: Control) -> int:
+        r = lib().clsparseCsrMetaSize(C.byref(self.s), ctrl.handle)
+        check(r.status, "clsparseCsrMetaSize")
+        return int(r.metaSize)
+
+    def create_meta(self, ctrl: Control):
+        check(lib().clsparseCsrMetaCreate(C.byref(self.s), ctrl.handle), "clsparseCsrMetaCreate")
+
+    def delete_meta(self):
+        check(lib().clsparseCsrMetaDelete(C.byref(self.s)), "clsparseCsrMetaDelete")
+
+    def row_blocks(self) -> np.ndarray:
+        n = C.c_size_t()
+        check(lib().clsparseB200CsrMetaGetRowBlocks(C.byref(self.s), None, 0, C.byref(n)), "GetRowBlocks")
+        out = np.zeros(n.value, dtype=np.uint64)
+        check(lib().clsparseB200CsrMetaGetRowBlocks(C.byref(self.s), out.ctypes.data_as(C.POINTER(L.cl_ulong)),
+                                                    n.value, C.byref(n)), "GetRowBlocks")
+        return out
+
+    def __del__(self):
+        try:
+            if self.s.meta:
+                lib().clsparseCsrMetaDelete(C.byref(self.s))
+        except Exception:
+            pass
+
+
+def csrmv(alpha: torch.Tensor, A: CsrMatrix, x: torch.Tensor, beta: torch.Tensor, y: torch.Tensor,
+          ctrl: Control, x_off: int = 0, y_off: int = 0):
+    """y = alpha*A*x + beta*y through clsparse{S,D}csrmv."""
+    p = _dtype_prefix(A.val)
+    fn = getattr(lib(), f"clsparse{p}csrmv")
+    xv = vector(x, x_off)
+    yv = vector(y, y_off)
+    check(fn(C.byref(scalar(alpha)), C.byref(A.s), C.byref(xv), C.byref(scalar(beta)), C.byref(yv),
+             ctrl.handle), f"clsparse{p}csrmv")
+
+
+class SolverControl:
+    def __init__(self, precond: int = L.DIAGONAL, max_iters: int = 100, rel_tol: float = 1e-2,
+                 abs_tol: float = 1e-5):
+        r = lib().clsparseCreateSolverControl(precond, max_iters, rel_tol, abs_tol)
+        check(r.status, "clsparseCreateSolverControl")
+        self.handle = r.control
+
+    def set_params(self, precond, max_iters, rel_tol, abs_tol):
+        check(lib().clsparseSetSolverParams(self.handle, precond, max_iters, rel_tol, abs_tol),
+              "clsparseSetSolverParams")
+
+    def print_mode(self, mode):
+        check(lib().clsparseSolverPrintMode(self.handle, mode), "clsparseSolverPrintMode")
+
+    def info(self):
+        it = L.cl_int()
+        r0 = C.c_double()
+        r1 = C.c_double()
+        check(lib().clsparseB200SolverGetInfo(self.handle, C.byref(it), C.byref(r0), C.byref(r1)), "GetInfo")
+        return {"nIters": it.value, "initialResidual": r0.value, "currentResidual": r1.value}
+
+    def device_status(self) -> int:
+        b = L.cl_uint()
+        check(lib().clsparseB200SolverGetDeviceStatus(self.handle, C.byref(b)), "GetDeviceStatus")
+        return b.value
+
+    def release(self):
+        if self.handle:
+            check(lib().clsparseReleaseSolverControl(self.handle), "clsparseReleaseSolverControl")
+            self.handle = None
+
+
+def solve(kind: str, x: torch.Tensor, A: CsrMatrix, b: torch.Tensor, sc: SolverControl, ctrl: Control):
+    """kind 'cg' -> clsparse{S,D}csrcg, 'bicgstab' -> clsparse{S,D}csrbicgStab."""
+    p = _dtype_prefix(A.val)
+    name = f"clsparse{p}csrcg" if kind == "cg" else f"clsparse{p}csrbicgStab"
+    fn = getattr(lib(), name)
+    st = fn(C.byref(vector(x)), C.byref(A.s), C.byref(vector(b)), sc.handle, ctrl.handle)
+    check(st, name)
+    return sc.info()
+
+
+def blas1(name: str, *args, ctrl: Control):
+    """Calls a cldense* entry point; tensors become vectors, 1-element tensors
+    passed as ('s', t) become scalars."""
+    conv = []
+    for a in args:
+        if isinstance(a, tuple) and a[0] == "s":
+            conv.append(C.byref(scalar(a[1])))
+        else:
+            conv.append(C.byref(vector(a)))
+    check(getattr(lib(), name)(*conv, ctrl.handle), name)

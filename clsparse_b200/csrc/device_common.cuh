@@ -1,0 +1,180 @@
+// Device helpers shared by the SpMV, BLAS-1 and solver kernels: cache-hinted
+// loads, compensated accumulation, warp / CTA reductions and the
+// deterministic grid reduction that lets the last CTA of a launch finish a
+// reduction without a second kernel and without any spin-wait.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace clsp {
+namespace dev {
+
+// Streaming loads for data read exactly once (matrix values and column
+// indices): evict-first, so the gathered vector stays in L2.
+template <typename T>
+__device__ __forceinline__ T ld_stream(const T* p) {
+    return __ldcs(p);
+}
+
+// Read-only loads through the non-coherent path (gathered vector, row pointers).
+template <typename T>
+__device__ __forceinline__ T ld_ro(const T* p) {
+    return __ldg(p);
+}
+
+// Knuth's TwoSum: returns fl(a+b) and adds the exact rounding error to err.
+template <typename T>
+__device__ __forceinline__ T two_sum(T a, T b, T& err) {
+    const T s = a + b;
+    const T bp = s - a;
+    err += (a - (s - bp)) + (b - bp);
+    return s;
+}
+
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
+// Sum accumulator; with EXT it carries a running compensation term
+// (compensated dot product in the style of Ogita, Rump and Oishi, "Accurate
+// sum and dot product", SIAM J. Sci. Comput. 26(6), 2005), which is the
+// extended-precision mode of the reference kernels
+// (src/library/kernels/csrmv_adaptive.cl:167-308).
+template <typename T, bool EXT>
+struct Acc {
+    T s = T(0);
+    T c = T(0);
+    __device__ __forceinline__ void add(T v) {
+        if constexpr (EXT) {
+            s = two_sum(s, v, c);
+        } else {
+            s += v;
+        }
+    }
+    __device__ __forceinline__ void add_prod(T a, T b) {
+        if constexpr (EXT) {
+            const T p = mul_rn(a, b);
+            const T e = fma_rn(a, b, -p);
+            s = two_sum(s, p, c);
+            c += e;
+        } else {
+            s = fma_rn(a, b, s);
+        }
+    }
+    __device__ __forceinline__ void merge(T os, T oc) {
+        if constexpr (EXT) {
+            s = two_sum(s, os, c);
+            c += oc;
+        } else {
+            s += os;
+        }
+    }
+    __device__ __forceinline__ T value() const {
+        if constexpr (EXT) return s + c;
+        return s;
+    }
+};
+
+// Reduces an accumulator over aligned groups of W lanes (W a power of two
+// <= 32). Every lane of the warp must call it. Lane 0 of each group ends with
+// the group total.
+template <int W, typename T, bool EXT>
+__device__ __forceinline__ void group_reduce(Acc<T, EXT>& a) {
+#pragma unroll
+    for (int off = W / 2; off > 0; off >>= 1) {
+        const T os = __shfl_xor_sync(0xffffffffu, a.s, off, W);
+        if constexpr (EXT) {
+            const T oc = __shfl_xor_sync(0xffffffffu, a.c, off, W);
+            a.merge(os, oc);
+        } else {
+            a.s += os;
+        }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// Sums one value per thread over the CTA (blockDim.x a multiple of 32, at
+// most 1024). The result is valid in every thread. `scratch` holds >= 32
+// elements. The summation order depends only on blockDim, so it is
+// reproducible.
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T* scratch) {
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    T t = (lane < nwarps) ? scratch[lane] : T(0);
+    t = warp_sum(t);
+    return t;
+}
+
+template <typename T, bool EXT>
+__device__ __forceinline__ Acc<T, EXT> block_reduce_acc(Acc<T, EXT> a, T* scratch_s, T* scratch_c) {
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+    group_reduce<32>(a);
+    __syncthreads();
+    if (lane == 0) {
+        scratch_s[warp] = a.s;
+        scratch_c[warp] = a.c;
+    }
+    __syncthreads();
+    Acc<T, EXT> b;
+    if (lane < nwarps) {
+        b.s = scratch_s[lane];
+        b.c = scratch_c[lane];
+    }
+    group_reduce<32>(b);
+    return b;
+}
+
+// Deterministic grid-wide sum of K per-thread values of type U (double or
+// long long). Each CTA stores its
+// partial totals in partials[k * gridDim.x + blockIdx.x], then takes a ticket;
+// the CTA that draws the last ticket re-reads all partials in index order and
+// returns true with the totals in out[] (valid in every thread of that CTA).
+// It also resets the ticket to zero for the next launch. No CTA ever waits
+// for another, so there is nothing to deadlock.
+template <int K, typename U = double>
+__device__ __forceinline__ bool grid_reduce_last(const U (&v)[K], U* partials, uint32_t* ticket,
+                                                 U (&out)[K]) {
+    __shared__ U red[32];
+    __shared__ bool is_last;
+    U tot[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) tot[k] = block_sum(v[k], red);
+    const uint32_t G = gridDim.x;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) partials[(size_t)k * G + blockIdx.x] = tot[k];
+        __threadfence();
+        const uint32_t t = atomicAdd(ticket, 1u);
+        is_last = (t == G - 1);
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        U a = U(0);
+        for (uint32_t i = threadIdx.x; i < G; i += blockDim.x) a += __ldcg(partials + (size_t)k * G + i);
+        out[k] = block_sum(a, red);
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
+    return true;
+}
+
+}  // namespace dev
+}  // namespace clsp

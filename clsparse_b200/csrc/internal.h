@@ -1,0 +1,165 @@
+// Library-private runtime state of clsparse-b200: the control object, the
+// CSR-Adaptive meta, the solver control and the helpers every entry point
+// uses. Host C++17; included by the .cpp and .cu translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <cstdio>
+#include <memory>
+#include <vector>
+
+#include "clSPARSE.h"
+#include "clSPARSE-b200.h"
+
+namespace clsp {
+
+// Library initialisation counter (reference clsparse-init.cpp:25 keeps a plain
+// int; an atomic makes concurrent Setup/Teardown well defined).
+extern std::atomic<int> g_initialized;
+
+// CSR-Adaptive constants (reference src/library/include/clSPARSE-private.hpp:46-50).
+// These five numbers define the row-block format and must equal the reference's
+// so that clsparseCsrMetaCreate produces the same words.
+constexpr uint32_t kWgBits = 24;
+constexpr uint32_t kRowBits = 32;
+constexpr uint32_t kBlkSize = 1024;
+constexpr uint32_t kBlockMultiplier = 3;
+constexpr uint32_t kRowsForVector = 1;
+
+// A grow-only device allocation.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t need);
+    void release();
+    ~DeviceBuffer() { release(); }
+};
+
+struct SolverCache;  // cached CUDA graph + work vectors of the last solve
+
+}  // namespace clsp
+
+// The control object (reference internal/clsparse-control.hpp:30-80). Owns no
+// user memory; keeps a scratch area for reductions and the solver workspace.
+struct _clsparseControl {
+    cudaStream_t stream = nullptr;  // the caller's queue
+    int device = 0;
+    int sm_count = 148;
+    size_t l2_bytes = 0;
+    bool async = false;
+    bool extended_precision = false;
+    int solver_loop_mode = 0;       // 0 graph while-loop, 1 host chunks
+    cudaEvent_t event = nullptr;    // recorded after each call
+    cudaStream_t capture_stream = nullptr;  // private stream used for graph capture
+    // Reduction scratch: kMaxReduceCtas doubles x 4 partial slots + a ticket.
+    clsp::DeviceBuffer reduce_scratch;
+    // Pinned host word used to read back reduction results of solver calls.
+    void* pinned = nullptr;
+    std::unique_ptr<clsp::SolverCache> solver_cache;
+};
+
+// CSR-Adaptive meta attached to clsparseCsrMatrix::meta (reference
+// clSPARSE-1x.hpp:45-62). Immutable after creation except for the long-row
+// tickets, which every SpMV leaves at zero when it returns.
+struct matrix_meta {
+    clsparseIdx_t rowBlockSize = 0;     // 2 x number of row-block words (reference semantics)
+    size_t num_words = 0;               // row-block words; CTAs of one SpMV = num_words - 1
+    cl_ulong* d_rowBlocks = nullptr;    // device copy of the words
+    std::vector<cl_ulong> h_rowBlocks;  // host copy (for inspection)
+    double* d_lr_partial = nullptr;     // one partial sum per row-block word (long rows)
+    uint32_t* d_lr_ticket = nullptr;    // one arrival counter per row-block word (long rows)
+    clsparseIdx_t num_rows = 0;
+    clsparseIdx_t num_nonzeros = 0;
+    int device = 0;
+    ~matrix_meta();
+};
+
+// Solver control (reference solvers/solver-control.hpp:37-128).
+struct _solverControl {
+    cl_int nIters = 0;
+    cl_int maxIters = 0;
+    PRECONDITIONER preconditioner = NOPRECOND;
+    cl_double relativeTolerance = 0.0;
+    cl_double absoluteTolerance = 0.0;
+    cl_double initialResidual = 0.0;
+    cl_double currentResidual = 0.0;
+    PRINT_MODE printMode = QUIET;
+    cl_uint deviceStatus = 0;
+    void printSummary(clsparseStatus status) const;
+};
+
+namespace clsp {
+
+// Sets the control's device current for the scope of an API call.
+class DeviceGuard {
+public:
+    explicit DeviceGuard(int dev);
+    ~DeviceGuard();
+private:
+    int prev_ = -1;
+    bool changed_ = false;
+};
+
+// Ends an API call: records the control's event and, unless async, waits for
+// the stream. Maps launch / execution errors to clsparseInvalidKernelExecution.
+clsparseStatus finish_call(clsparseControl control);
+
+// Checks the common preconditions (library initialised, control present).
+inline clsparseStatus check_entry(clsparseControl control) {
+    if (g_initialized.load() == 0) return clsparseNotInitialized;
+    if (control == nullptr) return clsparseInvalidControlObject;
+    return clsparseSuccess;
+}
+
+template <typename T>
+inline T* dev_ptr(cl_mem base, clsparseIdx_t off) {
+    return static_cast<T*>(base) + off;
+}
+
+constexpr int kMaxReduceCtas = 2048;
+
+// ---- SpMV launch interface (spmv.cu) ----
+
+// Optional fused epilogue of an SpMV: per-row dot products of the result y
+// with w0 (and with y itself), reduced deterministically over the grid; the
+// last CTA to finish runs a solver-specific finaliser (spmv_epilogue_op).
+enum class EpiOp : int { None = 0, CgAlpha = 1, BicgAlpha = 2, BicgOmega = 3 };
+
+struct SpmvEpilogue {
+    int ndots = 0;            // 0, 1 or 2
+    const void* w0 = nullptr; // dot0 = sum y_i * w0_i
+    bool dot1_self = false;   // dot1 = sum y_i * y_i
+    double* partials = nullptr;   // [ndots][num_ctas]
+    uint32_t* ticket = nullptr;
+    EpiOp op = EpiOp::None;
+    void* state = nullptr;    // solver state the finaliser updates
+    unsigned long long cond = 0;  // graph conditional handle (0 = none)
+    const int* done = nullptr;    // when set and *done != 0 the kernel returns at once
+};
+
+template <typename T>
+struct CsrView {
+    const T* vals;
+    const uint32_t* cols;
+    const uint32_t* rp;
+    uint32_t nrows, ncols, nnz;
+    const matrix_meta* meta;
+};
+
+// Number of CTAs an SpMV of this matrix launches (sizes epilogue partials).
+uint32_t spmv_num_ctas(const matrix_meta* meta, uint32_t nrows, uint32_t nnz);
+
+template <typename T>
+cudaError_t launch_csrmv(const CsrView<T>& A, const T* alpha, const T* beta, const T* x, T* y,
+                         bool extended, const SpmvEpilogue& epi, cudaStream_t s);
+
+// Host binning (meta.cpp).
+void compute_row_blocks(cl_ulong* rowBlocks, clsparseIdx_t& rowBlockSize, const clsparseIdx_t* rp,
+                        clsparseIdx_t nRows, uint32_t blkSize, uint32_t blkMultiplier,
+                        uint32_t rowsForVector, bool allocate);
+
+}  // namespace clsp

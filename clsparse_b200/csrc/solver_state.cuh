@@ -1,0 +1,86 @@
+// Device-resident state of one CG / BiCGStab solve and the scalar steps the
+// reference ran as separate 1-element kernels and host reads
+// (src/library/solvers/conjugate-gradients.hpp:110-226,
+//  biconjugate-gradients-stabilized.hpp:103-266). Scalars are kept in the
+// solve's value type T, as the reference's clsparse::scalar<T> were; the
+// reductions feeding them are accumulated in double.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace clsp {
+
+// Device status bits reported through clsparseB200SolverGetDeviceStatus.
+enum : int {
+    kStatusMissingDiag = 1,
+    kStatusZeroDiag = 2,
+    kStatusCurvature = 4,
+    kStatusBicgBreakdown = 8,
+    kStatusNonFinite = 16,
+};
+
+template <typename T>
+struct SolverState {
+    // parameters (written by the host before each solve)
+    double relTol;
+    double absTol;
+    int maxIters;
+    int pad0;
+    // scalars of the iteration, in T like the reference
+    T norm_b, rz, rz_old, yp, alpha, beta, omega, norm_r, res;
+    T rsr_old, rsr_new, rs_amp, amss, amsams;
+    T one, zero;   // device constants for SpMV calls with alpha = 1, beta = 0
+    // bookkeeping
+    double init_res;
+    double cur_res;
+    int iteration;
+    int nIters;
+    int done;      // 1 once the stop test passed; later kernels return at once
+    int zero_b;    // ||b||_1 == 0: x = b and stop (conjugate-gradients.hpp:87-95)
+    int exit_s;    // BiCGStab stopped on ||s|| (biconjugate-gradients-stabilized.hpp:183-195)
+    int status_bits;
+};
+
+// The reference's stop test (solver-control.hpp:47-64): converged if
+// res <= relTol or res <= absTol * initial residual, or out of iterations.
+template <typename T>
+__device__ __forceinline__ bool solver_finished(const SolverState<T>& s, double res) {
+    return (res <= s.relTol) || (res <= s.absTol * s.init_res) || (s.nIters >= s.maxIters);
+}
+
+__device__ __forceinline__ void set_condition(unsigned long long h, unsigned int v) {
+    if (h != 0ull) cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(h), v);
+}
+
+template <typename T>
+__device__ __forceinline__ bool finite_t(T v) {
+    return isfinite(v);
+}
+
+// Finaliser after q = A p with dot0 = <q, p>: alpha = <r,z> / <q,p>.
+template <typename T>
+__device__ __forceinline__ void fin_cg_alpha(SolverState<T>* st, double yp) {
+    st->yp = static_cast<T>(yp);
+    st->alpha = st->rz / st->yp;
+    if (!(st->yp > T(0))) st->status_bits |= kStatusCurvature;
+}
+
+// Finaliser after AMp = A (M p) with dot0 = <AMp, r*>: alpha = <r*,r> / <r*,AMp>.
+template <typename T>
+__device__ __forceinline__ void fin_bicg_alpha(SolverState<T>* st, double rs_amp) {
+    st->rs_amp = static_cast<T>(rs_amp);
+    st->alpha = st->rsr_old / st->rs_amp;
+    if (st->rs_amp == T(0)) st->status_bits |= kStatusBicgBreakdown;
+}
+
+// Finaliser after AMs = A (M s) with dot0 = <AMs, s>, dot1 = <AMs, AMs>.
+template <typename T>
+__device__ __forceinline__ void fin_bicg_omega(SolverState<T>* st, double amss, double amsams) {
+    st->amss = static_cast<T>(amss);
+    st->amsams = static_cast<T>(amsams);
+    st->omega = st->amss / st->amsams;
+    if (st->omega == T(0)) st->status_bits |= kStatusBicgBreakdown;
+}
+
+}  // namespace clsp

@@ -1,0 +1,778 @@
+// Preconditioned CG and BiCGStab (clsparse{S,D}csrcg, clsparse{S,D}csrbicgStab)
+// for sm_100a.
+//
+// The iteration follows the reference operation for operation
+// (src/library/solvers/conjugate-gradients.hpp:65-226 and
+//  biconjugate-gradients-stabilized.hpp:61-266): same recurrences, same
+// roundings of every vector update, the L1 stop test of solver-control.hpp:47-64
+// and the same iteration bookkeeping. What changes is where it runs:
+//
+// * every scalar (alpha, beta, omega, the residual) lives in device memory and
+//   is computed by the last CTA of the kernel that finishes its reduction, so
+//   an iteration needs no host round trip (the reference blocks on a host read
+//   of the residual every iteration, conjugate-gradients.hpp:223);
+// * the BLAS-1 steps of an iteration are fused: CG runs three kernels per
+//   iteration (SpMV with <Ap,p> fused; x/r/z update with <r,z> and ||r||_1
+//   fused; p update), BiCGStab five;
+// * the whole solve -- Jacobi extraction, initial residual, the loop and the
+//   exit -- is one CUDA graph whose loop is a conditional WHILE node driven by
+//   the device-side stop test. The graph is cached per control and re-launched
+//   when the same operands are solved again.
+//
+// The host reads the solver state once, after the graph, to fill the solver
+// control (iteration count, residuals) exactly as the reference leaves it.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "device_common.cuh"
+#include "internal.h"
+#include "solver_cache.h"
+#include "solver_state.cuh"
+
+namespace clsp {
+namespace {
+
+constexpr int kThreads = 256;
+
+uint32_t vec_grid(size_t n, int sms) {
+    size_t ctas = (n + kThreads * 4 - 1) / (kThreads * 4);
+    size_t cap = static_cast<size_t>(sms) * 8;
+    if (cap > static_cast<size_t>(kMaxReduceCtas)) cap = kMaxReduceCtas;
+    if (ctas > cap) ctas = cap;
+    if (ctas == 0) ctas = 1;
+    return static_cast<uint32_t>(ctas);
+}
+
+template <typename T>
+__device__ __forceinline__ T apply_m(const T* __restrict__ invD, size_t i, T r) {
+    return invD ? r * invD[i] : r;
+}
+
+template <typename T>
+__device__ __forceinline__ double dabs(T v) {
+    return fabs(static_cast<double>(v));
+}
+
+// invD[row] = 1 / A[row,row], first matching entry of the row as in the
+// reference's extract_diagonal (src/library/kernels/matrix_utils.cl:65-98).
+// A row without a diagonal entry gets 0 and raises a status bit; a zero
+// diagonal gives inf like the reference and raises another.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+    extract_inv_diag_kernel(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols,
+                            const T* __restrict__ vals, uint32_t n, T* __restrict__ invD,
+                            SolverState<T>* st) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x) >> 5;
+    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * kThreads) >> 5;
+    for (uint64_t row = warp; row < n; row += nwarps) {
+        const uint32_t nb = rp[row], ne = rp[row + 1];
+        bool found = false;
+        for (uint32_t base = nb; base < ne && !found; base += 32) {
+            const uint32_t j = base + lane;
+            const bool m = (j < ne) && (cols[j] == row);
+            const unsigned ball = __ballot_sync(0xffffffffu, m);
+            if (ball) {
+                const int first = __ffs(ball) - 1;
+                if (lane == first) {
+                    const T v = vals[j];
+                    invD[row] = T(1) / v;
+                    if (v == T(0)) atomicOr(&st->status_bits, kStatusZeroDiag);
+                }
+                found = true;
+            }
+        }
+        if (!found && lane == 0) {
+            invD[row] = T(0);
+            atomicOr(&st->status_bits, kStatusMissingDiag);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- CG ----
+
+template <typename T>
+struct CgArgs {
+    T* x;
+    const T* b;
+    T* y;
+    T* r;
+    T* p;
+    const T* invD;  // nullptr: no preconditioner
+    SolverState<T>* st;
+    double* parts;
+    uint32_t* ticket;
+    size_t n;
+    unsigned long long cond;
+};
+
+// r = b - A x (y holds A x), z = M r, p = z; ||b||_1, ||r||_1, <r,z>; initial
+// stop test (conjugate-gradients.hpp:73-148).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) cg_init_kernel(CgArgs<T> a) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
+        const T bi = a.b[i];
+        const T ri = bi - a.y[i];
+        const T zi = apply_m(a.invD, i, ri);
+        a.r[i] = ri;
+        a.p[i] = zi;
+        acc[0] += dabs(bi);
+        acc[1] += dabs(ri);
+        acc[2] += static_cast<double>(ri) * static_cast<double>(zi);
+    }
+    double tot[3];
+    if (dev::grid_reduce_last<3>(acc, a.parts, a.ticket, tot) && threadIdx.x == 0) {
+        SolverState<T>* st = a.st;
+        st->norm_b = static_cast<T>(tot[0]);
+        if (st->norm_b == T(0)) {
+            st->zero_b = 1;
+            st->done = 1;
+            st->nIters = 0;
+            set_condition(a.cond, 0u);
+            return;
+        }
+        st->norm_r = static_cast<T>(tot[1]);
+        st->res = st->norm_r / st->norm_b;
+        st->init_res = static_cast<double>(st->res);
+        st->cur_res = st->init_res;
+        st->rz = static_cast<T>(tot[2]);
+        st->iteration = 0;
+        // The stop test sees the iteration count the solver control held
+        // before this solve, as the reference's does.
+        if (solver_finished(*st, st->init_res)) {
+            st->nIters = 0;
+            st->done = 1;
+            set_condition(a.cond, 0u);
+        } else {
+            set_condition(a.cond, 1u);
+        }
+    }
+}
+
+// x += alpha p; r -= alpha y; z = M r; <r,z>, ||r||_1; beta, residual, stop test
+// (conjugate-gradients.hpp:186-224).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) cg_update_kernel(CgArgs<T> a) {
+    if (a.st->done) return;
+    const T alpha = a.st->alpha;
+    double acc[2] = {0.0, 0.0};
+    const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
+        const T xi = a.x[i] + alpha * a.p[i];
+        const T ri = a.r[i] - alpha * a.y[i];
+        const T zi = apply_m(a.invD, i, ri);
+        a.x[i] = xi;
+        a.r[i] = ri;
+        acc[0] += static_cast<double>(ri) * static_cast<double>(zi);
+        acc[1] += dabs(ri);
+    }
+    double tot[2];
+    if (dev::grid_reduce_last<2>(acc, a.parts, a.ticket, tot) && threadIdx.x == 0) {
+        SolverState<T>* st = a.st;
+        st->rz_old = st->rz;
+        st->rz = static_cast<T>(tot[0]);
+        st->beta = st->rz / st->rz_old;
+        st->norm_r = static_cast<T>(tot[1]);
+        st->res = st->norm_r / st->norm_b;
+        st->nIters = st->iteration;
+        st->iteration += 1;
+        st->cur_res = static_cast<double>(st->res);
+        if (!isfinite(st->cur_res)) st->status_bits |= kStatusNonFinite;
+        const bool fin = solver_finished(*st, st->cur_res);
+        st->done = fin ? 1 : 0;
+        set_condition(a.cond, fin ? 0u : 1u);
+    }
+}
+
+// p = z + beta p with z = M r recomputed (conjugate-gradients.hpp:211).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) cg_p_kernel(CgArgs<T> a) {
+    if (a.st->done) return;
+    const T beta = a.st->beta;
+    const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride)
+        a.p[i] = apply_m(a.invD, i, a.r[i]) + beta * a.p[i];
+}
+
+// ||b||_1 == 0: x = b (conjugate-gradients.hpp:87-95).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) copy_if_zero_b_kernel(T* x, const T* b, size_t n,
+                                                                  const SolverState<T>* st) {
+    if (!st->zero_b) return;
+    const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride)
+        x[i] = b[i];
+}
+
+// ----------------------------------------------------------- BiCGStab ----
+
+template <typename T>
+struct BicgArgs {
+    T* x;
+    const T* b;
+    T* y;    // A x at start
+    T* r;
+    T* rs;   // r*
+    T* p;
+    T* s;
+    T* Mp;   // == p without preconditioner
+    T* Ms;   // == s without preconditioner
+    T* AMp;
+    T* AMs;
+    const T* invD;
+    SolverState<T>* st;
+    double* parts;
+    uint32_t* ticket;
+    size_t n;
+    unsigned long long cond;
+};
+
+// r = b - A x; r* = r; p = r; Mp = M p; ||b||_1, ||r||_1, <r*,r>
+// (biconjugate-gradients-stabilized.hpp:61-131).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) bicg_init_kernel(BicgArgs<T> a) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
+        const T bi = a.b[i];
+        const T ri = bi - a.y[i];
+        a.r[i] = ri;
+        a.rs[i] = ri;
+        a.p[i] = ri;
+        if (a.invD) a.Mp[i] = ri * a.invD[i];
+        acc[0] += dabs(bi);
+        acc[1] += dabs(ri);
+        acc[2] += static_cast<double>(ri) * static_cast<double>(ri);
+    }
+    double tot[3];
+    if (dev::grid_reduce_last<3>(acc, a.parts, a.ticket, tot) && threadIdx.x == 0) {
+        SolverState<T>* st = a.st;
+        st->norm_b = static_cast<T>(tot[0]);
+        if (st->norm_b <= std::numeric_limits<T>::min()) {
+            st->zero_b = 1;
+            st->done = 1;
+            st->nIters = 0;
+            set_condition(a.cond, 0u);
+            return;
+        }
+        st->norm_r = static_cast<T>(tot[1]);
+        st->res = st->norm_r / st->norm_b;
+        st->init_res = static_cast<double>(st->res);
+        st->cur_res = st->init_res;
+        st->rsr_old = static_cast<T>(tot[2]);
+        st->iteration = 0;
+        if (solver_finished(*st, st->init_res)) {
+            st->nIters = 0;
+            st->done = 1;
+            set_condition(a.cond, 0u);
+        } else {
+            set_condition(a.cond, 1u);
+        }
+    }
+}
+
+// s = r - alpha AMp; Ms = M s; ||s||_1 and the first stop test
+// (biconjugate-gradients-stabilized.hpp:175-195). On stop, done = 2 asks the
+// x kernel to apply x += alpha Mp once and finish.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) bicg_s_kernel(BicgArgs<T> a) {
+    if (a.st->done) return;
+    const T alpha = a.st->alpha;
+    double acc[1] = {0.0};
+    const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
+        const T si = a.r[i] - alpha * a.AMp[i];
+        a.s[i] = si;
+        if (a.invD) a.Ms[i] = si * a.invD[i];
+        acc[0] += dabs(si);
+    }
+    double tot[1];
+    if (dev::grid_reduce_last<1>(acc, a.parts, a.ticket, tot) && threadIdx.x == 0) {
+        SolverState<T>* st = a.st;
+        const T norm_s = static_cast<T>(tot[0]);
+        st->res = norm_s / st->norm_b;
+        st->cur_res = static_cast<double>(st->res);
+        if (!isfinite(st->cur_res)) st->status_bits |= kStatusNonFinite;
+        if (solver_finished(*st, st->cur_res)) {
+            st->nIters = st->iteration;
+            st->exit_s = 1;
+            st->done = 2;
+            set_condition(a.cond, 0u);
+        }
+    }
+}
+
+// x = (x + alpha Mp) + omega Ms; r = s - omega AMs; ||r||_1, <r*,r>; second
+// stop test, beta (biconjugate-gradients-stabilized.hpp:213-250).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) bicg_x_kernel(BicgArgs<T> a) {
+    const int done = a.st->done;
+    if (done == 1) return;
+    const T alpha = a.st->alpha;
+    const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
+    double acc[2] = {0.0, 0.0};
+    if (done == 2) {
+        for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride)
+            a.x[i] = a.x[i] + alpha * a.Mp[i];
+    } else {
+        const T omega = a.st->omega;
+        for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
+            const T x1 = a.x[i] + alpha * a.Mp[i];
+            a.x[i] = x1 + omega * a.Ms[i];
+            const T ri = a.s[i] - omega * a.AMs[i];
+            a.r[i] = ri;
+            acc[0] += dabs(ri);
+            acc[1] += static_cast<double>(a.rs[i]) * static_cast<double>(ri);
+        }
+    }
+    double tot[2];
+    if (dev::grid_reduce_last<2>(acc, a.parts, a.ticket, tot) && threadIdx.x == 0) {
+        SolverState<T>* st = a.st;
+        if (done == 2) {
+            st->done = 1;
+            return;
+        }
+        st->norm_r = static_cast<T>(tot[0]);
+        st->res = st->norm_r / st->norm_b;
+        st->cur_res = static_cast<double>(st->res);
+        if (!isfinite(st->cur_res)) st->status_bits |= kStatusNonFinite;
+        if (solver_finished(*st, st->cur_res)) {
+            st->nIters = st->iteration;
+            st->done = 1;
+            set_condition(a.cond, 0u);
+            return;
+        }
+        st->rsr_new = static_cast<T>(tot[1]);
+        T beta = st->rsr_new / st->rsr_old;
+        beta = beta * st->alpha;
+        beta = beta / st->omega;
+        st->beta = beta;
+        st->rsr_old = st->rsr_new;
+        st->iteration += 1;
+        st->nIters = st->iteration;
+    }
+}
+
+// p = (r + beta p) - (beta omega) AMp; Mp = M p
+// (biconjugate-gradients-stabilized.hpp:252-262).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) bicg_p_kernel(BicgArgs<T> a) {
+    if (a.st->done) return;
+    const T beta = a.st->beta;
+    const T bw = beta * a.st->omega;
+    const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
+        const T p1 = a.r[i] + beta * a.p[i];
+        const T pi = p1 - bw * a.AMp[i];
+        a.p[i] = pi;
+        if (a.invD) a.Mp[i] = pi * a.invD[i];
+    }
+}
+
+// ---------------------------------------------------------- driver ----
+
+// Runs prologue / body / epilogue either as one graph with a conditional
+// WHILE node around the body (mode 0) or as host-enqueued chunks of bodies
+// that return at once after the device set done (mode 1).
+template <typename Pro, typename Body, typename Epi>
+clsparseStatus run_solve(clsparseControl c, SolverCache& cache, bool rebuild, const int* d_done,
+                         int max_iters, Pro prologue, Body body, Epi epilogue) {
+    cudaStream_t s = c->stream;
+    if (c->solver_loop_mode == 0) {
+        if (rebuild || cache.exec == nullptr) {
+            cache.drop_graph();
+            cudaStream_t cs = c->capture_stream;
+            cudaStream_t bs = nullptr;
+            if (cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking) != cudaSuccess)
+                return clsparseOutOfResources;
+            bool ok = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            cudaGraph_t g = nullptr;
+            cudaStreamCaptureStatus cst;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t ndeps = 0;
+            cudaGraphConditionalHandle h = 0;
+            ok = ok && cudaStreamGetCaptureInfo(cs, &cst, nullptr, &g, &deps, &ndeps) == cudaSuccess;
+            ok = ok && cudaGraphConditionalHandleCreate(&h, g, 0u, cudaGraphCondAssignDefault) ==
+                           cudaSuccess;
+            if (ok) prologue(cs, static_cast<unsigned long long>(h));
+            ok = ok && cudaStreamGetCaptureInfo(cs, &cst, nullptr, &g, &deps, &ndeps) == cudaSuccess;
+            cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t cn = nullptr;
+            ok = ok && cudaGraphAddNode(&cn, g, deps, ndeps, &cp) == cudaSuccess;
+            ok = ok && cudaStreamUpdateCaptureDependencies(cs, &cn, 1,
+                                                           cudaStreamSetCaptureDependencies) ==
+                           cudaSuccess;
+            if (ok) {
+                ok = cudaStreamBeginCaptureToGraph(bs, cp.conditional.phGraph_out[0], nullptr,
+                                                   nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+                     cudaSuccess;
+                if (ok) {
+                    body(bs, static_cast<unsigned long long>(h));
+                    cudaGraph_t bg = nullptr;
+                    ok = cudaStreamEndCapture(bs, &bg) == cudaSuccess;
+                }
+            }
+            if (ok) epilogue(cs);
+            cudaGraph_t full = nullptr;
+            const bool ended = cudaStreamEndCapture(cs, &full) == cudaSuccess;
+            cudaStreamDestroy(bs);
+            if (!ok || !ended) {
+                if (full) cudaGraphDestroy(full);
+                cudaGetLastError();
+                return clsparseInvalidKernelExecution;
+            }
+            cache.graph = full;
+            if (cudaGraphInstantiate(&cache.exec, full, 0) != cudaSuccess) {
+                cache.drop_graph();
+                cudaGetLastError();
+                return clsparseInvalidKernelExecution;
+            }
+        }
+        if (cudaGraphLaunch(cache.exec, s) != cudaSuccess) return clsparseInvalidKernelExecution;
+        return clsparseSuccess;
+    }
+    // mode 1: chunks of iterations, checking the device flag between chunks
+    prologue(s, 0ull);
+    int* h_done = static_cast<int*>(c->pinned) + 1000;
+    const int chunk = 16;
+    long long ran = 0;
+    while (true) {
+        for (int k = 0; k < chunk; ++k) body(s, 0ull);
+        ran += chunk;
+        cudaMemcpyAsync(h_done, d_done, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) return clsparseInvalidKernelExecution;
+        if (*h_done != 0) break;
+        if (max_iters >= 0 && ran > static_cast<long long>(max_iters) + 2 * chunk) break;
+    }
+    epilogue(s);
+    return cudaGetLastError() == cudaSuccess ? clsparseSuccess : clsparseInvalidKernelExecution;
+}
+
+template <typename T>
+CsrView<T> view_of(const clsparseCsrMatrix* A) {
+    return CsrView<T>{dev_ptr<const T>(A->values, A->off_values),
+                      dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices),
+                      dev_ptr<const uint32_t>(A->row_pointer, A->off_row_pointer), A->num_rows,
+                      A->num_cols, A->num_nonzeros, static_cast<const matrix_meta*>(A->meta)};
+}
+
+// Shared entry checks of the four solver entry points
+// (conjugate-gradients.cpp:18-116, conjugate-gradients.hpp:56-62).
+clsparseStatus check_solver_args(const cldenseVector* x, const clsparseCsrMatrix* A,
+                                 const cldenseVector* b, clSParseSolverControl sc,
+                                 clsparseControl c) {
+    clsparseStatus st = check_entry(c);
+    if (st != clsparseSuccess) return st;
+    if (sc == nullptr) return clsparseInvalidSolverControlObject;
+    if (!x || !A || !b) return clsparseInvalidValue;
+    if (A->num_cols != b->num_values || A->num_rows != x->num_values) return clsparseInvalidSystemSize;
+    if (A->num_rows != A->num_cols) return clsparseInvalidSystemSize;
+    if (A->num_rows > 0 && (!A->row_pointer || !x->values || !b->values)) return clsparseInvalidMemObject;
+    if (A->num_nonzeros > 0 && (!A->values || !A->col_indices)) return clsparseInvalidMemObject;
+    const auto* meta = static_cast<const matrix_meta*>(A->meta);
+    if (meta && (meta->rowBlockSize == 0 || meta->num_rows != A->num_rows)) return clsparseStructInvalid;
+    return clsparseSuccess;
+}
+
+template <typename T>
+void init_state(SolverState<T>& h, clSParseSolverControl sc) {
+    std::memset(&h, 0, sizeof(h));
+    h.relTol = sc->relativeTolerance;
+    h.absTol = sc->absoluteTolerance;
+    h.maxIters = sc->maxIters;
+    h.nIters = sc->nIters;
+    h.one = T(1);
+    h.zero = T(0);
+}
+
+// Copies the device state back into the solver control the way the
+// reference leaves it after a solve.
+template <typename T>
+clsparseStatus read_back(clsparseControl c, SolverCache& cache, clSParseSolverControl sc) {
+    auto* h = reinterpret_cast<SolverState<T>*>(static_cast<char*>(c->pinned) + 2048);
+    cudaMemcpyAsync(h, cache.state.ptr, sizeof(SolverState<T>), cudaMemcpyDeviceToHost, c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return clsparseInvalidKernelExecution;
+    if (c->event) cudaEventRecord(c->event, c->stream);
+    sc->deviceStatus = static_cast<cl_uint>(h->status_bits);
+    if (h->zero_b) {
+        // conjugate-gradients.hpp:87-95 resets the tolerances of the control
+        sc->nIters = 0;
+        sc->absoluteTolerance = 0.0;
+        sc->relativeTolerance = 0.0;
+        return clsparseSuccess;
+    }
+    sc->initialResidual = h->init_res;
+    sc->currentResidual = h->cur_res;
+    sc->nIters = h->nIters;
+    return clsparseSuccess;
+}
+
+SolverKey make_key(int kind, int dsize, clSParseSolverControl sc, clsparseControl c,
+                   const clsparseCsrMatrix* A, const cldenseVector* x, const cldenseVector* b) {
+    SolverKey k;
+    std::memset(&k, 0, sizeof(k));
+    k.kind = kind;
+    k.dtype = dsize;
+    k.precond = sc->preconditioner == DIAGONAL ? 1 : 0;
+    k.ext = c->extended_precision ? 1 : 0;
+    k.loop_mode = c->solver_loop_mode;
+    k.ptrs[0] = static_cast<const char*>(A->values) + static_cast<size_t>(A->off_values) * dsize;
+    k.ptrs[1] = static_cast<const uint32_t*>(A->col_indices) + A->off_col_indices;
+    k.ptrs[2] = static_cast<const uint32_t*>(A->row_pointer) + A->off_row_pointer;
+    k.ptrs[3] = static_cast<const char*>(x->values) + static_cast<size_t>(x->off_values) * dsize;
+    k.ptrs[4] = static_cast<const char*>(b->values) + static_cast<size_t>(b->off_values) * dsize;
+    k.ptrs[5] = A->meta;
+    k.n = A->num_rows;
+    k.nnz = A->num_nonzeros;
+    k.meta_words = A->meta ? static_cast<const matrix_meta*>(A->meta)->num_words : 0;
+    k.stream = c->stream;
+    return k;
+}
+
+// Sizes the cache for `nvec` work vectors of n elements and the reduction
+// partials of both the SpMV and the vector kernels.
+template <typename T>
+clsparseStatus prepare_cache(clsparseControl c, SolverCache& cache, const SolverKey& key, int nvec,
+                             size_t n, uint32_t spmv_ctas, bool& rebuild) {
+    rebuild = !(cache.valid && cache.key == key);
+    const size_t vec_bytes = ((n * sizeof(T) + 255) / 256) * 256;
+    const size_t parts_doubles = std::max<size_t>(3 * kMaxReduceCtas, 2 * static_cast<size_t>(spmv_ctas));
+    if (cache.vecs.ensure(vec_bytes * nvec + 256) != cudaSuccess ||
+        cache.parts.ensure(parts_doubles * sizeof(double) + 256) != cudaSuccess ||
+        cache.state.ensure(sizeof(SolverState<T>) + 256) != cudaSuccess) {
+        cudaGetLastError();
+        cache.valid = false;
+        return clsparseOutOfResources;
+    }
+    if (rebuild) {
+        // tickets start at zero; kernels leave them at zero
+        cudaMemsetAsync(cache.parts.ptr, 0, cache.parts.bytes, c->stream);
+        cache.drop_graph();
+    }
+    cache.key = key;
+    cache.valid = true;
+    return clsparseSuccess;
+}
+
+template <typename T>
+clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
+                        clSParseSolverControl sc, clsparseControl c) {
+    clsparseStatus stt = check_solver_args(xv, A, bv, sc, c);
+    if (stt != clsparseSuccess) return stt;
+    DeviceGuard guard(c->device);
+    const size_t n = A->num_rows;
+    if (!c->solver_cache) c->solver_cache = std::make_unique<SolverCache>();
+    SolverCache& cache = *c->solver_cache;
+    const CsrView<T> Av = view_of<T>(A);
+    const uint32_t spmv_ctas = spmv_num_ctas(Av.meta, Av.nrows, Av.nnz);
+    const SolverKey key = make_key(1, sizeof(T), sc, c, A, xv, bv);
+    bool rebuild = false;
+    stt = prepare_cache<T>(c, cache, key, 4, n, spmv_ctas, rebuild);
+    if (stt != clsparseSuccess) return stt;
+
+    const size_t vb = ((n * sizeof(T) + 255) / 256) * 256;
+    char* base = static_cast<char*>(cache.vecs.ptr);
+    CgArgs<T> a;
+    a.x = dev_ptr<T>(xv->values, xv->off_values);
+    a.b = dev_ptr<const T>(bv->values, bv->off_values);
+    a.y = reinterpret_cast<T*>(base);
+    a.r = reinterpret_cast<T*>(base + vb);
+    a.p = reinterpret_cast<T*>(base + 2 * vb);
+    T* invD = reinterpret_cast<T*>(base + 3 * vb);
+    a.invD = key.precond ? invD : nullptr;
+    a.st = static_cast<SolverState<T>*>(cache.state.ptr);
+    a.parts = static_cast<double*>(cache.parts.ptr) + 1;
+    a.ticket = static_cast<uint32_t*>(cache.parts.ptr);
+    a.n = n;
+    a.cond = 0;
+
+    auto* hs = reinterpret_cast<SolverState<T>*>(c->pinned);
+    init_state(*hs, sc);
+    cudaMemcpyAsync(a.st, hs, sizeof(SolverState<T>), cudaMemcpyHostToDevice, c->stream);
+
+    const uint32_t vg = vec_grid(n, c->sm_count);
+    const bool ext = c->extended_precision;
+    SolverState<T>* st = a.st;
+
+    auto prologue = [&](cudaStream_t s, unsigned long long h) {
+        CgArgs<T> aa = a;
+        aa.cond = h;
+        if (aa.invD)
+            extract_inv_diag_kernel<T><<<vg, kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
+                                                               invD, st);
+        SpmvEpilogue none;
+        launch_csrmv<T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
+        cg_init_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+    };
+    auto body = [&](cudaStream_t s, unsigned long long h) {
+        CgArgs<T> aa = a;
+        aa.cond = h;
+        SpmvEpilogue epi;
+        epi.ndots = 1;
+        epi.w0 = aa.p;
+        epi.partials = aa.parts;
+        epi.ticket = aa.ticket;
+        epi.op = EpiOp::CgAlpha;
+        epi.state = st;
+        epi.done = &st->done;
+        launch_csrmv<T>(Av, &st->one, &st->zero, aa.p, aa.y, ext, epi, s);
+        cg_update_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+        cg_p_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+    };
+    auto epilogue = [&](cudaStream_t s) {
+        copy_if_zero_b_kernel<T><<<vg, kThreads, 0, s>>>(a.x, a.b, n, st);
+    };
+    if (n == 0) {
+        sc->nIters = 0;
+        return clsparseSuccess;
+    }
+    stt = run_solve(c, cache, rebuild, &st->done, sc->maxIters, prologue, body, epilogue);
+    if (stt != clsparseSuccess) {
+        cache.valid = false;
+        cache.drop_graph();
+        return stt;
+    }
+    stt = read_back<T>(c, cache, sc);
+    sc->printSummary(stt);
+    return stt;
+}
+
+template <typename T>
+clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
+                          clSParseSolverControl sc, clsparseControl c) {
+    clsparseStatus stt = check_solver_args(xv, A, bv, sc, c);
+    if (stt != clsparseSuccess) return stt;
+    DeviceGuard guard(c->device);
+    const size_t n = A->num_rows;
+    if (!c->solver_cache) c->solver_cache = std::make_unique<SolverCache>();
+    SolverCache& cache = *c->solver_cache;
+    const CsrView<T> Av = view_of<T>(A);
+    const uint32_t spmv_ctas = spmv_num_ctas(Av.meta, Av.nrows, Av.nnz);
+    const SolverKey key = make_key(2, sizeof(T), sc, c, A, xv, bv);
+    bool rebuild = false;
+    stt = prepare_cache<T>(c, cache, key, 11, n, spmv_ctas, rebuild);
+    if (stt != clsparseSuccess) return stt;
+
+    const size_t vb = ((n * sizeof(T) + 255) / 256) * 256;
+    char* base = static_cast<char*>(cache.vecs.ptr);
+    auto vec = [&](int k) { return reinterpret_cast<T*>(base + static_cast<size_t>(k) * vb); };
+    BicgArgs<T> a;
+    a.x = dev_ptr<T>(xv->values, xv->off_values);
+    a.b = dev_ptr<const T>(bv->values, bv->off_values);
+    a.y = vec(0);
+    a.r = vec(1);
+    a.rs = vec(2);
+    a.p = vec(3);
+    a.s = vec(4);
+    a.AMp = vec(5);
+    a.AMs = vec(6);
+    T* invD = vec(7);
+    const bool pre = key.precond != 0;
+    a.Mp = pre ? vec(8) : a.p;
+    a.Ms = pre ? vec(9) : a.s;
+    a.invD = pre ? invD : nullptr;
+    a.st = static_cast<SolverState<T>*>(cache.state.ptr);
+    a.parts = static_cast<double*>(cache.parts.ptr) + 1;
+    a.ticket = static_cast<uint32_t*>(cache.parts.ptr);
+    a.n = n;
+    a.cond = 0;
+
+    auto* hs = reinterpret_cast<SolverState<T>*>(c->pinned);
+    init_state(*hs, sc);
+    cudaMemcpyAsync(a.st, hs, sizeof(SolverState<T>), cudaMemcpyHostToDevice, c->stream);
+
+    const uint32_t vg = vec_grid(n, c->sm_count);
+    const bool ext = c->extended_precision;
+    SolverState<T>* st = a.st;
+
+    auto prologue = [&](cudaStream_t s, unsigned long long h) {
+        BicgArgs<T> aa = a;
+        aa.cond = h;
+        if (aa.invD)
+            extract_inv_diag_kernel<T><<<vg, kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
+                                                               invD, st);
+        SpmvEpilogue none;
+        launch_csrmv<T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
+        bicg_init_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+    };
+    auto body = [&](cudaStream_t s, unsigned long long h) {
+        BicgArgs<T> aa = a;
+        aa.cond = h;
+        SpmvEpilogue e1;
+        e1.ndots = 1;
+        e1.w0 = aa.rs;
+        e1.partials = aa.parts;
+        e1.ticket = aa.ticket;
+        e1.op = EpiOp::BicgAlpha;
+        e1.state = st;
+        e1.done = &st->done;
+        launch_csrmv<T>(Av, &st->one, &st->zero, aa.Mp, aa.AMp, ext, e1, s);
+        bicg_s_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+        SpmvEpilogue e2;
+        e2.ndots = 2;
+        e2.w0 = aa.s;
+        e2.dot1_self = true;
+        e2.partials = aa.parts;
+        e2.ticket = aa.ticket;
+        e2.op = EpiOp::BicgOmega;
+        e2.state = st;
+        e2.done = &st->done;
+        launch_csrmv<T>(Av, &st->one, &st->zero, aa.Ms, aa.AMs, ext, e2, s);
+        bicg_x_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+        bicg_p_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+    };
+    auto epilogue = [&](cudaStream_t s) {
+        copy_if_zero_b_kernel<T><<<vg, kThreads, 0, s>>>(a.x, a.b, n, st);
+    };
+    if (n == 0) {
+        sc->nIters = 0;
+        return clsparseSuccess;
+    }
+    stt = run_solve(c, cache, rebuild, &st->done, sc->maxIters, prologue, body, epilogue);
+    if (stt != clsparseSuccess) {
+        cache.valid = false;
+        cache.drop_graph();
+        return stt;
+    }
+    stt = read_back<T>(c, cache, sc);
+    sc->printSummary(stt);
+    return stt;
+}
+
+}  // namespace
+}  // namespace clsp
+
+using namespace clsp;
+
+extern "C" {
+
+clsparseStatus clsparseScsrcg(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                              clSParseSolverControl solverControl, clsparseControl control) {
+    return cg_solve<float>(x, A, b, solverControl, control);
+}
+
+clsparseStatus clsparseDcsrcg(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                              clSParseSolverControl solverControl, clsparseControl control) {
+    return cg_solve<double>(x, A, b, solverControl, control);
+}
+
+clsparseStatus clsparseScsrbicgStab(cldenseVector* x, const clsparseCsrMatrix* A,
+                                    const cldenseVector* b, clSParseSolverControl solverControl,
+                                    clsparseControl control) {
+    return bicg_solve<float>(x, A, b, solverControl, control);
+}
+
+clsparseStatus clsparseDcsrbicgStab(cldenseVector* x, const clsparseCsrMatrix* A,
+                                    const cldenseVector* b, clSParseSolverControl solverControl,
+                                    clsparseControl control) {
+    return bicg_solve<double>(x, A, b, solverControl, control);
+}
+
+}  // extern "C"

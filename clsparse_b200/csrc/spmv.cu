@@ -1,0 +1,405 @@
+// CSR sparse matrix-vector product y = alpha*A*x + beta*y for sm_100a, and the
+// clsparseScsrmv / clsparseDcsrmv entry points.
+//
+// Two kernels, chosen as the reference chooses (src/library/blas2/clsparse-csrmv.hpp:103-132):
+//
+// * csr_adaptive_kernel -- with a meta (row-block words from
+//   clsparseCsrMetaCreate) one 256-thread CTA runs per word, in one of three
+//   modes decided from the word pair (the CSR-Adaptive scheme of the reference's
+//   src/library/kernels/csrmv_adaptive.cl:312-687, rebuilt for B200):
+//     STREAM  a block of several short rows (<= 1024 nonzeros in total): the CTA
+//             streams alpha*val*x[col] for the whole block into shared memory
+//             with coalesced evict-first loads, then reduces every row out of
+//             shared memory with groups of up to 32 lanes (warp shuffles, no
+//             shared-memory tree).
+//     VECTOR  one row (up to 3072 nonzeros): the whole CTA reduces it.
+//     LONG    one chunk of 3072 nonzeros of a longer row. Each chunk CTA writes
+//             its partial sum to the meta's partial slot and takes an arrival
+//             ticket; the CTA that arrives last adds the partials in chunk order
+//             and writes y. No CTA waits for another (the reference spin-waits on
+//             a flag it flips inside the meta, csrmv_adaptive.cl:596-600), the
+//             result does not depend on arrival order, and the meta is left as
+//             it was found.
+// * csr_vector_kernel -- without a meta, G lanes per row (G = 2..32 from the
+//   average row length, as csrmv-vector.hpp:34-49 picks its sub-wave).
+//
+// beta == 0 overwrites y without reading it on every path (the reference reads
+// y on its LONG path; csrmv_adaptive.cl:481-483 skips it on the others).
+//
+// Both kernels can fuse the dot products a Krylov solver takes of the result
+// (<y, w> and <y, y>) and finish them with a deterministic grid reduction.
+#include <algorithm>
+#include <type_traits>
+
+#include "device_common.cuh"
+#include "internal.h"
+#include "solver_state.cuh"
+
+namespace clsp {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr uint32_t kLongChunk = kBlkSize * kBlockMultiplier;  // 3072 nonzeros per CTA
+
+template <typename T>
+struct EpiDev {
+    const T* w0;
+    int dot1_self;
+    double* partials;
+    uint32_t* ticket;
+    int op;
+    void* state;
+    unsigned long long cond;
+    const int* done;
+};
+
+template <typename T, int K>
+struct RowSink {
+    T* y;
+    const T* w0;
+    int dot1_self;
+    T beta;
+    double d[K > 0 ? K : 1];
+    __device__ __forceinline__ void init(T* y_, const EpiDev<T>& e, T beta_) {
+        y = y_;
+        w0 = e.w0;
+        dot1_self = e.dot1_self;
+        beta = beta_;
+#pragma unroll
+        for (int k = 0; k < (K > 0 ? K : 1); ++k) d[k] = 0.0;
+    }
+    // Final value of one row: adds beta*y (reading y only if beta != 0),
+    // stores it and feeds the fused dot products.
+    template <bool EXT>
+    __device__ __forceinline__ void put(uint32_t row, dev::Acc<T, EXT> a) {
+        if (beta != T(0)) a.add_prod(beta, y[row]);
+        const T v = a.value();
+        y[row] = v;
+        if constexpr (K >= 1) d[0] += static_cast<double>(v) * static_cast<double>(w0[row]);
+        if constexpr (K >= 2) {
+            if (dot1_self) d[1] += static_cast<double>(v) * static_cast<double>(v);
+        }
+    }
+};
+
+template <typename T, int K>
+__device__ __forceinline__ void run_epilogue(RowSink<T, K>& sink, const EpiDev<T>& e) {
+    if constexpr (K > 0) {
+        double tot[K];
+        if (dev::grid_reduce_last<K>(sink.d, e.partials, e.ticket, tot)) {
+            if (threadIdx.x == 0) {
+                auto* st = static_cast<SolverState<T>*>(e.state);
+                if (e.op == static_cast<int>(EpiOp::CgAlpha)) fin_cg_alpha(st, tot[0]);
+                if (e.op == static_cast<int>(EpiOp::BicgAlpha)) fin_bicg_alpha(st, tot[0]);
+                if constexpr (K >= 2) {
+                    if (e.op == static_cast<int>(EpiOp::BicgOmega)) fin_bicg_omega(st, tot[0], tot[1]);
+                }
+            }
+        }
+    }
+}
+
+template <typename T, bool EXT, int K>
+__global__ void __launch_bounds__(kThreads)
+    csr_adaptive_kernel(const T* __restrict__ vals, const uint32_t* __restrict__ cols,
+                        const uint32_t* __restrict__ rp, const T* __restrict__ x, T* __restrict__ y,
+                        const T* __restrict__ alpha_p, const T* __restrict__ beta_p,
+                        const uint64_t* __restrict__ words, uint32_t nblocks,
+                        double* __restrict__ lr_partial, uint32_t* __restrict__ lr_ticket,
+                        EpiDev<T> epi) {
+    __shared__ T stage[kBlkSize];
+    __shared__ T red_s[32];
+    __shared__ T red_c[32];
+    __shared__ bool lr_last;
+
+    if (epi.done != nullptr && *epi.done) return;
+
+    const T alpha = *alpha_p;
+    RowSink<T, K> sink;
+    sink.init(y, epi, *beta_p);
+
+    const uint32_t gid = blockIdx.x;
+    if (gid < nblocks) {
+        const uint64_t w0 = words[gid];
+        const uint64_t w1 = words[gid + 1];
+        const uint32_t row = static_cast<uint32_t>(w0 >> 32);
+        const uint32_t stop = static_cast<uint32_t>(w1 >> 32);
+        const uint32_t low = static_cast<uint32_t>(w0 & ((1u << kWgBits) - 1u));
+        const uint32_t nrows = stop - row;
+        const int tid = threadIdx.x;
+
+        if (nrows > kRowsForVector) {
+            // ---- STREAM: several short rows, <= kBlkSize nonzeros in total ----
+            const uint32_t nb = dev::ld_ro(rp + row);
+            const uint32_t cnt = dev::ld_ro(rp + stop) - nb;
+            // A block from clsparseCsrMetaCreate never exceeds the staging
+            // buffer; if the row pointers changed after the meta was made, the
+            // rows are summed straight from global memory instead.
+            const bool staged = cnt <= kBlkSize;
+            if (staged) {
+                for (uint32_t i = tid; i < cnt; i += kThreads) {
+                    const uint32_t c = dev::ld_stream(cols + nb + i);
+                    const T v = dev::ld_stream(vals + nb + i);
+                    stage[i] = dev::mul_rn(alpha * v, dev::ld_ro(x + c));
+                }
+            }
+            __syncthreads();
+            // Lanes per row: the reference's per-block reduction width, capped at
+            // one warp so each row reduces with shuffles inside a warp.
+            uint32_t g = low == 0 ? 1u : (low > 32u ? 32u : low);
+            auto reduce_rows = [&](auto gw) {
+                constexpr int G = decltype(gw)::value;
+                const uint32_t groups = kThreads / G;
+                const uint32_t grp = tid / G;
+                const uint32_t lane = tid & (G - 1);
+                for (uint32_t base = 0; base < nrows; base += groups) {
+                    const uint32_t r = base + grp;
+                    dev::Acc<T, EXT> a;
+                    if (r < nrows) {
+                        const uint32_t f = dev::ld_ro(rp + row + r) - nb;
+                        const uint32_t l = dev::ld_ro(rp + row + r + 1) - nb;
+                        if (staged) {
+                            for (uint32_t j = f + lane; j < l; j += G) a.add(stage[j]);
+                        } else {
+                            for (uint32_t j = nb + f + lane; j < nb + l; j += G)
+                                a.add(dev::mul_rn(alpha * vals[j], dev::ld_ro(x + cols[j])));
+                        }
+                    }
+                    dev::group_reduce<G>(a);
+                    if (r < nrows && lane == 0) sink.template put<EXT>(row + r, a);
+                }
+            };
+            switch (g) {
+                case 1: reduce_rows(std::integral_constant<int, 1>{}); break;
+                case 2: reduce_rows(std::integral_constant<int, 2>{}); break;
+                case 4: reduce_rows(std::integral_constant<int, 4>{}); break;
+                case 8: reduce_rows(std::integral_constant<int, 8>{}); break;
+                case 16: reduce_rows(std::integral_constant<int, 16>{}); break;
+                default: reduce_rows(std::integral_constant<int, 32>{}); break;
+            }
+        } else if (nrows == 1 && low == 0) {
+            // ---- VECTOR: one row, the whole CTA ----
+            const uint32_t nb = dev::ld_ro(rp + row);
+            const uint32_t ne = dev::ld_ro(rp + row + 1);
+            dev::Acc<T, EXT> a;
+#pragma unroll 4
+            for (uint32_t j = nb + tid; j < ne; j += kThreads)
+                a.add_prod(alpha * dev::ld_stream(vals + j), dev::ld_ro(x + dev::ld_stream(cols + j)));
+            a = dev::block_reduce_acc(a, red_s, red_c);
+            if (tid == 0) sink.template put<EXT>(row, a);
+        } else {
+            // ---- LONG: chunk `low` of a row split over several CTAs ----
+            const uint32_t nb = dev::ld_ro(rp + row);
+            const uint32_t ne = dev::ld_ro(rp + row + 1);
+            const uint32_t len = ne - nb;
+            const uint32_t nchunks = (len + kLongChunk - 1) / kLongChunk;
+            if (nchunks >= 2 && low < nchunks) {
+                const uint32_t first = gid - low;
+                const uint32_t cb = nb + low * kLongChunk;
+                const uint32_t ce = min(ne, cb + kLongChunk);
+                dev::Acc<T, EXT> a;
+#pragma unroll 4
+                for (uint32_t j = cb + tid; j < ce; j += kThreads)
+                    a.add_prod(alpha * dev::ld_stream(vals + j), dev::ld_ro(x + dev::ld_stream(cols + j)));
+                a = dev::block_reduce_acc(a, red_s, red_c);
+                if (tid == 0) {
+                    // partial of this chunk; compensation folded in
+                    lr_partial[gid] = static_cast<double>(a.value());
+                    __threadfence();
+                    const uint32_t t = atomicAdd(lr_ticket + first, 1u);
+                    lr_last = (t == nchunks - 1);
+                }
+                __syncthreads();
+                if (lr_last && tid == 0) {
+                    __threadfence();
+                    dev::Acc<T, EXT> tot;
+                    for (uint32_t w = 0; w < nchunks; ++w)
+                        tot.add(static_cast<T>(__ldcg(lr_partial + first + w)));
+                    lr_ticket[first] = 0u;
+                    sink.template put<EXT>(row, tot);
+                }
+            }
+        }
+    }
+    run_epilogue<T, K>(sink, epi);
+}
+
+template <typename T, bool EXT, int G, int K>
+__global__ void __launch_bounds__(kThreads)
+    csr_vector_kernel(const T* __restrict__ vals, const uint32_t* __restrict__ cols,
+                      const uint32_t* __restrict__ rp, const T* __restrict__ x, T* __restrict__ y,
+                      const T* __restrict__ alpha_p, const T* __restrict__ beta_p, uint32_t nrows,
+                      EpiDev<T> epi) {
+    if (epi.done != nullptr && *epi.done) return;
+    const T alpha = *alpha_p;
+    RowSink<T, K> sink;
+    sink.init(y, epi, *beta_p);
+    const uint32_t lane = threadIdx.x & (G - 1);
+    const uint64_t gtid = static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
+    const uint32_t grp = static_cast<uint32_t>(gtid / G);
+    const uint32_t ngroups = static_cast<uint32_t>(static_cast<uint64_t>(gridDim.x) * kThreads / G);
+    for (uint32_t base = 0; base < nrows; base += ngroups) {
+        const uint32_t row = base + grp;
+        dev::Acc<T, EXT> a;
+        if (row < nrows) {
+            const uint32_t nb = dev::ld_ro(rp + row);
+            const uint32_t ne = dev::ld_ro(rp + row + 1);
+            for (uint32_t j = nb + lane; j < ne; j += G)
+                a.add_prod(alpha * dev::ld_stream(vals + j), dev::ld_ro(x + dev::ld_stream(cols + j)));
+        }
+        dev::group_reduce<G>(a);
+        if (row < nrows && lane == 0) sink.template put<EXT>(row, a);
+        if (base > 0xFFFFFFFFu - ngroups) break;
+    }
+    run_epilogue<T, K>(sink, epi);
+}
+
+template <typename T>
+EpiDev<T> to_dev(const SpmvEpilogue& e) {
+    EpiDev<T> d;
+    d.w0 = static_cast<const T*>(e.w0);
+    d.dot1_self = e.dot1_self ? 1 : 0;
+    d.partials = e.partials;
+    d.ticket = e.ticket;
+    d.op = static_cast<int>(e.op);
+    d.state = e.state;
+    d.cond = e.cond;
+    d.done = e.done;
+    return d;
+}
+
+// Sub-warp width of the vector kernel from the average row length
+// (reference blas2/csrmv-vector.hpp:34-49 with a 32-wide warp).
+uint32_t vector_width(uint32_t nrows, uint32_t nnz) {
+    const uint32_t per_row = nrows ? nnz / nrows : 0;
+    uint32_t g = 32;
+    if (per_row < 32) g = 16;
+    if (per_row < 16) g = 8;
+    if (per_row < 8) g = 4;
+    if (per_row < 4) g = 2;
+    return g;
+}
+
+uint32_t vector_grid(uint32_t nrows, uint32_t g) {
+    const uint64_t threads = static_cast<uint64_t>(nrows) * g;
+    uint64_t ctas = (threads + kThreads - 1) / kThreads;
+    if (ctas == 0) ctas = 1;
+    if (ctas > 0x7fffffffull) ctas = 0x7fffffffull;
+    return static_cast<uint32_t>(ctas);
+}
+
+template <typename T, bool EXT, int K>
+cudaError_t launch_vector(const CsrView<T>& A, const T* alpha, const T* beta, const T* x, T* y,
+                          const EpiDev<T>& e, cudaStream_t s) {
+    const uint32_t g = vector_width(A.nrows, A.nnz);
+    const uint32_t grid = vector_grid(A.nrows, g);
+#define CLSP_VEC(GW)                                                                              \
+    csr_vector_kernel<T, EXT, GW, K><<<grid, kThreads, 0, s>>>(A.vals, A.cols, A.rp, x, y, alpha, \
+                                                               beta, A.nrows, e)
+    switch (g) {
+        case 2: CLSP_VEC(2); break;
+        case 4: CLSP_VEC(4); break;
+        case 8: CLSP_VEC(8); break;
+        case 16: CLSP_VEC(16); break;
+        default: CLSP_VEC(32); break;
+    }
+#undef CLSP_VEC
+    return cudaGetLastError();
+}
+
+template <typename T, bool EXT, int K>
+cudaError_t launch_kind(const CsrView<T>& A, const T* alpha, const T* beta, const T* x, T* y,
+                        const EpiDev<T>& e, cudaStream_t s) {
+    if (A.meta == nullptr) return launch_vector<T, EXT, K>(A, alpha, beta, x, y, e, s);
+    const uint32_t nblocks = static_cast<uint32_t>(A.meta->num_words - 1);
+    uint32_t grid = nblocks;
+    if (grid == 0) {
+        if (K == 0) return cudaSuccess;
+        grid = 1;  // one idle CTA still finishes the fused reduction
+    }
+    csr_adaptive_kernel<T, EXT, K><<<grid, kThreads, 0, s>>>(
+        A.vals, A.cols, A.rp, x, y, alpha, beta, A.meta->d_rowBlocks, nblocks,
+        A.meta->d_lr_partial, A.meta->d_lr_ticket, e);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+uint32_t spmv_num_ctas(const matrix_meta* meta, uint32_t nrows, uint32_t nnz) {
+    if (meta) return std::max<uint32_t>(1u, static_cast<uint32_t>(meta->num_words - 1));
+    return vector_grid(nrows, vector_width(nrows, nnz));
+}
+
+template <typename T>
+cudaError_t launch_csrmv(const CsrView<T>& A, const T* alpha, const T* beta, const T* x, T* y,
+                         bool extended, const SpmvEpilogue& epi, cudaStream_t s) {
+    const EpiDev<T> e = to_dev<T>(epi);
+    if (extended) {
+        if (epi.ndots == 0) return launch_kind<T, true, 0>(A, alpha, beta, x, y, e, s);
+        if (epi.ndots == 1) return launch_kind<T, true, 1>(A, alpha, beta, x, y, e, s);
+        return launch_kind<T, true, 2>(A, alpha, beta, x, y, e, s);
+    }
+    if (epi.ndots == 0) return launch_kind<T, false, 0>(A, alpha, beta, x, y, e, s);
+    if (epi.ndots == 1) return launch_kind<T, false, 1>(A, alpha, beta, x, y, e, s);
+    return launch_kind<T, false, 2>(A, alpha, beta, x, y, e, s);
+}
+
+template cudaError_t launch_csrmv<float>(const CsrView<float>&, const float*, const float*,
+                                         const float*, float*, bool, const SpmvEpilogue&,
+                                         cudaStream_t);
+template cudaError_t launch_csrmv<double>(const CsrView<double>&, const double*, const double*,
+                                          const double*, double*, bool, const SpmvEpilogue&,
+                                          cudaStream_t);
+
+namespace {
+
+template <typename T>
+clsparseStatus csrmv_entry(const clsparseScalar* alpha, const clsparseCsrMatrix* A,
+                           const cldenseVector* x, const clsparseScalar* beta, cldenseVector* y,
+                           clsparseControl control) {
+    clsparseStatus st = check_entry(control);
+    if (st != clsparseSuccess) return st;
+    if (!alpha || !A || !x || !beta || !y) return clsparseInvalidValue;
+    if (x->num_values < A->num_cols || y->num_values < A->num_rows) return clsparseInvalidSize;
+    if (A->num_rows == 0) return clsparseSuccess;
+    if (!alpha->value || !beta->value || !x->values || !y->values || !A->row_pointer ||
+        (A->num_nonzeros > 0 && (!A->values || !A->col_indices)))
+        return clsparseInvalidMemObject;
+    const auto* meta = static_cast<const matrix_meta*>(A->meta);
+    if (meta && meta->rowBlockSize == 0) return clsparseStructInvalid;
+    if (meta && meta->num_rows != A->num_rows) return clsparseStructInvalid;
+    DeviceGuard g(control->device);
+    CsrView<T> v{dev_ptr<const T>(A->values, A->off_values),
+                 dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices),
+                 dev_ptr<const uint32_t>(A->row_pointer, A->off_row_pointer),
+                 A->num_rows, A->num_cols, A->num_nonzeros, meta};
+    SpmvEpilogue none;
+    cudaError_t e = launch_csrmv<T>(v, dev_ptr<const T>(alpha->value, alpha->off_value),
+                                    dev_ptr<const T>(beta->value, beta->off_value),
+                                    dev_ptr<const T>(x->values, x->off_values),
+                                    dev_ptr<T>(y->values, y->off_values), control->extended_precision,
+                                    none, control->stream);
+    if (e != cudaSuccess) return clsparseInvalidKernelExecution;
+    return finish_call(control);
+}
+
+}  // namespace
+
+}  // namespace clsp
+
+extern "C" {
+
+clsparseStatus clsparseScsrmv(const clsparseScalar* alpha, const clsparseCsrMatrix* matx,
+                              const cldenseVector* x, const clsparseScalar* beta, cldenseVector* y,
+                              const clsparseControl control) {
+    return clsp::csrmv_entry<float>(alpha, matx, x, beta, y, control);
+}
+
+clsparseStatus clsparseDcsrmv(const clsparseScalar* alpha, const clsparseCsrMatrix* matx,
+                              const cldenseVector* x, const clsparseScalar* beta, cldenseVector* y,
+                              const clsparseControl control) {
+    return clsp::csrmv_entry<double>(alpha, matx, x, beta, y, control);
+}
+
+}  // extern "C"

@@ -1,0 +1,167 @@
+"""CG / BiCGStab through the C ABI against the oracle restatement of the
+reference solvers (src/library/solvers/conjugate-gradients.hpp,
+biconjugate-gradients-stabilized.hpp).
+
+Parity bar: the same stop decision (iteration counts within a small slack --
+the GPU sums reductions in a different order), the reported residuals agree,
+and the returned x meets the stop criterion on a fresh FP64 check."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from clsparse_b200 import _lib as L
+from clsparse_b200 import api, matgen
+
+pytestmark = pytest.mark.gpu
+
+NP = {torch.float64: np.float64, torch.float32: np.float32}
+
+
+def run(ctrl, kind, rp, col, val, x0, b, dtype, precond, max_iters, rel, abs_, meta=True, loop_mode=0):
+    ctrl.set_solver_loop_mode(loop_mode)
+    A = api.CsrMatrix.from_numpy(rp, col, val, dtype=dtype)
+    if meta:
+        A.create_meta(ctrl)
+    x = torch.tensor(np.asarray(x0), dtype=dtype, device="cuda")
+    bt = torch.tensor(np.asarray(b), dtype=dtype, device="cuda")
+    sc = api.SolverControl(precond, max_iters, rel, abs_)
+    info = api.solve(kind, x, A, bt, sc, ctrl)
+    status = sc.device_status()
+    sc.release()
+    return x.cpu().numpy().astype(np.float64), info, status
+
+
+def l1_residual(rp, col, val, x, b):
+    import scipy.sparse as sp
+    n = len(rp) - 1
+    A = sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64)), shape=(n, n))
+    return np.abs(b - A @ x).sum() / np.abs(b).sum()
+
+
+PROBLEMS = {
+    "poisson64": lambda: matgen.poisson2d(64),
+    "diffusion3d": lambda: matgen.diffusion3d_lognormal(16, sigma=1.0, seed=2),
+    "random_spd": lambda: matgen.random_spd(5000, seed=3),
+}
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+@pytest.mark.parametrize("precond", [L.DIAGONAL, L.NOPRECOND], ids=["jacobi", "none"])
+@pytest.mark.parametrize("prob", sorted(PROBLEMS))
+@pytest.mark.parametrize("kind", ["cg", "bicgstab"])
+def test_solver_parity(ctrl, orc, kind, prob, precond, dtype):
+    rp, col, val = PROBLEMS[prob]()
+    n = len(rp) - 1
+    b = np.random.default_rng(1).uniform(-1, 1, n)
+    rel = 1e-10 if dtype == torch.float64 else 1e-5
+    t = NP[dtype]
+    x, info, _ = run(ctrl, kind, rp, col, val, np.zeros(n), b, dtype, precond, 5000, rel, 0.0)
+    xo, oi = orc.solve(kind, t, rp, col, val, np.zeros(n, t), np.asarray(b, t), precond, 5000, rel, 0.0)
+    slack = max(3, int(0.03 * oi.nIters))
+    assert abs(info["nIters"] - oi.nIters) <= slack, (info, oi.nIters)
+    assert info["initialResidual"] == pytest.approx(oi.initialResidual, rel=1e-5)
+    assert info["currentResidual"] <= rel
+    r_true = l1_residual(rp, col, np.asarray(val, t).astype(np.float64), x, np.asarray(b, t).astype(np.float64))
+    assert r_true <= (10 * rel if dtype == torch.float64 else 50 * rel)
+
+
+@pytest.mark.parametrize("kind", ["cg", "bicgstab"])
+def test_solver_loop_modes_agree(ctrl, kind):
+    rp, col, val = matgen.poisson2d(48)
+    n = len(rp) - 1
+    b = np.random.default_rng(5).uniform(-1, 1, n)
+    x0, i0, _ = run(ctrl, kind, rp, col, val, np.zeros(n), b, torch.float64, L.DIAGONAL, 3000, 1e-9, 0.0,
+                    loop_mode=0)
+    x1, i1, _ = run(ctrl, kind, rp, col, val, np.zeros(n), b, torch.float64, L.DIAGONAL, 3000, 1e-9, 0.0,
+                    loop_mode=1)
+    assert i0 == i1
+    assert np.array_equal(x0, x1)
+
+
+@pytest.mark.parametrize("kind", ["cg", "bicgstab"])
+def test_solver_max_iters_bookkeeping(ctrl, orc, kind):
+    rp, col, val = matgen.poisson2d(40)
+    n = len(rp) - 1
+    b = np.ones(n)
+    _, info, _ = run(ctrl, kind, rp, col, val, np.zeros(n), b, torch.float64, L.DIAGONAL, 7, 1e-30, 0.0)
+    _, oi = orc.solve(kind, np.float64, rp, col, val, np.zeros(n), b, 1, 7, 1e-30, 0.0)
+    assert info["nIters"] == oi.nIters
+    assert info["currentResidual"] == pytest.approx(oi.currentResidual, rel=1e-8)
+
+
+@pytest.mark.parametrize("kind", ["cg", "bicgstab"])
+def test_solver_zero_rhs_returns_b(ctrl, kind):
+    rp, col, val = matgen.poisson2d(16)
+    n = len(rp) - 1
+    A = api.CsrMatrix.from_numpy(rp, col, val)
+    x = torch.full((n,), 3.0, dtype=torch.float64, device="cuda")
+    b = torch.zeros(n, dtype=torch.float64, device="cuda")
+    sc = api.SolverControl(L.DIAGONAL, 100, 1e-6, 1e-8)
+    info = api.solve(kind, x, A, b, sc, ctrl)
+    assert info["nIters"] == 0
+    assert float(x.abs().sum()) == 0.0
+    sc.release()
+
+
+@pytest.mark.parametrize("kind", ["cg", "bicgstab"])
+def test_solver_exact_initial_guess(ctrl, kind):
+    rp, col, val = matgen.poisson2d(16)
+    n = len(rp) - 1
+    xs = np.random.default_rng(2).uniform(-1, 1, n)
+    import scipy.sparse as sp
+    b = sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64))) @ xs
+    x, info, _ = run(ctrl, kind, rp, col, val, xs, b, torch.float64, L.DIAGONAL, 100, 1e-8, 0.0)
+    assert info["nIters"] == 0
+    np.testing.assert_array_equal(x, xs)
+
+
+def test_cg_vector_path_without_meta(ctrl, orc):
+    rp, col, val = matgen.poisson2d(50)
+    n = len(rp) - 1
+    b = np.random.default_rng(3).uniform(-1, 1, n)
+    x, info, _ = run(ctrl, "cg", rp, col, val, np.zeros(n), b, torch.float64, L.DIAGONAL, 2000, 1e-10, 0.0,
+                     meta=False)
+    _, oi = orc.solve("cg", np.float64, rp, col, val, np.zeros(n), b, 1, 2000, 1e-10, 0.0)
+    assert abs(info["nIters"] - oi.nIters) <= 3
+
+
+def test_cg_repeat_uses_cached_graph_and_is_deterministic(ctrl):
+    rp, col, val = matgen.poisson2d(64)
+    n = len(rp) - 1
+    b = np.random.default_rng(4).uniform(-1, 1, n)
+    A = api.CsrMatrix.from_numpy(rp, col, val)
+    A.create_meta(ctrl)
+    bt = torch.tensor(b, device="cuda")
+    outs = []
+    for _ in range(3):
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        sc = api.SolverControl(L.DIAGONAL, 1000, 1e-10, 0.0)
+        api.solve("cg", x, A, bt, sc, ctrl)
+        sc.release()
+        outs.append(x.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[1], outs[2])
+
+
+def test_missing_diagonal_is_reported(ctrl):
+    rp, col, val = matgen.random_lengths([2, 2, 2], 3, seed=1)
+    # make row 1 lack its diagonal: columns of row 1 are sorted distinct from {0,1,2}
+    col = col.copy()
+    col[2:4] = [0, 2]
+    n = 3
+    _, _, status = run(ctrl, "cg", rp, col, np.abs(val) + 1, np.zeros(n), np.ones(n), torch.float64,
+                       L.DIAGONAL, 5, 1e-12, 0.0)
+    assert status & 1
+
+
+def test_solver_argument_errors(ctrl):
+    rp, col, val = matgen.poisson2d(8)
+    A = api.CsrMatrix.from_numpy(rp, col, val)
+    x = torch.zeros(63, dtype=torch.float64, device="cuda")
+    b = torch.zeros(64, dtype=torch.float64, device="cuda")
+    sc = api.SolverControl()
+    with pytest.raises(api.ClsparseError) as e:
+        api.solve("cg", x, A, b, sc, ctrl)
+    assert e.value.status == L.clsparseInvalidSystemSize
+    sc.release()

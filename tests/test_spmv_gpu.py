@@ -1,0 +1,187 @@
+"""Parity of clsparse{S,D}csrmv (through the C ABI) with the CPU oracle.
+
+The oracle is the reference test suite's host SpMV (src/tests/test-blas2.cpp:
+146-163 for FP32 with double accumulation, :231-252 for FP64 with compensated
+summation). Tolerances are the path's stated bars, relative to the row's
+absolute scale sum_j |alpha a_ij x_j| + |beta y_i| (robust to cancellation)
+and as a norm-wise relative error:
+    FP64: 1e-12        FP32: 1e-5
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from clsparse_b200 import api, matgen
+
+pytestmark = pytest.mark.gpu
+
+TOL = {torch.float64: 1e-12, torch.float32: 1e-5}
+NP = {torch.float64: np.float64, torch.float32: np.float32}
+
+
+def gpu_spmv(ctrl, rp, col, val, x, y0, alpha, beta, dtype, meta=True, ncols=None):
+    ncols = len(x) if ncols is None else ncols
+    A = api.CsrMatrix.from_numpy(rp, col, val, num_cols=ncols, dtype=dtype)
+    if meta:
+        A.create_meta(ctrl)
+    xt = torch.tensor(np.asarray(x), dtype=dtype, device="cuda")
+    yt = torch.tensor(np.asarray(y0), dtype=dtype, device="cuda")
+    at = torch.tensor([alpha], dtype=dtype, device="cuda")
+    bt = torch.tensor([beta], dtype=dtype, device="cuda")
+    api.csrmv(at, A, xt, bt, yt, ctrl)
+    return yt.cpu().numpy(), A
+
+
+def oracle_spmv(orc, rp, col, val, x, y0, alpha, beta, dtype):
+    if dtype == torch.float64:
+        return orc.dcsrmv(rp, col, val, alpha, x, beta, y0)
+    return orc.scsrmv(rp, col, np.asarray(val, np.float32), np.float32(alpha), np.asarray(x, np.float32),
+                      np.float32(beta), np.asarray(y0, np.float32)).astype(np.float64)
+
+
+def assert_parity(orc, rp, col, val, x, y0, alpha, beta, out, dtype):
+    t = NP[dtype]
+    valc = np.asarray(val, t).astype(np.float64)
+    xc = np.asarray(x, t).astype(np.float64)
+    yc = np.asarray(y0, t).astype(np.float64)
+    ref = oracle_spmv(orc, rp, col, val, x, y0, alpha, beta, dtype)
+    scale = orc.dcsrmv_absscale(rp, col, valc, float(t(alpha)), xc, float(t(beta)), yc)
+    err = np.abs(out.astype(np.float64) - ref)
+    tol = TOL[dtype]
+    tiny = np.finfo(t).tiny
+    bad = err > tol * scale + tiny
+    assert not bad.any(), f"{bad.sum()} rows off; worst {(err / (scale + tiny)).max():.3e}"
+    if np.linalg.norm(ref) > 0:
+        assert np.linalg.norm(err) <= tol * max(np.linalg.norm(ref), np.linalg.norm(scale) * 1e-3)
+
+
+def vecs(n_rows, n_cols, seed):
+    rng = np.random.default_rng(seed)
+    return rng.uniform(-1, 1, n_cols), rng.uniform(-1, 1, n_rows)
+
+
+EDGE_LENGTHS = {
+    "threshold_rows": [0, 1, 31, 32, 33, 127, 128, 129, 1023, 1024, 1025, 3072, 3073, 6145, 2, 0, 5],
+    "many_short": list(np.random.default_rng(1).integers(0, 6, 4000)),
+    "all_empty": [0] * 777,
+    "one_row": [17],
+    "one_long_row": [50_000],
+    "long_rows_between_short": [3] * 100 + [9000, 7000] + [2] * 500 + [20000] + [1] * 10,
+    "lognormal": list(np.maximum(1, np.rint(np.exp(np.random.default_rng(2).normal(2.5, 1.2, 5000))))
+                      .astype(int)),
+    "stream_runs": list(np.random.default_rng(3).integers(100, 300, 800)),
+}
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+@pytest.mark.parametrize("meta", [True, False], ids=["adaptive", "vector"])
+@pytest.mark.parametrize("case", sorted(EDGE_LENGTHS))
+def test_spmv_edge_matrices(ctrl, orc, dtype, meta, case):
+    lens = EDGE_LENGTHS[case]
+    ncols = max(60_000, 1)
+    rp, col, val = matgen.random_lengths(lens, ncols, seed=len(lens))
+    x, y0 = vecs(len(lens), ncols, 5)
+    for alpha, beta in ((1.0, 0.0), (2.5, -1.5), (-0.75, 1.0)):
+        out, _ = gpu_spmv(ctrl, rp, col, val, x, y0, alpha, beta, dtype, meta)
+        assert_parity(orc, rp, col, val, x, y0, alpha, beta, out, dtype)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+def test_spmv_extended_precision(ctrl, orc, dtype):
+    ctrl.enable_extended_precision(True)
+    rp, col, val = matgen.irregular(20_000, n_dense=5, dense_len=40_000, seed=9)
+    x, y0 = vecs(20_000, 20_000, 6)
+    out, _ = gpu_spmv(ctrl, rp, col, val, x, y0, 1.0, 0.5, dtype)
+    assert_parity(orc, rp, col, val, x, y0, 1.0, 0.5, out, dtype)
+
+
+def test_meta_words_equal_reference_binning(ctrl, orc):
+    rp, col, val = matgen.irregular(30_000, n_dense=7, dense_len=20_000, seed=4)
+    A = api.CsrMatrix.from_numpy(rp, col, val)
+    size = A.meta_size(ctrl)
+    A.create_meta(ctrl)
+    words, s, dry = orc.row_blocks(rp)
+    assert size == dry
+    assert A.meta_size(ctrl) == s
+    np.testing.assert_array_equal(A.row_blocks(), words)
+    if orc.ref_lib() is not None:
+        np.testing.assert_array_equal(A.row_blocks(), orc.ref_row_blocks(rp)[0])
+
+
+def test_spmv_beta_zero_does_not_read_y(ctrl):
+    rp, col, val = matgen.random_lengths([3, 0, 5000, 40, 12000, 1], 20_000, seed=2)
+    for meta in (True, False):
+        y0 = np.full(6, np.nan)
+        out, _ = gpu_spmv(ctrl, rp, col, val, np.ones(20_000), y0, 1.0, 0.0, torch.float64, meta)
+        assert np.all(np.isfinite(out))
+
+
+def test_spmv_offsets_and_rectangular(ctrl, orc):
+    rng = np.random.default_rng(8)
+    rp, col, val = matgen.random_lengths(rng.integers(0, 50, 3000), 777, seed=8)
+    x, y0 = vecs(3000, 777, 9)
+    A = api.CsrMatrix.from_numpy(rp, col, val, num_cols=777)
+    A.create_meta(ctrl)
+    xt = torch.zeros(777 + 13, dtype=torch.float64, device="cuda")
+    xt[13:] = torch.tensor(x, device="cuda")
+    yt = torch.zeros(3000 + 5, dtype=torch.float64, device="cuda")
+    yt[5:] = torch.tensor(y0, device="cuda")
+    one = torch.tensor([0.0, 1.0], dtype=torch.float64, device="cuda")
+    A_vec = api.vector
+    from clsparse_b200 import _lib as L
+    import ctypes as C
+    al = L.clsparseScalar(C.c_void_p(one.data_ptr()), 1)
+    be = L.clsparseScalar(C.c_void_p(one.data_ptr()), 1)
+    st = L.load().clsparseDcsrmv(C.byref(al), C.byref(A.s), C.byref(A_vec(xt, 13)), C.byref(be),
+                                 C.byref(A_vec(yt, 5)), ctrl.handle)
+    assert st == 0
+    assert_parity(orc, rp, col, val, x, y0, 1.0, 1.0, yt[5:].cpu().numpy(), torch.float64)
+    assert float(yt[:5].abs().sum()) == 0.0
+
+
+def test_spmv_deterministic(ctrl):
+    rp, col, val = matgen.irregular(50_000, n_dense=10, dense_len=60_000, seed=12)
+    x, y0 = vecs(50_000, 50_000, 1)
+    a, _ = gpu_spmv(ctrl, rp, col, val, x, y0, 1.0, 1.0, torch.float64)
+    b, _ = gpu_spmv(ctrl, rp, col, val, x, y0, 1.0, 1.0, torch.float64)
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def test_spmv_size_errors(ctrl):
+    rp, col, val = matgen.random_lengths([1, 2], 4, seed=0)
+    A = api.CsrMatrix.from_numpy(rp, col, val, num_cols=4)
+    x = torch.zeros(3, dtype=torch.float64, device="cuda")
+    y = torch.zeros(2, dtype=torch.float64, device="cuda")
+    s = torch.ones(1, dtype=torch.float64, device="cuda")
+    with pytest.raises(api.ClsparseError) as e:
+        api.csrmv(s, A, x, s, y, ctrl)
+    assert e.value.status == -1021  # clsparseInvalidSize
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+def test_spmv_irregular_full_size(ctrl, orc, dtype):
+    """The 2M-row irregular workload (log-normal rows + 50 rows of 200k), full
+    parity against the oracle plus linearity A(x1+x2) = Ax1 + Ax2."""
+    rp, col, val = matgen.irregular(2_000_000, seed=7)
+    x, y0 = vecs(2_000_000, 2_000_000, 3)
+    out, A = gpu_spmv(ctrl, rp, col, val, x, y0, 1.0, 0.0, dtype)
+    assert_parity(orc, rp, col, val, x, y0, 1.0, 0.0, out, dtype)
+    x2 = np.random.default_rng(4).uniform(-1, 1, 2_000_000)
+    t = NP[dtype]
+    xa = torch.tensor(np.asarray(x, t), device="cuda")
+    xb = torch.tensor(np.asarray(x2, t), device="cuda")
+    one = torch.ones(1, dtype=dtype, device="cuda")
+    zero = torch.zeros(1, dtype=dtype, device="cuda")
+    ya = torch.zeros(2_000_000, dtype=dtype, device="cuda")
+    yb = torch.zeros_like(ya)
+    yab = torch.zeros_like(ya)
+    api.csrmv(one, A, xa, zero, ya, ctrl)
+    api.csrmv(one, A, xb, zero, yb, ctrl)
+    api.csrmv(one, A, xa + xb, zero, yab, ctrl)
+    lin = (yab - ya - yb).abs().double().cpu().numpy()
+    valc = np.asarray(val, t).astype(np.float64)
+    s1 = orc.dcsrmv_absscale(rp, col, valc, 1.0, np.asarray(x, t).astype(np.float64), 0.0, y0)
+    s2 = orc.dcsrmv_absscale(rp, col, valc, 1.0, np.asarray(x2, t).astype(np.float64), 0.0, y0)
+    assert np.all(lin <= 4 * TOL[dtype] * (s1 + s2) + np.finfo(t).tiny)
