@@ -70,10 +70,13 @@ struct matrix_meta {
     size_t num_words = 0;               // row-block words; CTAs of one SpMV = num_words - 1
     cl_ulong* d_rowBlocks = nullptr;    // device copy of the words
     std::vector<cl_ulong> h_rowBlocks;  // host copy (for inspection)
+    uint32_t* d_word_nnz = nullptr;     // row_pointer[first row of word w], one per word
     double* d_lr_partial = nullptr;     // one partial sum per row-block word (long rows)
     uint32_t* d_lr_ticket = nullptr;    // one arrival counter per row-block word (long rows)
     clsparseIdx_t num_rows = 0;
     clsparseIdx_t num_nonzeros = 0;
+    uint32_t nnz_lo = 0;                // row_pointer[0]
+    uint32_t nnz_hi = 0;                // row_pointer[num_rows]
     int device = 0;
     ~matrix_meta();
 };

@@ -167,6 +167,7 @@ matrix_meta::~matrix_meta() {
     cudaGetDevice(&prev);
     if (prev != device) cudaSetDevice(device);
     if (d_rowBlocks) cudaFree(d_rowBlocks);
+    if (d_word_nnz) cudaFree(d_word_nnz);
     if (d_lr_partial) cudaFree(d_lr_partial);
     if (d_lr_ticket) cudaFree(d_lr_ticket);
     if (prev >= 0 && prev != device) cudaSetDevice(prev);
@@ -230,7 +231,14 @@ clsparseStatus clsparseCsrMetaCreate(clsparseCsrMatrix* csrMatx, clsparseControl
     meta->h_rowBlocks.resize(meta->num_words);
 
     const size_t w = meta->num_words;
+    // Nonzero offset of every word's first row, so a CTA finds its range
+    // without a dependent row-pointer load.
+    std::vector<uint32_t> word_nnz(w);
+    for (size_t k = 0; k < w; ++k) word_nnz[k] = rp[static_cast<size_t>(meta->h_rowBlocks[k] >> 32)];
+    meta->nnz_lo = rp.front();
+    meta->nnz_hi = rp.back();
     if (cudaMalloc(&meta->d_rowBlocks, w * sizeof(cl_ulong)) != cudaSuccess ||
+        cudaMalloc(&meta->d_word_nnz, w * sizeof(uint32_t)) != cudaSuccess ||
         cudaMalloc(&meta->d_lr_partial, w * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&meta->d_lr_ticket, w * sizeof(uint32_t)) != cudaSuccess) {
         cudaGetLastError();
@@ -238,6 +246,9 @@ clsparseStatus clsparseCsrMetaCreate(clsparseCsrMatrix* csrMatx, clsparseControl
     }
     cudaError_t e = cudaMemcpyAsync(meta->d_rowBlocks, meta->h_rowBlocks.data(),
                                     w * sizeof(cl_ulong), cudaMemcpyHostToDevice, control->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(meta->d_word_nnz, word_nnz.data(), w * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, control->stream);
     if (e == cudaSuccess)
         e = cudaMemsetAsync(meta->d_lr_ticket, 0, w * sizeof(uint32_t), control->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(control->stream);

@@ -29,6 +29,7 @@
 // Both kernels can fuse the dot products a Krylov solver takes of the result
 // (<y, w> and <y, y>) and finish them with a deterministic grid reduction.
 #include <algorithm>
+#include <cstdlib>
 #include <type_traits>
 
 #include "device_common.cuh"
@@ -100,15 +101,115 @@ __device__ __forceinline__ void run_epilogue(RowSink<T, K>& sink, const EpiDev<T
     }
 }
 
-template <typename T, bool EXT, int K>
-__global__ void __launch_bounds__(kThreads)
+// Four consecutive nonzeros [e0, e0+4) of the CSR arrays; `mask` marks the
+// ones inside the block [nb, ne) being processed (the others are not used).
+template <typename T>
+struct Quad {
+    uint32_t c[4];
+    T v[4];
+    uint32_t mask;
+};
+
+// Loads one quad. When the quad lies inside the matrix's nonzero range
+// [lo, hi) and the arrays are 16-byte aligned, the column indices come in one
+// 16-byte load and the values in one (FP32) or two (FP64) 16-byte loads;
+// otherwise element by element. Nothing outside [lo, hi) is ever read.
+template <typename T>
+__device__ __forceinline__ void load_quad(const T* __restrict__ vals, const uint32_t* __restrict__ cols,
+                                          uint32_t e0, uint32_t nb, uint32_t ne, uint32_t lo,
+                                          uint32_t hi, bool vec, Quad<T>& q) {
+    q.mask = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (e0 + k >= nb && e0 + k < ne) q.mask |= 1u << k;
+    if (vec && e0 >= lo && e0 + 4 <= hi) {
+        const uint4 ci = dev::ld_stream(reinterpret_cast<const uint4*>(cols + e0));
+        q.c[0] = ci.x;
+        q.c[1] = ci.y;
+        q.c[2] = ci.z;
+        q.c[3] = ci.w;
+        if constexpr (sizeof(T) == 8) {
+            const double2 a = dev::ld_stream(reinterpret_cast<const double2*>(vals + e0));
+            const double2 b = dev::ld_stream(reinterpret_cast<const double2*>(vals + e0 + 2));
+            q.v[0] = a.x;
+            q.v[1] = a.y;
+            q.v[2] = b.x;
+            q.v[3] = b.y;
+        } else {
+            const float4 a = dev::ld_stream(reinterpret_cast<const float4*>(vals + e0));
+            q.v[0] = a.x;
+            q.v[1] = a.y;
+            q.v[2] = a.z;
+            q.v[3] = a.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (q.mask & (1u << k)) {
+                q.c[k] = dev::ld_stream(cols + e0 + k);
+                q.v[k] = dev::ld_stream(vals + e0 + k);
+            } else {
+                q.c[k] = 0;
+                q.v[k] = T(0);
+            }
+        }
+    }
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void gather_quads(const T* __restrict__ x, const Quad<T> (&q)[N], T (&xv)[N][4]) {
+#pragma unroll
+    for (int j = 0; j < N; ++j)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) xv[j][k] = (q[j].mask & (1u << k)) ? dev::ld_ro(x + q[j].c[k]) : T(0);
+}
+
+// Sum of alpha*a_j*x[col_j] over [cb, ce) by the whole CTA (VECTOR rows and
+// LONG chunks). Each round a thread has two quads (8 nonzeros) in flight
+// before it gathers x.
+template <typename T, bool EXT, int NT>
+__device__ __forceinline__ dev::Acc<T, EXT> range_sum(const T* __restrict__ vals,
+                                                      const uint32_t* __restrict__ cols,
+                                                      const T* __restrict__ x, T alpha, uint32_t cb,
+                                                      uint32_t ce, uint32_t lo, uint32_t hi, bool vec) {
+    dev::Acc<T, EXT> a;
+    const uint32_t base = cb & ~3u;
+    const uint32_t nq = (ce - base + 3) >> 2;
+    constexpr int U = 2;
+    for (uint32_t g0 = threadIdx.x; g0 < nq; g0 += U * NT) {
+        Quad<T> q[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t g = g0 + u * NT;
+            if (g < nq)
+                load_quad(vals, cols, base + 4 * g, cb, ce, lo, hi, vec, q[u]);
+            else
+                q[u].mask = 0;
+        }
+        T xv[U][4];
+        gather_quads(x, q, xv);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (q[u].mask & (1u << k)) a.add_prod(alpha * q[u].v[k], xv[u][k]);
+    }
+    return a;
+}
+
+constexpr uint32_t kRpStage = kBlkSize + 1;  // row pointers of a STREAM block kept in shared memory
+
+template <typename T, bool EXT, int K, int NT>
+__global__ void __launch_bounds__(NT)
     csr_adaptive_kernel(const T* __restrict__ vals, const uint32_t* __restrict__ cols,
                         const uint32_t* __restrict__ rp, const T* __restrict__ x, T* __restrict__ y,
                         const T* __restrict__ alpha_p, const T* __restrict__ beta_p,
-                        const uint64_t* __restrict__ words, uint32_t nblocks,
+                        const uint64_t* __restrict__ words, const uint32_t* __restrict__ word_nnz,
+                        uint32_t nblocks, uint32_t lo, uint32_t hi, int vec,
                         double* __restrict__ lr_partial, uint32_t* __restrict__ lr_ticket,
                         EpiDev<T> epi) {
     __shared__ T stage[kBlkSize];
+    __shared__ uint32_t srp[kRpStage];
     __shared__ T red_s[32];
     __shared__ T red_c[32];
     __shared__ bool lr_last;
@@ -121,44 +222,78 @@ __global__ void __launch_bounds__(kThreads)
 
     const uint32_t gid = blockIdx.x;
     if (gid < nblocks) {
+        // Independent loads: the block's words and the nonzero offsets of
+        // their first rows (no dependent row-pointer load).
         const uint64_t w0 = words[gid];
         const uint64_t w1 = words[gid + 1];
+        const uint32_t nb = word_nnz[gid];
+        const uint32_t ne = word_nnz[gid + 1];
         const uint32_t row = static_cast<uint32_t>(w0 >> 32);
         const uint32_t stop = static_cast<uint32_t>(w1 >> 32);
         const uint32_t low = static_cast<uint32_t>(w0 & ((1u << kWgBits) - 1u));
         const uint32_t nrows = stop - row;
-        const int tid = threadIdx.x;
+        const uint32_t tid = threadIdx.x;
 
         if (nrows > kRowsForVector) {
             // ---- STREAM: several short rows, <= kBlkSize nonzeros in total ----
-            const uint32_t nb = dev::ld_ro(rp + row);
-            const uint32_t cnt = dev::ld_ro(rp + stop) - nb;
+            const uint32_t cnt = ne - nb;
             // A block from clsparseCsrMetaCreate never exceeds the staging
             // buffer; if the row pointers changed after the meta was made, the
             // rows are summed straight from global memory instead.
             const bool staged = cnt <= kBlkSize;
+            const bool rp_staged = nrows < kRpStage;
             if (staged) {
-                for (uint32_t i = tid; i < cnt; i += kThreads) {
-                    const uint32_t c = dev::ld_stream(cols + nb + i);
-                    const T v = dev::ld_stream(vals + nb + i);
-                    stage[i] = dev::mul_rn(alpha * v, dev::ld_ro(x + c));
+                constexpr int QPT = static_cast<int>(kBlkSize) / 4 / NT;
+                const uint32_t base = nb & ~3u;
+                const uint32_t nq = (ne - base + 3) >> 2;  // <= kBlkSize/4 + 1
+                Quad<T> q[QPT];
+#pragma unroll
+                for (int j = 0; j < QPT; ++j) {
+                    const uint32_t g = tid + j * NT;
+                    if (g < nq)
+                        load_quad(vals, cols, base + 4 * g, nb, ne, lo, hi, vec != 0, q[j]);
+                    else
+                        q[j].mask = 0;
                 }
+                if (rp_staged)
+                    for (uint32_t i = tid; i <= nrows; i += NT) srp[i] = dev::ld_ro(rp + row + i);
+                T xv[QPT][4];
+                gather_quads(x, q, xv);
+#pragma unroll
+                for (int j = 0; j < QPT; ++j) {
+                    const uint32_t e0 = base + 4 * (tid + j * NT);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (q[j].mask & (1u << k)) stage[e0 + k - nb] = dev::mul_rn(alpha * q[j].v[k], xv[j][k]);
+                }
+                // the quad past QPT*NT, present when the block starts unaligned
+                for (uint32_t g = QPT * NT + tid; g < nq; g += NT) {
+                    Quad<T> r[1];
+                    load_quad(vals, cols, base + 4 * g, nb, ne, lo, hi, vec != 0, r[0]);
+                    T rv[1][4];
+                    gather_quads(x, r, rv);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (r[0].mask & (1u << k)) stage[base + 4 * g + k - nb] = dev::mul_rn(alpha * r[0].v[k], rv[0][k]);
+                }
+            } else if (rp_staged) {
+                for (uint32_t i = tid; i <= nrows; i += NT) srp[i] = dev::ld_ro(rp + row + i);
             }
             __syncthreads();
             // Lanes per row: the reference's per-block reduction width, capped at
             // one warp so each row reduces with shuffles inside a warp.
-            uint32_t g = low == 0 ? 1u : (low > 32u ? 32u : low);
-            auto reduce_rows = [&](auto gw) {
-                constexpr int G = decltype(gw)::value;
-                const uint32_t groups = kThreads / G;
+            const uint32_t gw = low == 0 ? 1u : (low > 32u ? 32u : low);
+            auto reduce_rows = [&](auto gc) {
+                constexpr int G = decltype(gc)::value;
+                const uint32_t groups = NT / G;
                 const uint32_t grp = tid / G;
                 const uint32_t lane = tid & (G - 1);
-                for (uint32_t base = 0; base < nrows; base += groups) {
-                    const uint32_t r = base + grp;
+                for (uint32_t rb = 0; rb < nrows; rb += groups) {
+                    const uint32_t r = rb + grp;
                     dev::Acc<T, EXT> a;
                     if (r < nrows) {
-                        const uint32_t f = dev::ld_ro(rp + row + r) - nb;
-                        const uint32_t l = dev::ld_ro(rp + row + r + 1) - nb;
+                        const uint32_t f = (rp_staged ? srp[r] : dev::ld_ro(rp + row + r)) - nb;
+                        const uint32_t l = (rp_staged ? srp[r + 1] : dev::ld_ro(rp + row + r + 1)) - nb;
                         if (staged) {
                             for (uint32_t j = f + lane; j < l; j += G) a.add(stage[j]);
                         } else {
@@ -170,7 +305,7 @@ __global__ void __launch_bounds__(kThreads)
                     if (r < nrows && lane == 0) sink.template put<EXT>(row + r, a);
                 }
             };
-            switch (g) {
+            switch (gw) {
                 case 1: reduce_rows(std::integral_constant<int, 1>{}); break;
                 case 2: reduce_rows(std::integral_constant<int, 2>{}); break;
                 case 4: reduce_rows(std::integral_constant<int, 4>{}); break;
@@ -180,28 +315,19 @@ __global__ void __launch_bounds__(kThreads)
             }
         } else if (nrows == 1 && low == 0) {
             // ---- VECTOR: one row, the whole CTA ----
-            const uint32_t nb = dev::ld_ro(rp + row);
-            const uint32_t ne = dev::ld_ro(rp + row + 1);
-            dev::Acc<T, EXT> a;
-#pragma unroll 4
-            for (uint32_t j = nb + tid; j < ne; j += kThreads)
-                a.add_prod(alpha * dev::ld_stream(vals + j), dev::ld_ro(x + dev::ld_stream(cols + j)));
+            dev::Acc<T, EXT> a = range_sum<T, EXT, NT>(vals, cols, x, alpha, nb, ne, lo, hi, vec != 0);
             a = dev::block_reduce_acc(a, red_s, red_c);
             if (tid == 0) sink.template put<EXT>(row, a);
         } else {
             // ---- LONG: chunk `low` of a row split over several CTAs ----
-            const uint32_t nb = dev::ld_ro(rp + row);
-            const uint32_t ne = dev::ld_ro(rp + row + 1);
-            const uint32_t len = ne - nb;
+            const uint32_t re = dev::ld_ro(rp + row + 1);
+            const uint32_t len = re - nb;
             const uint32_t nchunks = (len + kLongChunk - 1) / kLongChunk;
             if (nchunks >= 2 && low < nchunks) {
                 const uint32_t first = gid - low;
                 const uint32_t cb = nb + low * kLongChunk;
-                const uint32_t ce = min(ne, cb + kLongChunk);
-                dev::Acc<T, EXT> a;
-#pragma unroll 4
-                for (uint32_t j = cb + tid; j < ce; j += kThreads)
-                    a.add_prod(alpha * dev::ld_stream(vals + j), dev::ld_ro(x + dev::ld_stream(cols + j)));
+                const uint32_t ce = min(re, cb + kLongChunk);
+                dev::Acc<T, EXT> a = range_sum<T, EXT, NT>(vals, cols, x, alpha, cb, ce, lo, hi, vec != 0);
                 a = dev::block_reduce_acc(a, red_s, red_c);
                 if (tid == 0) {
                     // partial of this chunk; compensation folded in
@@ -308,6 +434,17 @@ cudaError_t launch_vector(const CsrView<T>& A, const T* alpha, const T* beta, co
     return cudaGetLastError();
 }
 
+// Threads per CTA of the adaptive kernel (128 or 256); CLSPARSE_B200_SPMV_NT
+// overrides the default for tuning.
+int adaptive_threads() {
+    static int nt = [] {
+        const char* e = std::getenv("CLSPARSE_B200_SPMV_NT");
+        const int v = e ? std::atoi(e) : 128;
+        return v == 256 ? 256 : 128;
+    }();
+    return nt;
+}
+
 template <typename T, bool EXT, int K>
 cudaError_t launch_kind(const CsrView<T>& A, const T* alpha, const T* beta, const T* x, T* y,
                         const EpiDev<T>& e, cudaStream_t s) {
@@ -318,9 +455,16 @@ cudaError_t launch_kind(const CsrView<T>& A, const T* alpha, const T* beta, cons
         if (K == 0) return cudaSuccess;
         grid = 1;  // one idle CTA still finishes the fused reduction
     }
-    csr_adaptive_kernel<T, EXT, K><<<grid, kThreads, 0, s>>>(
-        A.vals, A.cols, A.rp, x, y, alpha, beta, A.meta->d_rowBlocks, nblocks,
-        A.meta->d_lr_partial, A.meta->d_lr_ticket, e);
+    const int vec = ((reinterpret_cast<uintptr_t>(A.vals) | reinterpret_cast<uintptr_t>(A.cols)) & 15u) == 0;
+    const matrix_meta* m = A.meta;
+    if (adaptive_threads() == 256)
+        csr_adaptive_kernel<T, EXT, K, 256><<<grid, 256, 0, s>>>(
+            A.vals, A.cols, A.rp, x, y, alpha, beta, m->d_rowBlocks, m->d_word_nnz, nblocks, m->nnz_lo,
+            m->nnz_hi, vec, m->d_lr_partial, m->d_lr_ticket, e);
+    else
+        csr_adaptive_kernel<T, EXT, K, 128><<<grid, 128, 0, s>>>(
+            A.vals, A.cols, A.rp, x, y, alpha, beta, m->d_rowBlocks, m->d_word_nnz, nblocks, m->nnz_lo,
+            m->nnz_hi, vec, m->d_lr_partial, m->d_lr_ticket, e);
     return cudaGetLastError();
 }
 

@@ -119,6 +119,8 @@ def irregular(n: int, mu: float = 2.5, sigma: float = 1.2, n_dense: int = 50,
     nnz = int(rp[-1])
     if nnz >= 2 ** 32:
         raise ValueError("nnz exceeds 32-bit indices")
+    if int(lens.max(initial=0)) * 2 > ncols:
+        raise ValueError("rows longer than half the columns: use random_lengths")
     row_of = np.repeat(np.arange(n, dtype=np.int64), lens)
     cols = rng.integers(0, ncols, size=nnz, dtype=np.int64)
     # draw again wherever a row repeats a column, until every row is distinct

@@ -91,7 +91,7 @@ def test_spmv_edge_matrices(ctrl, orc, dtype, meta, case):
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
 def test_spmv_extended_precision(ctrl, orc, dtype):
     ctrl.enable_extended_precision(True)
-    rp, col, val = matgen.irregular(20_000, n_dense=5, dense_len=40_000, seed=9)
+    rp, col, val = matgen.irregular(20_000, n_dense=5, dense_len=9_000, seed=9)
     x, y0 = vecs(20_000, 20_000, 6)
     out, _ = gpu_spmv(ctrl, rp, col, val, x, y0, 1.0, 0.5, dtype)
     assert_parity(orc, rp, col, val, x, y0, 1.0, 0.5, out, dtype)
@@ -142,7 +142,7 @@ def test_spmv_offsets_and_rectangular(ctrl, orc):
 
 
 def test_spmv_deterministic(ctrl):
-    rp, col, val = matgen.irregular(50_000, n_dense=10, dense_len=60_000, seed=12)
+    rp, col, val = matgen.irregular(50_000, n_dense=10, dense_len=20_000, seed=12)
     x, y0 = vecs(50_000, 50_000, 1)
     a, _ = gpu_spmv(ctrl, rp, col, val, x, y0, 1.0, 1.0, torch.float64)
     b, _ = gpu_spmv(ctrl, rp, col, val, x, y0, 1.0, 1.0, torch.float64)
