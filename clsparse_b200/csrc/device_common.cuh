@@ -4,8 +4,11 @@
 // reduction without a second kernel and without any spin-wait.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <type_traits>
 
 namespace clsp {
 namespace dev {
@@ -21,6 +24,27 @@ __device__ __forceinline__ T ld_stream(const T* p) {
 template <typename T>
 __device__ __forceinline__ T ld_ro(const T* p) {
     return __ldg(p);
+}
+
+// Loads one matrix value (double, float or bf16) as the arithmetic type T.
+template <typename T, typename V>
+__device__ __forceinline__ T ld_val(const V* p) {
+    if constexpr (std::is_same_v<V, __nv_bfloat16>) {
+        const unsigned short u = __ldcs(reinterpret_cast<const unsigned short*>(p));
+        return static_cast<T>(__uint_as_float(static_cast<unsigned>(u) << 16));
+    } else {
+        return static_cast<T>(__ldcs(p));
+    }
+}
+
+// Converts a matrix value held in registers or shared memory to T.
+template <typename T, typename V>
+__device__ __forceinline__ T to_t(V v) {
+    if constexpr (std::is_same_v<V, __nv_bfloat16>) {
+        return static_cast<T>(__bfloat162float(v));
+    } else {
+        return static_cast<T>(v);
+    }
 }
 
 // Knuth's TwoSum: returns fl(a+b) and adds the exact rounding error to err.

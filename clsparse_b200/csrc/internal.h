@@ -3,6 +3,7 @@
 // uses. Host C++17; included by the .cpp and .cu translation units.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -73,6 +74,7 @@ struct matrix_meta {
     uint32_t* d_word_nnz = nullptr;     // row_pointer[first row of word w], one per word
     double* d_lr_partial = nullptr;     // one partial sum per row-block word (long rows)
     uint32_t* d_lr_ticket = nullptr;    // one arrival counter per row-block word (long rows)
+    int* d_error = nullptr;             // set by an SpMV whose bounded barrier wait timed out
     clsparseIdx_t num_rows = 0;
     clsparseIdx_t num_nonzeros = 0;
     uint32_t nnz_lo = 0;                // row_pointer[0]
@@ -156,8 +158,10 @@ struct CsrView {
 // Number of CTAs an SpMV of this matrix launches (sizes epilogue partials).
 uint32_t spmv_num_ctas(const matrix_meta* meta, uint32_t nrows, uint32_t nnz);
 
-template <typename T>
-cudaError_t launch_csrmv(const CsrView<T>& A, const T* alpha, const T* beta, const T* x, T* y,
+// y = alpha*A*x + beta*y with matrix values of type V (double, float or
+// bf16) and vectors / arithmetic in T.
+template <typename V, typename T>
+cudaError_t launch_csrmv(const CsrView<V>& A, const T* alpha, const T* beta, const T* x, T* y,
                          bool extended, const SpmvEpilogue& epi, cudaStream_t s);
 
 // Host binning (meta.cpp).

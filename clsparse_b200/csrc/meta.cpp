@@ -170,6 +170,7 @@ matrix_meta::~matrix_meta() {
     if (d_word_nnz) cudaFree(d_word_nnz);
     if (d_lr_partial) cudaFree(d_lr_partial);
     if (d_lr_ticket) cudaFree(d_lr_ticket);
+    if (d_error) cudaFree(d_error);
     if (prev >= 0 && prev != device) cudaSetDevice(prev);
 }
 
@@ -240,7 +241,8 @@ clsparseStatus clsparseCsrMetaCreate(clsparseCsrMatrix* csrMatx, clsparseControl
     if (cudaMalloc(&meta->d_rowBlocks, w * sizeof(cl_ulong)) != cudaSuccess ||
         cudaMalloc(&meta->d_word_nnz, w * sizeof(uint32_t)) != cudaSuccess ||
         cudaMalloc(&meta->d_lr_partial, w * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&meta->d_lr_ticket, w * sizeof(uint32_t)) != cudaSuccess) {
+        cudaMalloc(&meta->d_lr_ticket, w * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&meta->d_error, sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         return clsparseOutOfResources;
     }
@@ -251,6 +253,7 @@ clsparseStatus clsparseCsrMetaCreate(clsparseCsrMatrix* csrMatx, clsparseControl
                             cudaMemcpyHostToDevice, control->stream);
     if (e == cudaSuccess)
         e = cudaMemsetAsync(meta->d_lr_ticket, 0, w * sizeof(uint32_t), control->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(meta->d_error, 0, sizeof(int), control->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(control->stream);
     if (e != cudaSuccess) return clsparseInvalidKernelExecution;
     csrMatx->meta = meta.release();

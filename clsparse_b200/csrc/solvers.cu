@@ -608,7 +608,7 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
             extract_inv_diag_kernel<T><<<vg, kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
                                                                invD, st);
         SpmvEpilogue none;
-        launch_csrmv<T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
+        launch_csrmv<T, T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
         cg_init_kernel<T><<<vg, kThreads, 0, s>>>(aa);
     };
     auto body = [&](cudaStream_t s, unsigned long long h) {
@@ -622,7 +622,7 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
         epi.op = EpiOp::CgAlpha;
         epi.state = st;
         epi.done = &st->done;
-        launch_csrmv<T>(Av, &st->one, &st->zero, aa.p, aa.y, ext, epi, s);
+        launch_csrmv<T, T>(Av, &st->one, &st->zero, aa.p, aa.y, ext, epi, s);
         cg_update_kernel<T><<<vg, kThreads, 0, s>>>(aa);
         cg_p_kernel<T><<<vg, kThreads, 0, s>>>(aa);
     };
@@ -699,7 +699,7 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
             extract_inv_diag_kernel<T><<<vg, kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
                                                                invD, st);
         SpmvEpilogue none;
-        launch_csrmv<T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
+        launch_csrmv<T, T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
         bicg_init_kernel<T><<<vg, kThreads, 0, s>>>(aa);
     };
     auto body = [&](cudaStream_t s, unsigned long long h) {
@@ -713,7 +713,7 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
         e1.op = EpiOp::BicgAlpha;
         e1.state = st;
         e1.done = &st->done;
-        launch_csrmv<T>(Av, &st->one, &st->zero, aa.Mp, aa.AMp, ext, e1, s);
+        launch_csrmv<T, T>(Av, &st->one, &st->zero, aa.Mp, aa.AMp, ext, e1, s);
         bicg_s_kernel<T><<<vg, kThreads, 0, s>>>(aa);
         SpmvEpilogue e2;
         e2.ndots = 2;
@@ -724,7 +724,7 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
         e2.op = EpiOp::BicgOmega;
         e2.state = st;
         e2.done = &st->done;
-        launch_csrmv<T>(Av, &st->one, &st->zero, aa.Ms, aa.AMs, ext, e2, s);
+        launch_csrmv<T, T>(Av, &st->one, &st->zero, aa.Ms, aa.AMs, ext, e2, s);
         bicg_x_kernel<T><<<vg, kThreads, 0, s>>>(aa);
         bicg_p_kernel<T><<<vg, kThreads, 0, s>>>(aa);
     };

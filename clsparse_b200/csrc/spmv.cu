@@ -30,10 +30,12 @@
 // (<y, w> and <y, y>) and finish them with a deterministic grid reduction.
 #include <algorithm>
 #include <cstdlib>
+#include <string>
 #include <type_traits>
 
 #include "device_common.cuh"
 #include "internal.h"
+#include "pipeline.cuh"
 #include "solver_state.cuh"
 
 namespace clsp {
@@ -114,8 +116,8 @@ struct Quad {
 // [lo, hi) and the arrays are 16-byte aligned, the column indices come in one
 // 16-byte load and the values in one (FP32) or two (FP64) 16-byte loads;
 // otherwise element by element. Nothing outside [lo, hi) is ever read.
-template <typename T>
-__device__ __forceinline__ void load_quad(const T* __restrict__ vals, const uint32_t* __restrict__ cols,
+template <typename V, typename T>
+__device__ __forceinline__ void load_quad(const V* __restrict__ vals, const uint32_t* __restrict__ cols,
                                           uint32_t e0, uint32_t nb, uint32_t ne, uint32_t lo,
                                           uint32_t hi, bool vec, Quad<T>& q) {
     q.mask = 0;
@@ -128,7 +130,13 @@ __device__ __forceinline__ void load_quad(const T* __restrict__ vals, const uint
         q.c[1] = ci.y;
         q.c[2] = ci.z;
         q.c[3] = ci.w;
-        if constexpr (sizeof(T) == 8) {
+        if constexpr (std::is_same_v<V, __nv_bfloat16>) {
+            const uint2 a = dev::ld_stream(reinterpret_cast<const uint2*>(vals + e0));
+            q.v[0] = static_cast<T>(__uint_as_float(a.x << 16));
+            q.v[1] = static_cast<T>(__uint_as_float(a.x & 0xffff0000u));
+            q.v[2] = static_cast<T>(__uint_as_float(a.y << 16));
+            q.v[3] = static_cast<T>(__uint_as_float(a.y & 0xffff0000u));
+        } else if constexpr (sizeof(V) == 8) {
             const double2 a = dev::ld_stream(reinterpret_cast<const double2*>(vals + e0));
             const double2 b = dev::ld_stream(reinterpret_cast<const double2*>(vals + e0 + 2));
             q.v[0] = a.x;
@@ -147,7 +155,7 @@ __device__ __forceinline__ void load_quad(const T* __restrict__ vals, const uint
         for (int k = 0; k < 4; ++k) {
             if (q.mask & (1u << k)) {
                 q.c[k] = dev::ld_stream(cols + e0 + k);
-                q.v[k] = dev::ld_stream(vals + e0 + k);
+                q.v[k] = dev::ld_val<T>(vals + e0 + k);
             } else {
                 q.c[k] = 0;
                 q.v[k] = T(0);
@@ -167,8 +175,8 @@ __device__ __forceinline__ void gather_quads(const T* __restrict__ x, const Quad
 // Sum of alpha*a_j*x[col_j] over [cb, ce) by the whole CTA (VECTOR rows and
 // LONG chunks). Each round a thread has two quads (8 nonzeros) in flight
 // before it gathers x.
-template <typename T, bool EXT, int NT>
-__device__ __forceinline__ dev::Acc<T, EXT> range_sum(const T* __restrict__ vals,
+template <typename V, typename T, bool EXT, int NT>
+__device__ __forceinline__ dev::Acc<T, EXT> range_sum(const V* __restrict__ vals,
                                                       const uint32_t* __restrict__ cols,
                                                       const T* __restrict__ x, T alpha, uint32_t cb,
                                                       uint32_t ce, uint32_t lo, uint32_t hi, bool vec) {
@@ -199,9 +207,9 @@ __device__ __forceinline__ dev::Acc<T, EXT> range_sum(const T* __restrict__ vals
 
 constexpr uint32_t kRpStage = kBlkSize + 1;  // row pointers of a STREAM block kept in shared memory
 
-template <typename T, bool EXT, int K, int NT>
+template <typename V, typename T, bool EXT, int K, int NT>
 __global__ void __launch_bounds__(NT)
-    csr_adaptive_kernel(const T* __restrict__ vals, const uint32_t* __restrict__ cols,
+    csr_adaptive_kernel(const V* __restrict__ vals, const uint32_t* __restrict__ cols,
                         const uint32_t* __restrict__ rp, const T* __restrict__ x, T* __restrict__ y,
                         const T* __restrict__ alpha_p, const T* __restrict__ beta_p,
                         const uint64_t* __restrict__ words, const uint32_t* __restrict__ word_nnz,
@@ -298,7 +306,7 @@ __global__ void __launch_bounds__(NT)
                             for (uint32_t j = f + lane; j < l; j += G) a.add(stage[j]);
                         } else {
                             for (uint32_t j = nb + f + lane; j < nb + l; j += G)
-                                a.add(dev::mul_rn(alpha * vals[j], dev::ld_ro(x + cols[j])));
+                                a.add(dev::mul_rn(alpha * dev::ld_val<T>(vals + j), dev::ld_ro(x + cols[j])));
                         }
                     }
                     dev::group_reduce<G>(a);
@@ -315,7 +323,7 @@ __global__ void __launch_bounds__(NT)
             }
         } else if (nrows == 1 && low == 0) {
             // ---- VECTOR: one row, the whole CTA ----
-            dev::Acc<T, EXT> a = range_sum<T, EXT, NT>(vals, cols, x, alpha, nb, ne, lo, hi, vec != 0);
+            dev::Acc<T, EXT> a = range_sum<V, T, EXT, NT>(vals, cols, x, alpha, nb, ne, lo, hi, vec != 0);
             a = dev::block_reduce_acc(a, red_s, red_c);
             if (tid == 0) sink.template put<EXT>(row, a);
         } else {
@@ -327,7 +335,7 @@ __global__ void __launch_bounds__(NT)
                 const uint32_t first = gid - low;
                 const uint32_t cb = nb + low * kLongChunk;
                 const uint32_t ce = min(re, cb + kLongChunk);
-                dev::Acc<T, EXT> a = range_sum<T, EXT, NT>(vals, cols, x, alpha, cb, ce, lo, hi, vec != 0);
+                dev::Acc<T, EXT> a = range_sum<V, T, EXT, NT>(vals, cols, x, alpha, cb, ce, lo, hi, vec != 0);
                 a = dev::block_reduce_acc(a, red_s, red_c);
                 if (tid == 0) {
                     // partial of this chunk; compensation folded in
@@ -351,9 +359,9 @@ __global__ void __launch_bounds__(NT)
     run_epilogue<T, K>(sink, epi);
 }
 
-template <typename T, bool EXT, int G, int K>
+template <typename V, typename T, bool EXT, int G, int K>
 __global__ void __launch_bounds__(kThreads)
-    csr_vector_kernel(const T* __restrict__ vals, const uint32_t* __restrict__ cols,
+    csr_vector_kernel(const V* __restrict__ vals, const uint32_t* __restrict__ cols,
                       const uint32_t* __restrict__ rp, const T* __restrict__ x, T* __restrict__ y,
                       const T* __restrict__ alpha_p, const T* __restrict__ beta_p, uint32_t nrows,
                       EpiDev<T> epi) {
@@ -372,7 +380,7 @@ __global__ void __launch_bounds__(kThreads)
             const uint32_t nb = dev::ld_ro(rp + row);
             const uint32_t ne = dev::ld_ro(rp + row + 1);
             for (uint32_t j = nb + lane; j < ne; j += G)
-                a.add_prod(alpha * dev::ld_stream(vals + j), dev::ld_ro(x + dev::ld_stream(cols + j)));
+                a.add_prod(alpha * dev::ld_val<T>(vals + j), dev::ld_ro(x + dev::ld_stream(cols + j)));
         }
         dev::group_reduce<G>(a);
         if (row < nrows && lane == 0) sink.template put<EXT>(row, a);
@@ -415,13 +423,13 @@ uint32_t vector_grid(uint32_t nrows, uint32_t g) {
     return static_cast<uint32_t>(ctas);
 }
 
-template <typename T, bool EXT, int K>
-cudaError_t launch_vector(const CsrView<T>& A, const T* alpha, const T* beta, const T* x, T* y,
+template <typename V, typename T, bool EXT, int K>
+cudaError_t launch_vector(const CsrView<V>& A, const T* alpha, const T* beta, const T* x, T* y,
                           const EpiDev<T>& e, cudaStream_t s) {
     const uint32_t g = vector_width(A.nrows, A.nnz);
     const uint32_t grid = vector_grid(A.nrows, g);
 #define CLSP_VEC(GW)                                                                              \
-    csr_vector_kernel<T, EXT, GW, K><<<grid, kThreads, 0, s>>>(A.vals, A.cols, A.rp, x, y, alpha, \
+    csr_vector_kernel<V, T, EXT, GW, K><<<grid, kThreads, 0, s>>>(A.vals, A.cols, A.rp, x, y, alpha, \
                                                                beta, A.nrows, e)
     switch (g) {
         case 2: CLSP_VEC(2); break;
@@ -431,6 +439,47 @@ cudaError_t launch_vector(const CsrView<T>& A, const T* alpha, const T* beta, co
         default: CLSP_VEC(32); break;
     }
 #undef CLSP_VEC
+    return cudaGetLastError();
+}
+
+#include "spmv_tma.cuh"
+
+// Adaptive kernel choice: the TMA-staged pipeline (default) or the plain
+// one-CTA-per-block kernel (CLSPARSE_B200_SPMV_KERNEL=plain).
+bool use_tma_kernel() {
+    static bool on = [] {
+        const char* e = std::getenv("CLSPARSE_B200_SPMV_KERNEL");
+        return !(e && std::string(e) == "plain");
+    }();
+    return on;
+}
+
+template <typename V, typename T, bool EXT, int K>
+cudaError_t launch_tma(const CsrView<V>& A, const T* alpha, const T* beta, const T* x, T* y,
+                       const EpiDev<T>& e, cudaStream_t s, int* err) {
+    using L = tma::Layout<V, T>;
+    auto kern = tma::csr_adaptive_tma_kernel<V, T, EXT, K>;
+    static int blocks_per_sm = -1;
+    static int sms = 0;
+    if (blocks_per_sm < 0) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L::total));
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, tma::kThreads, L::total);
+        blocks_per_sm = b > 0 ? b : 1;
+    }
+    const matrix_meta* m = A.meta;
+    const uint32_t nblocks = static_cast<uint32_t>(m->num_words - 1);
+    uint64_t grid = static_cast<uint64_t>(sms) * blocks_per_sm;
+    if (grid > nblocks) grid = nblocks;
+    if (grid == 0) grid = 1;
+    const int aligned = ((reinterpret_cast<uintptr_t>(A.vals) | reinterpret_cast<uintptr_t>(A.cols) |
+                          reinterpret_cast<uintptr_t>(A.rp)) & 15u) == 0;
+    kern<<<static_cast<uint32_t>(grid), tma::kThreads, L::total, s>>>(
+        A.vals, A.cols, A.rp, x, y, alpha, beta, m->d_rowBlocks, m->d_word_nnz, nblocks, A.nrows,
+        m->nnz_hi, aligned, m->d_lr_partial, m->d_lr_ticket, err, e);
     return cudaGetLastError();
 }
 
@@ -445,24 +494,25 @@ int adaptive_threads() {
     return nt;
 }
 
-template <typename T, bool EXT, int K>
-cudaError_t launch_kind(const CsrView<T>& A, const T* alpha, const T* beta, const T* x, T* y,
+template <typename V, typename T, bool EXT, int K>
+cudaError_t launch_kind(const CsrView<V>& A, const T* alpha, const T* beta, const T* x, T* y,
                         const EpiDev<T>& e, cudaStream_t s) {
-    if (A.meta == nullptr) return launch_vector<T, EXT, K>(A, alpha, beta, x, y, e, s);
+    if (A.meta == nullptr) return launch_vector<V, T, EXT, K>(A, alpha, beta, x, y, e, s);
     const uint32_t nblocks = static_cast<uint32_t>(A.meta->num_words - 1);
     uint32_t grid = nblocks;
     if (grid == 0) {
         if (K == 0) return cudaSuccess;
         grid = 1;  // one idle CTA still finishes the fused reduction
     }
+    if (use_tma_kernel()) return launch_tma<V, T, EXT, K>(A, alpha, beta, x, y, e, s, A.meta->d_error);
     const int vec = ((reinterpret_cast<uintptr_t>(A.vals) | reinterpret_cast<uintptr_t>(A.cols)) & 15u) == 0;
     const matrix_meta* m = A.meta;
     if (adaptive_threads() == 256)
-        csr_adaptive_kernel<T, EXT, K, 256><<<grid, 256, 0, s>>>(
+        csr_adaptive_kernel<V, T, EXT, K, 256><<<grid, 256, 0, s>>>(
             A.vals, A.cols, A.rp, x, y, alpha, beta, m->d_rowBlocks, m->d_word_nnz, nblocks, m->nnz_lo,
             m->nnz_hi, vec, m->d_lr_partial, m->d_lr_ticket, e);
     else
-        csr_adaptive_kernel<T, EXT, K, 128><<<grid, 128, 0, s>>>(
+        csr_adaptive_kernel<V, T, EXT, K, 128><<<grid, 128, 0, s>>>(
             A.vals, A.cols, A.rp, x, y, alpha, beta, m->d_rowBlocks, m->d_word_nnz, nblocks, m->nnz_lo,
             m->nnz_hi, vec, m->d_lr_partial, m->d_lr_ticket, e);
     return cudaGetLastError();
@@ -475,26 +525,29 @@ uint32_t spmv_num_ctas(const matrix_meta* meta, uint32_t nrows, uint32_t nnz) {
     return vector_grid(nrows, vector_width(nrows, nnz));
 }
 
-template <typename T>
-cudaError_t launch_csrmv(const CsrView<T>& A, const T* alpha, const T* beta, const T* x, T* y,
+template <typename V, typename T>
+cudaError_t launch_csrmv(const CsrView<V>& A, const T* alpha, const T* beta, const T* x, T* y,
                          bool extended, const SpmvEpilogue& epi, cudaStream_t s) {
     const EpiDev<T> e = to_dev<T>(epi);
     if (extended) {
-        if (epi.ndots == 0) return launch_kind<T, true, 0>(A, alpha, beta, x, y, e, s);
-        if (epi.ndots == 1) return launch_kind<T, true, 1>(A, alpha, beta, x, y, e, s);
-        return launch_kind<T, true, 2>(A, alpha, beta, x, y, e, s);
+        if (epi.ndots == 0) return launch_kind<V, T, true, 0>(A, alpha, beta, x, y, e, s);
+        if (epi.ndots == 1) return launch_kind<V, T, true, 1>(A, alpha, beta, x, y, e, s);
+        return launch_kind<V, T, true, 2>(A, alpha, beta, x, y, e, s);
     }
-    if (epi.ndots == 0) return launch_kind<T, false, 0>(A, alpha, beta, x, y, e, s);
-    if (epi.ndots == 1) return launch_kind<T, false, 1>(A, alpha, beta, x, y, e, s);
-    return launch_kind<T, false, 2>(A, alpha, beta, x, y, e, s);
+    if (epi.ndots == 0) return launch_kind<V, T, false, 0>(A, alpha, beta, x, y, e, s);
+    if (epi.ndots == 1) return launch_kind<V, T, false, 1>(A, alpha, beta, x, y, e, s);
+    return launch_kind<V, T, false, 2>(A, alpha, beta, x, y, e, s);
 }
 
-template cudaError_t launch_csrmv<float>(const CsrView<float>&, const float*, const float*,
-                                         const float*, float*, bool, const SpmvEpilogue&,
-                                         cudaStream_t);
-template cudaError_t launch_csrmv<double>(const CsrView<double>&, const double*, const double*,
-                                          const double*, double*, bool, const SpmvEpilogue&,
-                                          cudaStream_t);
+template cudaError_t launch_csrmv<float, float>(const CsrView<float>&, const float*, const float*,
+                                                const float*, float*, bool, const SpmvEpilogue&,
+                                                cudaStream_t);
+template cudaError_t launch_csrmv<double, double>(const CsrView<double>&, const double*,
+                                                  const double*, const double*, double*, bool,
+                                                  const SpmvEpilogue&, cudaStream_t);
+template cudaError_t launch_csrmv<__nv_bfloat16, float>(const CsrView<__nv_bfloat16>&, const float*,
+                                                        const float*, const float*, float*, bool,
+                                                        const SpmvEpilogue&, cudaStream_t);
 
 namespace {
 
@@ -519,7 +572,7 @@ clsparseStatus csrmv_entry(const clsparseScalar* alpha, const clsparseCsrMatrix*
                  dev_ptr<const uint32_t>(A->row_pointer, A->off_row_pointer),
                  A->num_rows, A->num_cols, A->num_nonzeros, meta};
     SpmvEpilogue none;
-    cudaError_t e = launch_csrmv<T>(v, dev_ptr<const T>(alpha->value, alpha->off_value),
+    cudaError_t e = launch_csrmv<T, T>(v, dev_ptr<const T>(alpha->value, alpha->off_value),
                                     dev_ptr<const T>(beta->value, beta->off_value),
                                     dev_ptr<const T>(x->values, x->off_values),
                                     dev_ptr<T>(y->values, y->off_values), control->extended_precision,

@@ -98,7 +98,7 @@ def test_spmv_extended_precision(ctrl, orc, dtype):
 
 
 def test_meta_words_equal_reference_binning(ctrl, orc):
-    rp, col, val = matgen.irregular(30_000, n_dense=7, dense_len=20_000, seed=4)
+    rp, col, val = matgen.irregular(30_000, n_dense=7, dense_len=12_000, seed=4)
     A = api.CsrMatrix.from_numpy(rp, col, val)
     size = A.meta_size(ctrl)
     A.create_meta(ctrl)
