@@ -8,9 +8,10 @@ fallback implementation behind this module.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "libclsparse_b200.so"
+LIB_PATH = Path(os.environ.get("CLSPARSE_B200_LIB", Path(__file__).resolve().parent / "libclsparse_b200.so"))
 
 cl_uint = C.c_uint32
 cl_int = C.c_int32
@@ -90,6 +91,11 @@ class clsparseCreateSolverResult(C.Structure):
 
 class clsparseMetaSizeResult(C.Structure):
     _fields_ = [("status", clsparseStatus), ("metaSize", clsparseIdx_t)]
+
+
+class clsparseB200MixedInfo(C.Structure):
+    _fields_ = [("outerIterations", cl_int), ("innerIterations", cl_int),
+                ("initialTrueResidual", C.c_double), ("trueResidual", C.c_double), ("converged", cl_int)]
 
 
 P = C.POINTER
@@ -175,6 +181,8 @@ SIGNATURES = {
     "clsparseB200SolverGetInfo": (clsparseStatus, [_V, P(cl_int), P(C.c_double), P(C.c_double)]),
     "clsparseB200SolverGetDeviceStatus": (clsparseStatus, [_V, P(cl_uint)]),
     "clsparseB200SetSolverLoopMode": (clsparseStatus, [_V, cl_int]),
+    "clsparseB200SolverSetNormType": (clsparseStatus, [_V, cl_int]),
+    "clsparseDcsrcgMixed": (clsparseStatus, [_D, _M, _D, _V, cl_int, C.c_double, P(clsparseB200MixedInfo), _V]),
 }
 
 _lib = None

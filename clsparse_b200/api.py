@@ -184,6 +184,10 @@ class SolverControl:
         check(lib().clsparseB200SolverGetInfo(self.handle, C.byref(it), C.byref(r0), C.byref(r1)), "GetInfo")
         return {"nIters": it.value, "initialResidual": r0.value, "currentResidual": r1.value}
 
+    def set_norm(self, norm: int):
+        """1: the reference's ||r||_1/||b||_1 stop test, 2: ||r||_2/||b||_2."""
+        check(lib().clsparseB200SolverSetNormType(self.handle, norm), "clsparseB200SolverSetNormType")
+
     def device_status(self) -> int:
         b = L.cl_uint()
         check(lib().clsparseB200SolverGetDeviceStatus(self.handle, C.byref(b)), "GetDeviceStatus")
@@ -203,6 +207,17 @@ def solve(kind: str, x: torch.Tensor, A: CsrMatrix, b: torch.Tensor, sc: SolverC
     st = fn(C.byref(vector(x)), C.byref(A.s), C.byref(vector(b)), sc.handle, ctrl.handle)
     check(st, name)
     return sc.info()
+
+
+def cg_mixed(x: torch.Tensor, A: CsrMatrix, b: torch.Tensor, sc: SolverControl, ctrl: Control,
+             inner: str = "fp32", inner_tol: float = 1e-4) -> dict:
+    """FP64 iterative refinement with FP32- or BF16-valued inner CG
+    (clsparseDcsrcgMixed); returns the refinement statistics."""
+    info = L.clsparseB200MixedInfo()
+    prec = {"fp32": 0, "bf16": 1}[inner]
+    check(lib().clsparseDcsrcgMixed(C.byref(vector(x)), C.byref(A.s), C.byref(vector(b)), sc.handle, prec,
+                                    inner_tol, C.byref(info), ctrl.handle), "clsparseDcsrcgMixed")
+    return {f[0]: getattr(info, f[0]) for f in info._fields_}
 
 
 def blas1(name: str, *args, ctrl: Control):

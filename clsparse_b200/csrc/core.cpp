@@ -192,6 +192,7 @@ clsparseStatus clsparseReleaseControl(clsparseControl control) {
         DeviceGuard g(control->device);
         cudaStreamSynchronize(control->stream);
         control->solver_cache.reset();
+        control->mixed_work.reset();
         control->reduce_scratch.release();
         if (control->event) cudaEventDestroy(control->event);
         if (control->capture_stream) cudaStreamDestroy(control->capture_stream);

@@ -26,6 +26,35 @@ __device__ __forceinline__ T ld_ro(const T* p) {
     return __ldg(p);
 }
 
+// Gathered loads of the dense vector x. CLSP_GATHER selects the cache
+// treatment: 0 read-only path (default), 1 L2 only, 2 read-only without L1
+// allocation.
+#ifndef CLSP_GATHER
+#define CLSP_GATHER 0
+#endif
+__device__ __forceinline__ double ld_gather(const double* p) {
+#if CLSP_GATHER == 1
+    return __ldcg(p);
+#elif CLSP_GATHER == 2
+    double v;
+    asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+#else
+    return __ldg(p);
+#endif
+}
+__device__ __forceinline__ float ld_gather(const float* p) {
+#if CLSP_GATHER == 1
+    return __ldcg(p);
+#elif CLSP_GATHER == 2
+    float v;
+    asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+#else
+    return __ldg(p);
+#endif
+}
+
 // Loads one matrix value (double, float or bf16) as the arithmetic type T.
 template <typename T, typename V>
 __device__ __forceinline__ T ld_val(const V* p) {

@@ -42,6 +42,15 @@ struct DeviceBuffer {
 
 struct SolverCache;  // cached CUDA graph + work vectors of the last solve
 
+// Work area of the mixed-precision refinement (mixed.cu), owned by the control.
+struct MixedWork {
+    DeviceBuffer lowvals, y, r32, d, parts;
+    void* pinned = nullptr;
+    ~MixedWork() {
+        if (pinned) cudaFreeHost(pinned);
+    }
+};
+
 }  // namespace clsp
 
 // The control object (reference internal/clsparse-control.hpp:30-80). Owns no
@@ -61,6 +70,7 @@ struct _clsparseControl {
     // Pinned host word used to read back reduction results of solver calls.
     void* pinned = nullptr;
     std::unique_ptr<clsp::SolverCache> solver_cache;
+    std::unique_ptr<clsp::MixedWork> mixed_work;
 };
 
 // CSR-Adaptive meta attached to clsparseCsrMatrix::meta (reference
@@ -94,6 +104,7 @@ struct _solverControl {
     cl_double currentResidual = 0.0;
     PRINT_MODE printMode = QUIET;
     cl_uint deviceStatus = 0;
+    cl_int normType = 0;  // 0: reference L1 stop test, 1: L2 (clsparseB200SolverSetNormType)
     void printSummary(clsparseStatus status) const;
 };
 
@@ -163,6 +174,12 @@ uint32_t spmv_num_ctas(const matrix_meta* meta, uint32_t nrows, uint32_t nnz);
 template <typename V, typename T>
 cudaError_t launch_csrmv(const CsrView<V>& A, const T* alpha, const T* beta, const T* x, T* y,
                          bool extended, const SpmvEpilogue& epi, cudaStream_t s);
+
+// CG with matrix values of type V and vectors in T (solvers.cu); the drop-in
+// entry points use V == T, the mixed-precision refinement uses float / bf16.
+template <typename V, typename T>
+clsparseStatus cg_solve_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                              clSParseSolverControl sc, clsparseControl c);
 
 // Host binning (meta.cpp).
 void compute_row_blocks(cl_ulong* rowBlocks, clsparseIdx_t& rowBlockSize, const clsparseIdx_t* rp,

@@ -1,0 +1,212 @@
+// Mixed-precision iterative refinement around CG (clsparseDcsrcgMixed), a
+// project extension with no reference counterpart.
+//
+// Outer loop, all in FP64 on the device: r = b - A x with the FP64 matrix,
+// ||r||_2 / ||b||_2 is the stop test. Inner solve: Jacobi-PCG (the library's
+// own CG, in the graph/while-loop form) on A d = r / ||b||_2 with the matrix
+// values rounded to FP32 or BF16 (column indices, row pointers and the
+// CSR-Adaptive meta are shared with the FP64 matrix) and FP32 vectors,
+// accumulated in FP32. Then x += ||b||_2 * d in FP64. The inner tolerance is
+// relative (L2) to the inner right-hand side.
+#include <cmath>
+#include <cstring>
+
+#include "device_common.cuh"
+#include "internal.h"
+
+namespace clsp {
+namespace {
+
+constexpr int kThreads = 256;
+
+uint32_t grid_for(size_t n, int sms) {
+    size_t c = (n + kThreads * 4 - 1) / (kThreads * 4);
+    size_t cap = static_cast<size_t>(sms) * 8;
+    if (cap > static_cast<size_t>(kMaxReduceCtas)) cap = kMaxReduceCtas;
+    if (c > cap) c = cap;
+    return static_cast<uint32_t>(c ? c : 1);
+}
+
+template <typename V>
+__global__ void round_values_kernel(const double* __restrict__ src, V* __restrict__ dst, size_t n) {
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        if constexpr (std::is_same_v<V, __nv_bfloat16>)
+            dst[i] = __double2bfloat16(src[i]);
+        else
+            dst[i] = static_cast<V>(src[i]);
+    }
+}
+
+// r = b - y; r32 = r * inv_scale (rounded to FP32); out = {sum r^2, sum b^2}.
+__global__ void __launch_bounds__(kThreads)
+    residual_kernel(const double* __restrict__ b, const double* __restrict__ y, float* __restrict__ r32,
+                    double inv_scale, size_t n, double* parts, uint32_t* ticket, double* out) {
+    double acc[2] = {0.0, 0.0};
+    const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride) {
+        const double bi = b[i];
+        const double ri = bi - y[i];
+        r32[i] = static_cast<float>(ri * inv_scale);
+        acc[0] += ri * ri;
+        acc[1] += bi * bi;
+    }
+    double tot[2];
+    if (dev::grid_reduce_last<2>(acc, parts, ticket, tot) && threadIdx.x == 0) {
+        out[0] = tot[0];
+        out[1] = tot[1];
+    }
+}
+
+__global__ void update_kernel(double* __restrict__ x, const float* __restrict__ d, double scale, size_t n) {
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        x[i] += scale * static_cast<double>(d[i]);
+}
+
+MixedWork& work_of(clsparseControl c) {
+    if (!c->mixed_work) {
+        c->mixed_work = std::make_unique<MixedWork>();
+        cudaMallocHost(&c->mixed_work->pinned, 64);
+    }
+    return *c->mixed_work;
+}
+
+template <typename V>
+clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
+                      clSParseSolverControl sc, double inner_tol, clsparseB200MixedInfo* info,
+                      clsparseControl c) {
+    const size_t n = A->num_rows, nnz = A->num_nonzeros;
+    MixedWork& w = work_of(c);
+    if (w.lowvals.ensure(nnz * sizeof(V) + 256) != cudaSuccess || w.y.ensure(n * 8 + 256) != cudaSuccess ||
+        w.r32.ensure(n * 4 + 256) != cudaSuccess || w.d.ensure(n * 4 + 256) != cudaSuccess ||
+        w.parts.ensure((2 * kMaxReduceCtas + 8) * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return clsparseOutOfResources;
+    }
+    cudaStream_t s = c->stream;
+    const double* Avals = dev_ptr<const double>(A->values, A->off_values);
+    double* x = dev_ptr<double>(xv->values, xv->off_values);
+    const double* b = dev_ptr<const double>(bv->values, bv->off_values);
+    V* lv = static_cast<V*>(w.lowvals.ptr);
+    round_values_kernel<V><<<grid_for(nnz, c->sm_count), kThreads, 0, s>>>(Avals, lv, nnz);
+
+    // FP64 operator and the low-precision copy sharing its structure and meta
+    CsrView<double> A64{Avals, dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices),
+                        dev_ptr<const uint32_t>(A->row_pointer, A->off_row_pointer), A->num_rows,
+                        A->num_cols, A->num_nonzeros, static_cast<const matrix_meta*>(A->meta)};
+    clsparseCsrMatrix Alow = *A;
+    Alow.values = lv;
+    Alow.off_values = 0;
+
+    double* consts = static_cast<double*>(w.parts.ptr);  // [0]=1, [1]=0, [2..3] results
+    uint32_t* ticket = reinterpret_cast<uint32_t*>(consts + 4);
+    double* parts = consts + 8;
+    const double h_consts[4] = {1.0, 0.0, 0.0, 0.0};
+    cudaMemcpyAsync(consts, h_consts, sizeof(h_consts), cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(ticket, 0, 4 * sizeof(uint32_t), s);
+
+    cldenseVector dvec{static_cast<clsparseIdx_t>(n), w.d.ptr, 0};
+    cldenseVector rvec{static_cast<clsparseIdx_t>(n), w.r32.ptr, 0};
+    _solverControl inner;
+    inner.preconditioner = sc->preconditioner;
+    inner.normType = 1;
+    inner.printMode = QUIET;
+
+    const double target = sc->relativeTolerance;
+    const int max_inner_total = sc->maxIters;
+    double bnorm = -1.0, res = 0.0, prev = 1e300;
+    int outer = 0, inner_total = 0, stalls = 0;
+    double* hres = static_cast<double*>(w.pinned);
+    const uint32_t g = grid_for(n, c->sm_count);
+    clsparseStatus st = clsparseSuccess;
+    info->converged = 0;
+    for (;;) {
+        SpmvEpilogue none;
+        if (launch_csrmv<double, double>(A64, consts, consts + 1, x, static_cast<double*>(w.y.ptr), false,
+                                         none, s) != cudaSuccess)
+            return clsparseInvalidKernelExecution;
+        const double inv = bnorm > 0 ? 1.0 / bnorm : 1.0;
+        residual_kernel<<<g, kThreads, 0, s>>>(b, static_cast<const double*>(w.y.ptr),
+                                               static_cast<float*>(w.r32.ptr), inv, n, parts, ticket,
+                                               consts + 2);
+        cudaMemcpyAsync(hres, consts + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) return clsparseInvalidKernelExecution;
+        if (bnorm < 0) {
+            bnorm = std::sqrt(hres[1]);
+            if (bnorm == 0.0) {
+                cudaMemcpyAsync(x, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+                info->outerIterations = 0;
+                info->innerIterations = 0;
+                info->trueResidual = 0.0;
+                info->initialTrueResidual = 0.0;
+                info->converged = 1;
+                return finish_call(c);
+            }
+            // first pass computed r without scaling; redo the rounding
+            continue;
+        }
+        res = std::sqrt(hres[0]) / bnorm;
+        if (outer == 0) info->initialTrueResidual = res;
+        if (res <= target) {
+            info->converged = 1;
+            break;
+        }
+        if (inner_total >= max_inner_total) break;
+        if (res > 0.5 * prev && ++stalls >= 3) break;  // refinement no longer contracts
+        prev = res;
+        // inner solve A_low d = r / ||b||, from d = 0
+        cudaMemsetAsync(w.d.ptr, 0, n * sizeof(float), s);
+        inner.maxIters = max_inner_total - inner_total;
+        inner.relativeTolerance = inner_tol;
+        inner.absoluteTolerance = 0.0;
+        inner.nIters = 0;
+        st = cg_solve_typed<V, float>(&dvec, &Alow, &rvec, &inner, c);
+        if (st != clsparseSuccess) return st;
+        inner_total += inner.nIters + 1;
+        update_kernel<<<g, kThreads, 0, s>>>(x, static_cast<const float*>(w.d.ptr), bnorm, n);
+        ++outer;
+    }
+    info->outerIterations = outer;
+    info->innerIterations = inner_total;
+    info->trueResidual = res;
+    sc->nIters = inner_total;
+    sc->currentResidual = res;
+    sc->initialResidual = info->initialTrueResidual;
+    return finish_call(c);
+}
+
+}  // namespace
+}  // namespace clsp
+
+using namespace clsp;
+
+extern "C" {
+
+clsparseStatus clsparseDcsrcgMixed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                                   clSParseSolverControl solverControl, cl_int innerPrecision,
+                                   cl_double innerTolerance, clsparseB200MixedInfo* info,
+                                   clsparseControl control) {
+    clsparseStatus st = check_entry(control);
+    if (st != clsparseSuccess) return st;
+    if (solverControl == nullptr) return clsparseInvalidSolverControlObject;
+    if (!x || !A || !b || !info) return clsparseInvalidValue;
+    if (A->num_rows != A->num_cols || A->num_rows != x->num_values || A->num_cols != b->num_values)
+        return clsparseInvalidSystemSize;
+    if (innerPrecision != 0 && innerPrecision != 1) return clsparseInvalidType;
+    std::memset(info, 0, sizeof(*info));
+    if (A->num_rows == 0) return clsparseSuccess;
+    DeviceGuard g(control->device);
+    if (innerPrecision == 0)
+        return refine<float>(x, A, b, solverControl, innerTolerance, info, control);
+    return refine<__nv_bfloat16>(x, A, b, solverControl, innerTolerance, info, control);
+}
+
+clsparseStatus clsparseB200SolverSetNormType(clSParseSolverControl solverControl, cl_int normType) {
+    if (solverControl == nullptr) return clsparseInvalidSolverControlObject;
+    if (normType != 1 && normType != 2) return clsparseInvalidValue;
+    solverControl->normType = normType == 2 ? 1 : 0;
+    return clsparseSuccess;
+}
+
+}  // extern "C"

@@ -10,7 +10,10 @@
 namespace clsp {
 namespace pipe {
 
-constexpr uint32_t kSpinLimit = 1u << 22;
+// Each poll may suspend the warp for up to kSuspendNs before it returns; the
+// product bounds one wait to about two seconds.
+constexpr uint32_t kSpinLimit = 1u << 17;
+constexpr uint32_t kSuspendNs = 16384;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -44,10 +47,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(kSuspendNs)
         : "memory");
     return ok != 0;
 }

@@ -26,7 +26,7 @@ struct SolverState {
     double relTol;
     double absTol;
     int maxIters;
-    int pad0;
+    int norm_type;  // 0: ||.||_1 as the reference, 1: ||.||_2
     // scalars of the iteration, in T like the reference
     T norm_b, rz, rz_old, yp, alpha, beta, omega, norm_r, res;
     T rsr_old, rsr_new, rs_amp, amss, amsams;

@@ -55,14 +55,26 @@ __device__ __forceinline__ double dabs(T v) {
     return fabs(static_cast<double>(v));
 }
 
+// Contribution of one residual entry to the stop-test norm: |v| for the
+// reference's L1 test, v^2 for the L2 option.
+template <typename T>
+__device__ __forceinline__ double norm_term(T v, int l2) {
+    const double d = static_cast<double>(v);
+    return l2 ? d * d : fabs(d);
+}
+
+__device__ __forceinline__ double norm_finish(double acc, int l2) {
+    return l2 ? sqrt(acc) : acc;
+}
+
 // invD[row] = 1 / A[row,row], first matching entry of the row as in the
 // reference's extract_diagonal (src/library/kernels/matrix_utils.cl:65-98).
 // A row without a diagonal entry gets 0 and raises a status bit; a zero
 // diagonal gives inf like the reference and raises another.
-template <typename T>
+template <typename V, typename T>
 __global__ void __launch_bounds__(kThreads)
     extract_inv_diag_kernel(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols,
-                            const T* __restrict__ vals, uint32_t n, T* __restrict__ invD,
+                            const V* __restrict__ vals, uint32_t n, T* __restrict__ invD,
                             SolverState<T>* st) {
     const int lane = threadIdx.x & 31;
     const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x) >> 5;
@@ -77,7 +89,7 @@ __global__ void __launch_bounds__(kThreads)
             if (ball) {
                 const int first = __ffs(ball) - 1;
                 if (lane == first) {
-                    const T v = vals[j];
+                    const T v = dev::to_t<T>(vals[j]);
                     invD[row] = T(1) / v;
                     if (v == T(0)) atomicOr(&st->status_bits, kStatusZeroDiag);
                 }
@@ -113,6 +125,7 @@ struct CgArgs {
 template <typename T>
 __global__ void __launch_bounds__(kThreads) cg_init_kernel(CgArgs<T> a) {
     double acc[3] = {0.0, 0.0, 0.0};
+    const int l2 = a.st->norm_type;
     const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
     for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
         const T bi = a.b[i];
@@ -120,14 +133,14 @@ __global__ void __launch_bounds__(kThreads) cg_init_kernel(CgArgs<T> a) {
         const T zi = apply_m(a.invD, i, ri);
         a.r[i] = ri;
         a.p[i] = zi;
-        acc[0] += dabs(bi);
-        acc[1] += dabs(ri);
+        acc[0] += norm_term(bi, l2);
+        acc[1] += norm_term(ri, l2);
         acc[2] += static_cast<double>(ri) * static_cast<double>(zi);
     }
     double tot[3];
     if (dev::grid_reduce_last<3>(acc, a.parts, a.ticket, tot) && threadIdx.x == 0) {
         SolverState<T>* st = a.st;
-        st->norm_b = static_cast<T>(tot[0]);
+        st->norm_b = static_cast<T>(norm_finish(tot[0], l2));
         if (st->norm_b == T(0)) {
             st->zero_b = 1;
             st->done = 1;
@@ -135,7 +148,7 @@ __global__ void __launch_bounds__(kThreads) cg_init_kernel(CgArgs<T> a) {
             set_condition(a.cond, 0u);
             return;
         }
-        st->norm_r = static_cast<T>(tot[1]);
+        st->norm_r = static_cast<T>(norm_finish(tot[1], l2));
         st->res = st->norm_r / st->norm_b;
         st->init_res = static_cast<double>(st->res);
         st->cur_res = st->init_res;
@@ -159,6 +172,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) cg_update_kernel(CgArgs<T> a) {
     if (a.st->done) return;
     const T alpha = a.st->alpha;
+    const int l2 = a.st->norm_type;
     double acc[2] = {0.0, 0.0};
     const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
     for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
@@ -168,7 +182,7 @@ __global__ void __launch_bounds__(kThreads) cg_update_kernel(CgArgs<T> a) {
         a.x[i] = xi;
         a.r[i] = ri;
         acc[0] += static_cast<double>(ri) * static_cast<double>(zi);
-        acc[1] += dabs(ri);
+        acc[1] += norm_term(ri, l2);
     }
     double tot[2];
     if (dev::grid_reduce_last<2>(acc, a.parts, a.ticket, tot) && threadIdx.x == 0) {
@@ -176,7 +190,7 @@ __global__ void __launch_bounds__(kThreads) cg_update_kernel(CgArgs<T> a) {
         st->rz_old = st->rz;
         st->rz = static_cast<T>(tot[0]);
         st->beta = st->rz / st->rz_old;
-        st->norm_r = static_cast<T>(tot[1]);
+        st->norm_r = static_cast<T>(norm_finish(tot[1], l2));
         st->res = st->norm_r / st->norm_b;
         st->nIters = st->iteration;
         st->iteration += 1;
@@ -236,6 +250,7 @@ struct BicgArgs {
 template <typename T>
 __global__ void __launch_bounds__(kThreads) bicg_init_kernel(BicgArgs<T> a) {
     double acc[3] = {0.0, 0.0, 0.0};
+    const int l2 = a.st->norm_type;
     const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
     for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
         const T bi = a.b[i];
@@ -244,14 +259,14 @@ __global__ void __launch_bounds__(kThreads) bicg_init_kernel(BicgArgs<T> a) {
         a.rs[i] = ri;
         a.p[i] = ri;
         if (a.invD) a.Mp[i] = ri * a.invD[i];
-        acc[0] += dabs(bi);
-        acc[1] += dabs(ri);
+        acc[0] += norm_term(bi, l2);
+        acc[1] += norm_term(ri, l2);
         acc[2] += static_cast<double>(ri) * static_cast<double>(ri);
     }
     double tot[3];
     if (dev::grid_reduce_last<3>(acc, a.parts, a.ticket, tot) && threadIdx.x == 0) {
         SolverState<T>* st = a.st;
-        st->norm_b = static_cast<T>(tot[0]);
+        st->norm_b = static_cast<T>(norm_finish(tot[0], l2));
         if (st->norm_b <= std::numeric_limits<T>::min()) {
             st->zero_b = 1;
             st->done = 1;
@@ -259,7 +274,7 @@ __global__ void __launch_bounds__(kThreads) bicg_init_kernel(BicgArgs<T> a) {
             set_condition(a.cond, 0u);
             return;
         }
-        st->norm_r = static_cast<T>(tot[1]);
+        st->norm_r = static_cast<T>(norm_finish(tot[1], l2));
         st->res = st->norm_r / st->norm_b;
         st->init_res = static_cast<double>(st->res);
         st->cur_res = st->init_res;
@@ -282,18 +297,19 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) bicg_s_kernel(BicgArgs<T> a) {
     if (a.st->done) return;
     const T alpha = a.st->alpha;
+    const int l2 = a.st->norm_type;
     double acc[1] = {0.0};
     const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
     for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
         const T si = a.r[i] - alpha * a.AMp[i];
         a.s[i] = si;
         if (a.invD) a.Ms[i] = si * a.invD[i];
-        acc[0] += dabs(si);
+        acc[0] += norm_term(si, l2);
     }
     double tot[1];
     if (dev::grid_reduce_last<1>(acc, a.parts, a.ticket, tot) && threadIdx.x == 0) {
         SolverState<T>* st = a.st;
-        const T norm_s = static_cast<T>(tot[0]);
+        const T norm_s = static_cast<T>(norm_finish(tot[0], l2));
         st->res = norm_s / st->norm_b;
         st->cur_res = static_cast<double>(st->res);
         if (!isfinite(st->cur_res)) st->status_bits |= kStatusNonFinite;
@@ -312,6 +328,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) bicg_x_kernel(BicgArgs<T> a) {
     const int done = a.st->done;
     if (done == 1) return;
+    const int l2 = a.st->norm_type;
     const T alpha = a.st->alpha;
     const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
     double acc[2] = {0.0, 0.0};
@@ -325,7 +342,7 @@ __global__ void __launch_bounds__(kThreads) bicg_x_kernel(BicgArgs<T> a) {
             a.x[i] = x1 + omega * a.Ms[i];
             const T ri = a.s[i] - omega * a.AMs[i];
             a.r[i] = ri;
-            acc[0] += dabs(ri);
+            acc[0] += norm_term(ri, l2);
             acc[1] += static_cast<double>(a.rs[i]) * static_cast<double>(ri);
         }
     }
@@ -336,7 +353,7 @@ __global__ void __launch_bounds__(kThreads) bicg_x_kernel(BicgArgs<T> a) {
             st->done = 1;
             return;
         }
-        st->norm_r = static_cast<T>(tot[0]);
+        st->norm_r = static_cast<T>(norm_finish(tot[0], l2));
         st->res = st->norm_r / st->norm_b;
         st->cur_res = static_cast<double>(st->res);
         if (!isfinite(st->cur_res)) st->status_bits |= kStatusNonFinite;
@@ -487,6 +504,7 @@ void init_state(SolverState<T>& h, clSParseSolverControl sc) {
     h.relTol = sc->relativeTolerance;
     h.absTol = sc->absoluteTolerance;
     h.maxIters = sc->maxIters;
+    h.norm_type = sc->normType & 1;
     h.nIters = sc->nIters;
     h.one = T(1);
     h.zero = T(0);
@@ -514,16 +532,16 @@ clsparseStatus read_back(clsparseControl c, SolverCache& cache, clSParseSolverCo
     return clsparseSuccess;
 }
 
-SolverKey make_key(int kind, int dsize, clSParseSolverControl sc, clsparseControl c,
+SolverKey make_key(int kind, int vsize, int dsize, clSParseSolverControl sc, clsparseControl c,
                    const clsparseCsrMatrix* A, const cldenseVector* x, const cldenseVector* b) {
     SolverKey k;
     std::memset(&k, 0, sizeof(k));
     k.kind = kind;
-    k.dtype = dsize;
+    k.dtype = dsize * 16 + vsize + 256 * (sc->normType & 1);
     k.precond = sc->preconditioner == DIAGONAL ? 1 : 0;
     k.ext = c->extended_precision ? 1 : 0;
     k.loop_mode = c->solver_loop_mode;
-    k.ptrs[0] = static_cast<const char*>(A->values) + static_cast<size_t>(A->off_values) * dsize;
+    k.ptrs[0] = static_cast<const char*>(A->values) + static_cast<size_t>(A->off_values) * vsize;
     k.ptrs[1] = static_cast<const uint32_t*>(A->col_indices) + A->off_col_indices;
     k.ptrs[2] = static_cast<const uint32_t*>(A->row_pointer) + A->off_row_pointer;
     k.ptrs[3] = static_cast<const char*>(x->values) + static_cast<size_t>(x->off_values) * dsize;
@@ -561,7 +579,7 @@ clsparseStatus prepare_cache(clsparseControl c, SolverCache& cache, const Solver
     return clsparseSuccess;
 }
 
-template <typename T>
+template <typename V, typename T>
 clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
                         clSParseSolverControl sc, clsparseControl c) {
     clsparseStatus stt = check_solver_args(xv, A, bv, sc, c);
@@ -570,9 +588,9 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
     const size_t n = A->num_rows;
     if (!c->solver_cache) c->solver_cache = std::make_unique<SolverCache>();
     SolverCache& cache = *c->solver_cache;
-    const CsrView<T> Av = view_of<T>(A);
+    const CsrView<V> Av = view_of<V>(A);
     const uint32_t spmv_ctas = spmv_num_ctas(Av.meta, Av.nrows, Av.nnz);
-    const SolverKey key = make_key(1, sizeof(T), sc, c, A, xv, bv);
+    const SolverKey key = make_key(1, sizeof(V), sizeof(T), sc, c, A, xv, bv);
     bool rebuild = false;
     stt = prepare_cache<T>(c, cache, key, 4, n, spmv_ctas, rebuild);
     if (stt != clsparseSuccess) return stt;
@@ -605,10 +623,10 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
         CgArgs<T> aa = a;
         aa.cond = h;
         if (aa.invD)
-            extract_inv_diag_kernel<T><<<vg, kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
-                                                               invD, st);
+            extract_inv_diag_kernel<V, T><<<vg, kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
+                                                                  invD, st);
         SpmvEpilogue none;
-        launch_csrmv<T, T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
+        launch_csrmv<V, T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
         cg_init_kernel<T><<<vg, kThreads, 0, s>>>(aa);
     };
     auto body = [&](cudaStream_t s, unsigned long long h) {
@@ -622,7 +640,7 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
         epi.op = EpiOp::CgAlpha;
         epi.state = st;
         epi.done = &st->done;
-        launch_csrmv<T, T>(Av, &st->one, &st->zero, aa.p, aa.y, ext, epi, s);
+        launch_csrmv<V, T>(Av, &st->one, &st->zero, aa.p, aa.y, ext, epi, s);
         cg_update_kernel<T><<<vg, kThreads, 0, s>>>(aa);
         cg_p_kernel<T><<<vg, kThreads, 0, s>>>(aa);
     };
@@ -655,7 +673,7 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
     SolverCache& cache = *c->solver_cache;
     const CsrView<T> Av = view_of<T>(A);
     const uint32_t spmv_ctas = spmv_num_ctas(Av.meta, Av.nrows, Av.nnz);
-    const SolverKey key = make_key(2, sizeof(T), sc, c, A, xv, bv);
+    const SolverKey key = make_key(2, sizeof(T), sizeof(T), sc, c, A, xv, bv);
     bool rebuild = false;
     stt = prepare_cache<T>(c, cache, key, 11, n, spmv_ctas, rebuild);
     if (stt != clsparseSuccess) return stt;
@@ -696,8 +714,8 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
         BicgArgs<T> aa = a;
         aa.cond = h;
         if (aa.invD)
-            extract_inv_diag_kernel<T><<<vg, kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
-                                                               invD, st);
+            extract_inv_diag_kernel<T, T><<<vg, kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
+                                                                  invD, st);
         SpmvEpilogue none;
         launch_csrmv<T, T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
         bicg_init_kernel<T><<<vg, kThreads, 0, s>>>(aa);
@@ -747,6 +765,22 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
 }
 
 }  // namespace
+
+template <typename V, typename T>
+clsparseStatus cg_solve_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                              clSParseSolverControl sc, clsparseControl c) {
+    return cg_solve<V, T>(x, A, b, sc, c);
+}
+template clsparseStatus cg_solve_typed<double, double>(cldenseVector*, const clsparseCsrMatrix*,
+                                                       const cldenseVector*, clSParseSolverControl,
+                                                       clsparseControl);
+template clsparseStatus cg_solve_typed<float, float>(cldenseVector*, const clsparseCsrMatrix*,
+                                                     const cldenseVector*, clSParseSolverControl,
+                                                     clsparseControl);
+template clsparseStatus cg_solve_typed<__nv_bfloat16, float>(cldenseVector*, const clsparseCsrMatrix*,
+                                                             const cldenseVector*,
+                                                             clSParseSolverControl, clsparseControl);
+
 }  // namespace clsp
 
 using namespace clsp;
@@ -755,12 +789,12 @@ extern "C" {
 
 clsparseStatus clsparseScsrcg(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
                               clSParseSolverControl solverControl, clsparseControl control) {
-    return cg_solve<float>(x, A, b, solverControl, control);
+    return cg_solve<float, float>(x, A, b, solverControl, control);
 }
 
 clsparseStatus clsparseDcsrcg(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
                               clSParseSolverControl solverControl, clsparseControl control) {
-    return cg_solve<double>(x, A, b, solverControl, control);
+    return cg_solve<double, double>(x, A, b, solverControl, control);
 }
 
 clsparseStatus clsparseScsrbicgStab(cldenseVector* x, const clsparseCsrMatrix* A,

@@ -169,7 +169,7 @@ __device__ __forceinline__ void gather_quads(const T* __restrict__ x, const Quad
 #pragma unroll
     for (int j = 0; j < N; ++j)
 #pragma unroll
-        for (int k = 0; k < 4; ++k) xv[j][k] = (q[j].mask & (1u << k)) ? dev::ld_ro(x + q[j].c[k]) : T(0);
+        for (int k = 0; k < 4; ++k) xv[j][k] = (q[j].mask & (1u << k)) ? dev::ld_gather(x + q[j].c[k]) : T(0);
 }
 
 // Sum of alpha*a_j*x[col_j] over [cb, ce) by the whole CTA (VECTOR rows and
@@ -206,6 +206,7 @@ __device__ __forceinline__ dev::Acc<T, EXT> range_sum(const V* __restrict__ vals
 }
 
 constexpr uint32_t kRpStage = kBlkSize + 1;  // row pointers of a STREAM block kept in shared memory
+constexpr uint32_t kStageRow = kBlkSize / 4 + 2;  // quads per block (+1 ragged) + 1 bank skew
 
 template <typename V, typename T, bool EXT, int K, int NT>
 __global__ void __launch_bounds__(NT)
@@ -216,7 +217,11 @@ __global__ void __launch_bounds__(NT)
                         uint32_t nblocks, uint32_t lo, uint32_t hi, int vec,
                         double* __restrict__ lr_partial, uint32_t* __restrict__ lr_ticket,
                         EpiDev<T> epi) {
-    __shared__ T stage[kBlkSize];
+    // Products of a STREAM block, quad-transposed: element e (counted from the
+    // block's 16-byte-aligned start) lives at stage[(e & 3) * kStageRow + e / 4],
+    // so a warp's stores of one quad slot are contiguous and the row
+    // reductions read with few bank conflicts.
+    __shared__ T stage[4 * kStageRow];
     __shared__ uint32_t srp[kRpStage];
     __shared__ T red_s[32];
     __shared__ T red_c[32];
@@ -272,7 +277,8 @@ __global__ void __launch_bounds__(NT)
                     const uint32_t e0 = base + 4 * (tid + j * NT);
 #pragma unroll
                     for (int k = 0; k < 4; ++k)
-                        if (q[j].mask & (1u << k)) stage[e0 + k - nb] = dev::mul_rn(alpha * q[j].v[k], xv[j][k]);
+                        if (q[j].mask & (1u << k))
+                            stage[k * kStageRow + (e0 - base) / 4] = dev::mul_rn(alpha * q[j].v[k], xv[j][k]);
                 }
                 // the quad past QPT*NT, present when the block starts unaligned
                 for (uint32_t g = QPT * NT + tid; g < nq; g += NT) {
@@ -282,7 +288,7 @@ __global__ void __launch_bounds__(NT)
                     gather_quads(x, r, rv);
 #pragma unroll
                     for (int k = 0; k < 4; ++k)
-                        if (r[0].mask & (1u << k)) stage[base + 4 * g + k - nb] = dev::mul_rn(alpha * r[0].v[k], rv[0][k]);
+                        if (r[0].mask & (1u << k)) stage[k * kStageRow + g] = dev::mul_rn(alpha * r[0].v[k], rv[0][k]);
                 }
             } else if (rp_staged) {
                 for (uint32_t i = tid; i <= nrows; i += NT) srp[i] = dev::ld_ro(rp + row + i);
@@ -303,7 +309,11 @@ __global__ void __launch_bounds__(NT)
                         const uint32_t f = (rp_staged ? srp[r] : dev::ld_ro(rp + row + r)) - nb;
                         const uint32_t l = (rp_staged ? srp[r + 1] : dev::ld_ro(rp + row + r + 1)) - nb;
                         if (staged) {
-                            for (uint32_t j = f + lane; j < l; j += G) a.add(stage[j]);
+                            const uint32_t off = nb & 3u;
+                            for (uint32_t j = f + lane; j < l; j += G) {
+                                const uint32_t e = j + off;
+                                a.add(stage[(e & 3u) * kStageRow + (e >> 2)]);
+                            }
                         } else {
                             for (uint32_t j = nb + f + lane; j < nb + l; j += G)
                                 a.add(dev::mul_rn(alpha * dev::ld_val<T>(vals + j), dev::ld_ro(x + cols[j])));

@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(kThreads, EXT ? 1 : 2)
                     }
 #pragma unroll
                     for (int u = 0; u < 4; ++u)
-                        if (tid + u * kConsumers < cnt) xv[u] = dev::ld_ro(x + cc[u]);
+                        if (tid + u * kConsumers < cnt) xv[u] = dev::ld_gather(x + cc[u]);
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         const uint32_t i = tid + u * kConsumers;

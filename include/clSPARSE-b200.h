@@ -53,6 +53,35 @@ clsparseB200SolverGetInfo(clSParseSolverControl solverControl, cl_int* nIters,
 CLSPARSE_EXPORT clsparseStatus
 clsparseB200SolverGetDeviceStatus(clSParseSolverControl solverControl, cl_uint* statusBits);
 
+/* Stop-test norm of clsparse{S,D}csrcg / csrbicgStab on this solver control:
+ * 1 = ||r||_1 / ||b||_1 as the reference (the default), 2 = ||r||_2 / ||b||_2. */
+CLSPARSE_EXPORT clsparseStatus
+clsparseB200SolverSetNormType(clSParseSolverControl solverControl, cl_int normType);
+
+/* Outcome of a mixed-precision refinement solve. */
+typedef struct clsparseB200MixedInfo_
+{
+    cl_int outerIterations;       /* FP64 residual evaluations after the first */
+    cl_int innerIterations;       /* CG iterations in the low-precision inner solves */
+    cl_double initialTrueResidual;/* ||b - A x0||_2 / ||b||_2, FP64 */
+    cl_double trueResidual;       /* ||b - A x||_2 / ||b||_2 on exit, FP64 */
+    cl_int converged;             /* trueResidual <= the control's relative tolerance */
+} clsparseB200MixedInfo;
+
+/* FP64 iterative refinement around a low-precision Jacobi/none-preconditioned
+ * CG: the FP64 residual r = b - A x, the update x += d and the stop test
+ * ||r||_2 / ||b||_2 <= relTol run in FP64 on the device; the inner solves of
+ * A d = r use the matrix values rounded to FP32 (innerPrecision 0) or BF16
+ * (innerPrecision 1) with FP32 vectors and FP32 accumulation, each to a
+ * relative L2 reduction of innerTolerance. maxIters of the solver control
+ * bounds the total inner iterations. x holds the initial guess on entry.
+ * No reference counterpart (a project extension). */
+CLSPARSE_EXPORT clsparseStatus
+clsparseDcsrcgMixed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                    clSParseSolverControl solverControl, cl_int innerPrecision,
+                    cl_double innerTolerance, clsparseB200MixedInfo* info,
+                    clsparseControl control);
+
 /* Solver loop driver: 0 = one CUDA graph per solve with a device-side
  * conditional WHILE node (no host round trip per iteration, the default);
  * 1 = host-enqueued chunks of iterations with a device done flag. Both give
