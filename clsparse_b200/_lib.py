@@ -204,3 +204,13 @@ def load() -> C.CDLL:
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+class clsparseB200BatchResult(C.Structure):
+    _fields_ = [("iterations", C.POINTER(cl_int)), ("residuals", C.POINTER(C.c_double)),
+                ("systemsConverged", cl_int), ("maxIterations", cl_int), ("worstResidual", C.c_double)]
+
+
+SIGNATURES["clsparseScsrcgBatched"] = (
+    clsparseStatus, [P(cldenseVector), P(clsparseCsrMatrix), P(cldenseVector), P(clsparseIdx_t), cl_int,
+                     P(cl_int), C.c_void_p, P(clsparseB200BatchResult), C.c_void_p])

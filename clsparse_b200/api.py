@@ -230,3 +230,24 @@ def blas1(name: str, *args, ctrl: Control):
         else:
             conv.append(C.byref(vector(a)))
     check(getattr(lib(), name)(*conv, ctrl.handle), name)
+
+
+def cg_batched(x: torch.Tensor, A: CsrMatrix, b: torch.Tensor, offsets, sc: SolverControl, ctrl: Control,
+               lanes=None) -> dict:
+    """Batched FP32 Jacobi-CG over the block-diagonal systems of A
+    (clsparseScsrcgBatched). offsets: numpy/sequence of num_systems+1 row offsets."""
+    off = np.ascontiguousarray(offsets, dtype=np.uint32)
+    nsys = len(off) - 1
+    iters = np.zeros(nsys, dtype=np.int32)
+    res = np.zeros(nsys, dtype=np.float64)
+    out = L.clsparseB200BatchResult(iters.ctypes.data_as(C.POINTER(L.cl_int)),
+                                    res.ctypes.data_as(C.POINTER(C.c_double)), 0, 0, 0.0)
+    lp = None
+    if lanes is not None:
+        lanes = np.ascontiguousarray(lanes, dtype=np.int32)
+        lp = lanes.ctypes.data_as(C.POINTER(L.cl_int))
+    check(lib().clsparseScsrcgBatched(C.byref(vector(x)), C.byref(A.s), C.byref(vector(b)),
+                                      off.ctypes.data_as(C.POINTER(L.clsparseIdx_t)), nsys, lp, sc.handle,
+                                      C.byref(out), ctrl.handle), "clsparseScsrcgBatched")
+    return {"iterations": iters, "residuals": res, "converged": out.systemsConverged,
+            "max_iterations": out.maxIterations, "worst_residual": out.worstResidual}

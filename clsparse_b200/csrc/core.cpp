@@ -193,6 +193,7 @@ clsparseStatus clsparseReleaseControl(clsparseControl control) {
         cudaStreamSynchronize(control->stream);
         control->solver_cache.reset();
         control->mixed_work.reset();
+        control->batch_work.reset();
         control->reduce_scratch.release();
         if (control->event) cudaEventDestroy(control->event);
         if (control->capture_stream) cudaStreamDestroy(control->capture_stream);

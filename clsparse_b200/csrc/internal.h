@@ -51,6 +51,17 @@ struct MixedWork {
     }
 };
 
+// Work area and cached graph of the batched solver (batched.cu).
+struct BatchWork {
+    DeviceBuffer vecs, meta, out;
+    cudaGraphExec_t exec = nullptr;
+    unsigned char args[256] = {};  // kernel arguments the graph was captured with
+    uint32_t grid = 0;
+    ~BatchWork() {
+        if (exec) cudaGraphExecDestroy(exec);
+    }
+};
+
 }  // namespace clsp
 
 // The control object (reference internal/clsparse-control.hpp:30-80). Owns no
@@ -71,6 +82,7 @@ struct _clsparseControl {
     void* pinned = nullptr;
     std::unique_ptr<clsp::SolverCache> solver_cache;
     std::unique_ptr<clsp::MixedWork> mixed_work;
+    std::unique_ptr<clsp::BatchWork> batch_work;
 };
 
 // CSR-Adaptive meta attached to clsparseCsrMatrix::meta (reference

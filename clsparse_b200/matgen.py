@@ -193,3 +193,48 @@ def spmv_bytes(n_rows: int, n_cols: int, nnz: int, val_bytes: int, vec_bytes: in
     if beta_nonzero:
         b += vec_bytes * n_rows
     return b
+
+
+def stencil_prefix(n: int, dim: int, k):
+    """The first n cells (natural order) of a dim-D cell grid just big enough
+    to hold them, as a variable-coefficient diffusion operator: the principal
+    n x n block of the full grid's operator, so still SPD."""
+    side = int(np.ceil(n ** (1.0 / dim) - 1e-9))
+    while side ** dim < n:
+        side += 1
+    rp, col, val = diffusion((side,) * dim, k[: side ** dim] if len(k) >= side ** dim else
+                             np.resize(k, side ** dim))
+    # keep rows < n and columns < n
+    nnz_keep = int(rp[n])
+    c = col[:nnz_keep]
+    v = val[:nnz_keep]
+    keep = c < n
+    rows = np.repeat(np.arange(n), np.diff(rp[: n + 1]).astype(np.int64))[keep]
+    out_rp = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(out_rp, rows + 1, 1)
+    return np.cumsum(out_rp).astype(np.uint32), c[keep].astype(np.uint32), v[keep]
+
+
+def batched_systems(num: int, n_min: int = 500, n_max: int = 50_000, sigma: float = 1.0, seed: int = 11):
+    """`num` SPD systems, n log-uniform in [n_min, n_max], each a 2D 5-point or
+    3D 7-point variable-coefficient diffusion (coin flip) with coefficients
+    exp(N(0, sigma^2)), stacked block-diagonally. Returns (row_ptr, col, val,
+    offsets, dims) with offsets the first row of each system (num + 1 entries)."""
+    rng = np.random.default_rng(seed)
+    ns = np.rint(np.exp(rng.uniform(np.log(n_min), np.log(n_max), size=num))).astype(np.int64)
+    dims = rng.integers(2, 4, size=num)
+    rps, cols, vals = [], [], []
+    offsets = np.zeros(num + 1, dtype=np.int64)
+    nnz_base = 0
+    for s in range(num):
+        n = int(ns[s])
+        side = int(np.ceil(n ** (1.0 / dims[s]) - 1e-9)) + 1
+        k = np.exp(rng.normal(0.0, sigma, size=side ** int(dims[s])))
+        rp, c, v = stencil_prefix(n, int(dims[s]), k)
+        offsets[s + 1] = offsets[s] + n
+        rps.append(rp[:-1].astype(np.int64) + nnz_base)
+        cols.append(c.astype(np.int64) + offsets[s])
+        vals.append(v)
+        nnz_base += int(rp[-1])
+    rp_all = np.concatenate(rps + [np.array([nnz_base])]).astype(np.uint32)
+    return rp_all, np.concatenate(cols).astype(np.uint32), np.concatenate(vals), offsets.astype(np.uint32), dims

@@ -82,6 +82,32 @@ clsparseDcsrcgMixed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseV
                     cl_double innerTolerance, clsparseB200MixedInfo* info,
                     clsparseControl control);
 
+/* Per-system results of a batched solve. The two arrays are optional (NULL) or
+ * hold numSystems entries each. */
+typedef struct clsparseB200BatchResult_
+{
+    cl_int* iterations;        /* CG iterations of each system */
+    cl_double* residuals;      /* FP64 ||b - A x||_2 / ||b||_2 of each system on exit */
+    cl_int systemsConverged;   /* systems whose FP64 residual met the tolerance */
+    cl_int maxIterations;
+    cl_double worstResidual;
+} clsparseB200BatchResult;
+
+/* Solves numSystems independent SPD systems stacked block-diagonally in A
+ * (system s owns rows and columns [systemOffsets[s], systemOffsets[s+1]),
+ * systemOffsets a host array of numSystems+1 entries starting at 0 and ending
+ * at num_rows) with Jacobi-CG in FP32, in one persistent launch captured into
+ * a CUDA graph. Each system stops when its FP64 true residual
+ * ||b - A x||_2 / ||b||_2 <= the control's relTol (checked whenever the FP32
+ * recursive residual says so; CG restarts from x otherwise) or after maxIters
+ * iterations. lanesPerRow (optional, per system: 1..32, a power of two) sets
+ * the SpMV width, e.g. from the autotuner. No reference counterpart. */
+CLSPARSE_EXPORT clsparseStatus
+clsparseScsrcgBatched(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                      const clsparseIdx_t* systemOffsets, cl_int numSystems,
+                      const cl_int* lanesPerRow, clSParseSolverControl solverControl,
+                      clsparseB200BatchResult* result, clsparseControl control);
+
 /* Solver loop driver: 0 = one CUDA graph per solve with a device-side
  * conditional WHILE node (no host round trip per iteration, the default);
  * 1 = host-enqueued chunks of iterations with a device done flag. Both give
