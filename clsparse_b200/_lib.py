@@ -211,6 +211,9 @@ class clsparseB200BatchResult(C.Structure):
                 ("systemsConverged", cl_int), ("maxIterations", cl_int), ("worstResidual", C.c_double)]
 
 
+SIGNATURES["cldenseDdotNoAlloc"] = (clsparseStatus, [P(clsparseScalar), P(cldenseVector), P(cldenseVector),
+                                                     C.c_void_p])
+
 SIGNATURES["clsparseScsrcgBatched"] = (
     clsparseStatus, [P(cldenseVector), P(clsparseCsrMatrix), P(cldenseVector), P(clsparseIdx_t), cl_int,
                      P(cl_int), C.c_void_p, P(clsparseB200BatchResult), C.c_void_p])

@@ -108,6 +108,21 @@ clsparseScsrcgBatched(cldenseVector* x, const clsparseCsrMatrix* A, const cldens
                       const cl_int* lanesPerRow, clSParseSolverControl solverControl,
                       clsparseB200BatchResult* result, clsparseControl control);
 
+/* FP64 dot product r = <x, y> that allocates nothing, for callers that may
+ * not call cudaMalloc (allocation-free real-time loops, applications that
+ * budget every device allocation themselves, code enqueuing into streams it
+ * does not own). It needs no clsparseControl (creating one allocates) and
+ * takes the CUDA stream directly; its scratch is a fixed device array of
+ * about 16 KB inside the library, resident on every GPU that loads it.
+ * Limit: at most 33,554,432 elements (clsparseInvalidSize beyond). Returns
+ * once the work is enqueued on queue. All calls share the array, so calls
+ * that overlap on the GPU race and must be serialised by the caller. The
+ * first call on a device looks the array up on that device; make it before
+ * beginning any stream capture. No counterpart in the reference. */
+CLSPARSE_EXPORT clsparseStatus
+cldenseDdotNoAlloc(clsparseScalar* r, const cldenseVector* x, const cldenseVector* y,
+                   cl_command_queue queue);
+
 /* Solver loop driver: 0 = one CUDA graph per solve with a device-side
  * conditional WHILE node (no host round trip per iteration, the default);
  * 1 = host-enqueued chunks of iterations with a device done flag. Both give
