@@ -217,3 +217,22 @@ SIGNATURES["cldenseDdotNoAlloc"] = (clsparseStatus, [P(clsparseScalar), P(cldens
 SIGNATURES["clsparseScsrcgBatched"] = (
     clsparseStatus, [P(cldenseVector), P(clsparseCsrMatrix), P(cldenseVector), P(clsparseIdx_t), cl_int,
                      P(cl_int), C.c_void_p, P(clsparseB200BatchResult), C.c_void_p])
+
+SIGNATURES.update({
+    "clsparseB200SpaiCreate": (clsparseStatus, [P(C.c_void_p), cl_ulong]),
+    "clsparseB200SpaiRelease": (clsparseStatus, [C.c_void_p]),
+    "clsparseB200SpaiSetMatrix": (clsparseStatus, [C.c_void_p, P(clsparseCsrMatrix), C.c_void_p]),
+    "clsparseB200SpaiParams": (clsparseStatus, [C.c_void_p, P(C.c_float), C.c_size_t, P(C.c_size_t), cl_int]),
+    "clsparseB200SpaiLossGrad": (clsparseStatus, [C.c_void_p, P(cldenseVector), cl_int, C.c_double, cl_int,
+                                                  P(C.c_double), P(C.c_float), C.c_size_t, C.c_void_p]),
+    "clsparseB200SpaiTrainStep": (clsparseStatus, [C.c_void_p, P(cldenseVector), cl_int, C.c_double, C.c_double,
+                                                   P(C.c_double), C.c_void_p]),
+    "clsparseB200SpaiBuild": (clsparseStatus, [C.c_void_p, C.c_void_p]),
+    "clsparseB200SpaiGetFactor": (clsparseStatus, [C.c_void_p, P(clsparseIdx_t), P(clsparseIdx_t), P(C.c_double),
+                                                   C.c_size_t, P(C.c_size_t)]),
+    "clsparseB200SpaiSave": (clsparseStatus, [C.c_void_p, C.c_char_p]),
+    "clsparseB200SpaiLoad": (clsparseStatus, [C.c_void_p, C.c_char_p]),
+    "clsparseDcsrcgLearned": (clsparseStatus, [P(cldenseVector), P(clsparseCsrMatrix), P(cldenseVector), C.c_void_p,
+                                               C.c_void_p, cl_int, C.c_double, P(clsparseB200MixedInfo), P(cl_int),
+                                               C.c_void_p]),
+})

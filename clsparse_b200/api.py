@@ -251,3 +251,95 @@ def cg_batched(x: torch.Tensor, A: CsrMatrix, b: torch.Tensor, offsets, sc: Solv
                                       C.byref(out), ctrl.handle), "clsparseScsrcgBatched")
     return {"iterations": iters, "residuals": res, "converged": out.systemsConverged,
             "max_iterations": out.maxIterations, "worst_residual": out.worstResidual}
+
+
+class Spai:
+    """The learned factorized sparse approximate inverse (clsparseB200Spai*)."""
+
+    def __init__(self, seed: int = 0):
+        h = C.c_void_p()
+        check(lib().clsparseB200SpaiCreate(C.byref(h), seed), "clsparseB200SpaiCreate")
+        self.handle = h
+
+    def set_matrix(self, A: CsrMatrix, ctrl: Control):
+        check(lib().clsparseB200SpaiSetMatrix(self.handle, C.byref(A.s), ctrl.handle), "clsparseB200SpaiSetMatrix")
+        self._A = A
+
+    def params(self) -> np.ndarray:
+        n = C.c_size_t()
+        check(lib().clsparseB200SpaiParams(self.handle, None, 0, C.byref(n), 0), "SpaiParams")
+        out = np.zeros(n.value, dtype=np.float32)
+        check(lib().clsparseB200SpaiParams(self.handle, out.ctypes.data_as(C.POINTER(C.c_float)), n.value,
+                                           C.byref(n), 0), "SpaiParams")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        n = C.c_size_t()
+        check(lib().clsparseB200SpaiParams(self.handle, p.ctypes.data_as(C.POINTER(C.c_float)), p.size,
+                                           C.byref(n), 1), "SpaiParams")
+
+    def _probes(self, probes):
+        if probes is None:
+            return None, 0
+        t = probes.reshape(-1).contiguous()
+        return C.byref(vector(t)), int(probes.shape[0])
+
+    def loss_grad(self, ctrl: Control, probes: torch.Tensor | None = None, lam: float = 0.0,
+                  fp32_weights: bool = False):
+        pv, K = self._probes(probes)
+        loss = C.c_double()
+        g = np.zeros(self.params().size, dtype=np.float32)
+        check(lib().clsparseB200SpaiLossGrad(self.handle, pv, K, lam, 1 if fp32_weights else 0, C.byref(loss),
+                                             g.ctypes.data_as(C.POINTER(C.c_float)), g.size, ctrl.handle),
+              "clsparseB200SpaiLossGrad")
+        return loss.value, g
+
+    def train_step(self, ctrl: Control, probes: torch.Tensor | None = None, lam: float = 0.0,
+                   lr: float = 1e-3) -> float:
+        pv, K = self._probes(probes)
+        loss = C.c_double()
+        check(lib().clsparseB200SpaiTrainStep(self.handle, pv, K, lam, lr, C.byref(loss), ctrl.handle),
+              "clsparseB200SpaiTrainStep")
+        return loss.value
+
+    def build(self, ctrl: Control):
+        check(lib().clsparseB200SpaiBuild(self.handle, ctrl.handle), "clsparseB200SpaiBuild")
+
+    def factor(self):
+        nnz = C.c_size_t()
+        check(lib().clsparseB200SpaiGetFactor(self.handle, None, None, None, 0, C.byref(nnz)), "GetFactor")
+        n = self._A.num_rows
+        rp = np.zeros(n + 1, dtype=np.uint32)
+        col = np.zeros(nnz.value, dtype=np.uint32)
+        val = np.zeros(nnz.value, dtype=np.float64)
+        check(lib().clsparseB200SpaiGetFactor(self.handle, rp.ctypes.data_as(C.POINTER(L.clsparseIdx_t)),
+                                              col.ctypes.data_as(C.POINTER(L.clsparseIdx_t)),
+                                              val.ctypes.data_as(C.POINTER(C.c_double)), nnz.value, C.byref(nnz)),
+              "GetFactor")
+        return rp, col, val
+
+    def save(self, path: str):
+        check(lib().clsparseB200SpaiSave(self.handle, str(path).encode()), "clsparseB200SpaiSave")
+
+    def load(self, path: str):
+        check(lib().clsparseB200SpaiLoad(self.handle, str(path).encode()), "clsparseB200SpaiLoad")
+
+    def release(self):
+        if self.handle:
+            check(lib().clsparseB200SpaiRelease(self.handle), "clsparseB200SpaiRelease")
+            self.handle = None
+
+
+def cg_learned(x: torch.Tensor, A: CsrMatrix, b: torch.Tensor, sc: SolverControl, spai: Spai, ctrl: Control,
+               inner: str = "fp32", inner_tol: float = 1e-3) -> dict:
+    """CG preconditioned with the learned G^T G (clsparseDcsrcgLearned)."""
+    info = L.clsparseB200MixedInfo()
+    fb = L.cl_int()
+    prec = {"fp32": 0, "bf16": 1, "fp64": 2}[inner]
+    check(lib().clsparseDcsrcgLearned(C.byref(vector(x)), C.byref(A.s), C.byref(vector(b)), sc.handle,
+                                      spai.handle, prec, inner_tol, C.byref(info), C.byref(fb), ctrl.handle),
+          "clsparseDcsrcgLearned")
+    out = {f[0]: getattr(info, f[0]) for f in info._fields_}
+    out["fell_back"] = fb.value
+    return out

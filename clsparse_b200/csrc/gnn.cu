@@ -1,0 +1,1081 @@
+// Learned factorized sparse approximate inverse (project extension, no
+// reference counterpart): a 4-layer message-passing network over the graph
+// of an SPD matrix A emits a lower-triangular G on the pattern of tril(A)
+// with a softplus-positive diagonal, so M^-1 = G^T G is SPD. The forward and
+// backward passes, the loss and the optimiser are the kernels of this file;
+// training runs on the GPU.
+//
+// Scaling: the network sees A_hat = D^-1/2 A D^-1/2 (unit diagonal) and emits
+// G_hat; the preconditioner factor is G = G_hat D^-1/2.
+//
+// Network (hidden width H = 64, message passing over the off-diagonal
+// pattern of A, which is symmetric):
+//   h0_i  = relu(W_in f_i + b_in)                 f_i = [1, sum_j|a_hat_ij|, deg_i/8, 0]
+//   layer l = 1..4:
+//     u_j  = U_l h_j
+//     s_i  = sum_{j != i} relu(u_j + a_hat_ij w_l + c_l)
+//     h_i <- h_i + relu(V_l [h_i ; s_i] + d_l)
+//   g_hat_ii = softplus(w_d . h_i + b_d)
+//   g_hat_ij = w_o . relu(P h_i + Q h_j + a_hat_ij r + t) + b_o   (j < i, a_ij != 0)
+// Weights are kept in FP32 for the optimiser and used as BF16 in the
+// forward and backward passes (products accumulated in FP32); a debug switch
+// uses the FP32 copies instead (gradient checks).
+//
+// Loss: the Kaporin condition-number bound of G_hat A_hat G_hat^T,
+//   L_K = log(tr(G_hat A_hat G_hat^T) / n) - (2/n) sum_i log g_hat_ii,
+// whose minimiser on a fixed pattern is the classical FSAI factor, plus
+// lambda times the mean over residual probes r (CG residual histories) of
+//   ||G_hat^T G_hat A_hat r - r||^2 / ||r||^2.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <initializer_list>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "device_common.cuh"
+#include "internal.h"
+
+namespace clsp {
+namespace gnn {
+
+constexpr int H = 64;      // hidden width
+constexpr int HO = 32;     // width of the edge output MLP
+constexpr int NF = 4;      // node input features
+constexpr int NL = 4;      // message-passing layers
+constexpr int kMaxP = 8;   // max entries per row of tril(A) handled by the loss
+
+// ---- flat parameter layout ----
+struct Offsets {
+    int w_in, b_in;
+    int U[NL], w[NL], c[NL], V[NL], d[NL];
+    int P, Q, r, t, w_o, b_o, w_d, b_d;
+    int total;
+};
+
+inline Offsets layout() {
+    Offsets o;
+    int k = 0;
+    auto take = [&](int n) {
+        const int s = k;
+        k += n;
+        return s;
+    };
+    o.w_in = take(H * NF);
+    o.b_in = take(H);
+    for (int l = 0; l < NL; ++l) {
+        o.U[l] = take(H * H);
+        o.w[l] = take(H);
+        o.c[l] = take(H);
+        o.V[l] = take(H * 2 * H);
+        o.d[l] = take(H);
+    }
+    o.P = take(HO * H);
+    o.Q = take(HO * H);
+    o.r = take(HO);
+    o.t = take(HO);
+    o.w_o = take(HO);
+    o.b_o = take(1);
+    o.w_d = take(H);
+    o.b_d = take(1);
+    o.total = k;
+    return o;
+}
+
+__device__ __forceinline__ float bfr(float v) {  // round a weight through BF16
+    return __bfloat162float(__float2bfloat16(v));
+}
+
+// Y[n x M] = act(X1 W1^T + X2 W2^T + b) (+ R), W = [W1 | W2] row-major M x (K1+K2).
+// act: 0 none, 1 relu. Rows tiled 32 per CTA; weights staged in shared memory.
+template <int M, int K1, int K2>
+__global__ void __launch_bounds__(256)
+    linear_fwd(const float* __restrict__ X1, const float* __restrict__ X2, const float* __restrict__ W,
+               const float* __restrict__ b, const float* __restrict__ R, float* __restrict__ Y,
+               float* __restrict__ A, size_t n, int act, int bf16) {
+    constexpr int K = K1 + K2;
+    constexpr int ROWS = 16;
+    __shared__ float sw[M * K];
+    __shared__ float sx[ROWS][K + 1];
+    for (int i = threadIdx.x; i < M * K; i += 256) sw[i] = bf16 ? bfr(W[i]) : W[i];
+    const size_t r0 = static_cast<size_t>(blockIdx.x) * ROWS;
+    for (int i = threadIdx.x; i < ROWS * K; i += 256) {
+        const int rr = i / K, kk = i % K;
+        const size_t row = r0 + rr;
+        float v = 0.f;
+        if (row < n) v = kk < K1 ? X1[row * K1 + kk] : X2[row * K2 + (kk - K1)];
+        sx[rr][kk] = v;
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < ROWS * M; o += 256) {
+        const int rr = o / M, m = o % M;
+        const size_t row = r0 + rr;
+        if (row >= n) continue;
+        float z = b ? b[m] : 0.f;
+#pragma unroll 8
+        for (int kk = 0; kk < K; ++kk) z = fmaf(sx[rr][kk], sw[m * K + kk], z);
+        const float a = act ? fmaxf(z, 0.f) : z;
+        if (A) A[row * M + m] = a;
+        Y[row * M + m] = R ? R[row * M + m] + a : a;
+    }
+}
+
+// Backward of linear_fwd. dZ = dY * act'(A); dX1 += dZ W1, dX2 += dZ W2 (when
+// given); per-CTA partial sums of dW (M x K) and db (M) go to `part` at
+// blockIdx * (M*K + M).
+template <int M, int K1, int K2>
+__global__ void __launch_bounds__(256)
+    linear_bwd(const float* __restrict__ X1, const float* __restrict__ X2, const float* __restrict__ W,
+               const float* __restrict__ A, const float* __restrict__ dY, float* __restrict__ dX1,
+               float* __restrict__ dX2, float* __restrict__ part, size_t n, int act, int bf16) {
+    constexpr int K = K1 + K2;
+    constexpr int ROWS = 16;
+    __shared__ float sw[M * K];
+    __shared__ float sx[ROWS][K + 1];
+    __shared__ float sdz[ROWS][M + 1];
+    for (int i = threadIdx.x; i < M * K; i += 256) sw[i] = bf16 ? bfr(W[i]) : W[i];
+    const size_t r0 = static_cast<size_t>(blockIdx.x) * ROWS;
+    for (int i = threadIdx.x; i < ROWS * K; i += 256) {
+        const int rr = i / K, kk = i % K;
+        const size_t row = r0 + rr;
+        float v = 0.f;
+        if (row < n) v = kk < K1 ? X1[row * K1 + kk] : X2[row * K2 + (kk - K1)];
+        sx[rr][kk] = v;
+    }
+    for (int i = threadIdx.x; i < ROWS * M; i += 256) {
+        const int rr = i / M, m = i % M;
+        const size_t row = r0 + rr;
+        float dz = 0.f;
+        if (row < n) {
+            dz = dY[row * M + m];
+            if (act && !(A[row * M + m] > 0.f)) dz = 0.f;
+        }
+        sdz[rr][m] = dz;
+    }
+    __syncthreads();
+    // input gradients
+    for (int i = threadIdx.x; i < ROWS * K; i += 256) {
+        const int rr = i / K, kk = i % K;
+        const size_t row = r0 + rr;
+        if (row >= n) continue;
+        float g = 0.f;
+#pragma unroll 8
+        for (int m = 0; m < M; ++m) g = fmaf(sdz[rr][m], sw[m * K + kk], g);
+        if (kk < K1) {
+            if (dX1) dX1[row * K1 + kk] += g;
+        } else {
+            if (dX2) dX2[row * K2 + (kk - K1)] += g;
+        }
+    }
+    // weight gradients of this tile
+    float* pw = part + static_cast<size_t>(blockIdx.x) * (M * K + M);
+    for (int i = threadIdx.x; i < M * K; i += 256) {
+        const int m = i / K, kk = i % K;
+        float g = 0.f;
+        for (int rr = 0; rr < ROWS; ++rr) g = fmaf(sdz[rr][m], sx[rr][kk], g);
+        pw[i] = g;
+    }
+    for (int m = threadIdx.x; m < M; m += 256) {
+        float g = 0.f;
+        for (int rr = 0; rr < ROWS; ++rr) g += sdz[rr][m];
+        pw[M * K + m] = g;
+    }
+}
+
+// grad[off + i] += sum over `ntiles` partial records (fixed order).
+__global__ void reduce_parts(const float* __restrict__ part, int rec, int ntiles, float* __restrict__ grad,
+                             int off_w, int off_b, int nw) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rec) return;
+    double s = 0.0;
+    for (int k = 0; k < ntiles; ++k) s += part[static_cast<size_t>(k) * rec + i];
+    if (i < nw)
+        grad[off_w + i] += static_cast<float>(s);
+    else if (off_b >= 0)
+        grad[off_b + (i - nw)] += static_cast<float>(s);
+}
+
+// One warp per receiving node i: S_i = sum_{j in row i, j != i} relu(Hu_j + e_ij w + c).
+__global__ void message_fwd(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols,
+                            const float* __restrict__ ehat, const float* __restrict__ Hu,
+                            const float* __restrict__ w, const float* __restrict__ c, float* __restrict__ S,
+                            uint32_t n, int bf16) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const int f0 = lane, f1 = lane + 32;
+    const float w0 = bf16 ? bfr(w[f0]) : w[f0], w1 = bf16 ? bfr(w[f1]) : w[f1];
+    const float c0 = bf16 ? bfr(c[f0]) : c[f0], c1 = bf16 ? bfr(c[f1]) : c[f1];
+    float s0 = 0.f, s1 = 0.f;
+    for (uint32_t k = rp[warp]; k < rp[warp + 1]; ++k) {
+        const uint32_t j = cols[k];
+        if (j == warp) continue;
+        const float e = ehat[k];
+        s0 += fmaxf(Hu[static_cast<size_t>(j) * H + f0] + e * w0 + c0, 0.f);
+        s1 += fmaxf(Hu[static_cast<size_t>(j) * H + f1] + e * w1 + c1, 0.f);
+    }
+    S[static_cast<size_t>(warp) * H + f0] = s0;
+    S[static_cast<size_t>(warp) * H + f1] = s1;
+}
+
+// Backward of message_fwd, one warp per sending node j (the pattern is
+// symmetric, so row j lists the receivers i and e_ji = e_ij):
+// dHu_j = sum_i dS_i * [Hu_j + e_ij w + c > 0]; partial dw, dc per warp into
+// part[warp * 2H].
+__global__ void message_bwd(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols,
+                            const float* __restrict__ ehat, const float* __restrict__ Hu,
+                            const float* __restrict__ w, const float* __restrict__ c,
+                            const float* __restrict__ dS, float* __restrict__ dHu, float* __restrict__ part,
+                            uint32_t n, int bf16) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const int f0 = lane, f1 = lane + 32;
+    const float w0 = bf16 ? bfr(w[f0]) : w[f0], w1 = bf16 ? bfr(w[f1]) : w[f1];
+    const float c0 = bf16 ? bfr(c[f0]) : c[f0], c1 = bf16 ? bfr(c[f1]) : c[f1];
+    const float u0 = Hu[static_cast<size_t>(warp) * H + f0], u1 = Hu[static_cast<size_t>(warp) * H + f1];
+    float g0 = 0.f, g1 = 0.f, dw0 = 0.f, dw1 = 0.f, dc0 = 0.f, dc1 = 0.f;
+    for (uint32_t k = rp[warp]; k < rp[warp + 1]; ++k) {
+        const uint32_t i = cols[k];
+        if (i == warp) continue;
+        const float e = ehat[k];
+        const float d0 = (u0 + e * w0 + c0 > 0.f) ? dS[static_cast<size_t>(i) * H + f0] : 0.f;
+        const float d1 = (u1 + e * w1 + c1 > 0.f) ? dS[static_cast<size_t>(i) * H + f1] : 0.f;
+        g0 += d0;
+        g1 += d1;
+        dw0 += d0 * e;
+        dw1 += d1 * e;
+        dc0 += d0;
+        dc1 += d1;
+    }
+    dHu[static_cast<size_t>(warp) * H + f0] = g0;
+    dHu[static_cast<size_t>(warp) * H + f1] = g1;
+    float* p = part + static_cast<size_t>(warp) * 2 * H;
+    p[f0] = dw0;
+    p[f1] = dw1;
+    p[H + f0] = dc0;
+    p[H + f1] = dc1;
+}
+
+__device__ __forceinline__ float softplus(float z) { return z > 20.f ? z : log1pf(expf(z)); }
+__device__ __forceinline__ float sigmoid(float z) { return 1.f / (1.f + expf(-z)); }
+
+// Output layer, one warp per row i of L = tril(A) (lane = output unit o < 32):
+// g_ii = softplus(w_d . h_i + b_d); g_ij = w_o . relu(Hp_i + Hq_j + e r + t) + b_o.
+__global__ void output_fwd(const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lcol,
+                           const float* __restrict__ Le, const float* __restrict__ Hh,
+                           const float* __restrict__ Hp, const float* __restrict__ Hq,
+                           const float* __restrict__ prm, Offsets o, float* __restrict__ g, uint32_t n,
+                           int bf16) {
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    auto W = [&](int k) { return bf16 ? bfr(prm[k]) : prm[k]; };
+    const float rr = W(o.r + lane), tt = W(o.t + lane), wo = W(o.w_o + lane), bo = W(o.b_o);
+    const float hp = Hp[static_cast<size_t>(i) * HO + lane];
+    for (uint32_t k = Lrp[i]; k < Lrp[i + 1]; ++k) {
+        const uint32_t j = Lcol[k];
+        float val;
+        if (j == i) {
+            float z = W(o.w_d + lane) * Hh[static_cast<size_t>(i) * H + lane] +
+                      W(o.w_d + lane + 32) * Hh[static_cast<size_t>(i) * H + lane + 32];
+            z = dev::warp_sum(z) + W(o.b_d);
+            val = softplus(z);
+        } else {
+            const float pre = hp + Hq[static_cast<size_t>(j) * HO + lane] + Le[k] * rr + tt;
+            val = dev::warp_sum(wo * fmaxf(pre, 0.f)) + bo;
+        }
+        if (lane == 0) g[k] = val;
+    }
+}
+
+// Backward of output_fwd over rows i: dh_i (diagonal part), dHp_i, and the
+// per-warp partial parameter gradients [r, t, w_o, b_o, w_d(64), b_d].
+constexpr int kOutPart = HO * 3 + 1 + H + 1;
+__global__ void output_bwd_rows(const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lcol,
+                                const float* __restrict__ Le, const float* __restrict__ Hh,
+                                const float* __restrict__ Hp, const float* __restrict__ Hq,
+                                const float* __restrict__ prm, Offsets o, const float* __restrict__ dg,
+                                float* __restrict__ dH, float* __restrict__ dHp, float* __restrict__ part,
+                                uint32_t n, int bf16) {
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    auto W = [&](int k) { return bf16 ? bfr(prm[k]) : prm[k]; };
+    const float rr = W(o.r + lane), tt = W(o.t + lane), wo = W(o.w_o + lane);
+    const float hp = Hp[static_cast<size_t>(i) * HO + lane];
+    float dhp = 0.f, dr = 0.f, dt = 0.f, dwo = 0.f, dbo = 0.f, dwd0 = 0.f, dwd1 = 0.f, dbd = 0.f, dh0 = 0.f,
+          dh1 = 0.f;
+    const float h0 = Hh[static_cast<size_t>(i) * H + lane], h1 = Hh[static_cast<size_t>(i) * H + lane + 32];
+    for (uint32_t k = Lrp[i]; k < Lrp[i + 1]; ++k) {
+        const uint32_t j = Lcol[k];
+        const float d = dg[k];
+        if (j == i) {
+            const float wd0 = W(o.w_d + lane), wd1 = W(o.w_d + lane + 32);
+            const float z = dev::warp_sum(wd0 * h0 + wd1 * h1) + W(o.b_d);
+            const float dz = d * sigmoid(z);
+            dh0 += dz * wd0;
+            dh1 += dz * wd1;
+            dwd0 += dz * h0;
+            dwd1 += dz * h1;
+            dbd += dz;
+        } else {
+            const float pre = hp + Hq[static_cast<size_t>(j) * HO + lane] + Le[k] * rr + tt;
+            const float a = fmaxf(pre, 0.f);
+            dwo += d * a;
+            dbo += d;
+            const float dp = pre > 0.f ? d * wo : 0.f;
+            dhp += dp;
+            dr += dp * Le[k];
+            dt += dp;
+        }
+    }
+    dHp[static_cast<size_t>(i) * HO + lane] = dhp;
+    dH[static_cast<size_t>(i) * H + lane] += dh0;
+    dH[static_cast<size_t>(i) * H + lane + 32] += dh1;
+    float* p = part + static_cast<size_t>(i) * kOutPart;
+    p[lane] = dr;
+    p[HO + lane] = dt;
+    p[2 * HO + lane] = dwo;
+    if (lane == 0) p[3 * HO] = dbo;  // lanes agree on dbo
+    p[3 * HO + 1 + lane] = dwd0;
+    p[3 * HO + 1 + lane + 32] = dwd1;
+    if (lane == 0) p[3 * HO + 1 + H] = dbd;
+}
+
+// dHq_j = sum over rows i > j of L holding (i, j): dg_ij w_o [pre_ij > 0],
+// gathered through the transposed pattern (LTrp, LTrow, LTidx -> entry of L).
+__global__ void output_bwd_cols(const uint32_t* __restrict__ LTrp, const uint32_t* __restrict__ LTrow,
+                                const uint32_t* __restrict__ LTidx, const float* __restrict__ Le,
+                                const float* __restrict__ Hp, const float* __restrict__ Hq,
+                                const float* __restrict__ prm, Offsets o, const float* __restrict__ dg,
+                                float* __restrict__ dHq, uint32_t n, int bf16) {
+    const uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (j >= n) return;
+    auto W = [&](int k) { return bf16 ? bfr(prm[k]) : prm[k]; };
+    const float rr = W(o.r + lane), tt = W(o.t + lane), wo = W(o.w_o + lane);
+    const float hq = Hq[static_cast<size_t>(j) * HO + lane];
+    float acc = 0.f;
+    for (uint32_t k = LTrp[j]; k < LTrp[j + 1]; ++k) {
+        const uint32_t i = LTrow[k];
+        if (i == j) continue;
+        const uint32_t e = LTidx[k];
+        const float pre = Hp[static_cast<size_t>(i) * HO + lane] + hq + Le[e] * rr + tt;
+        if (pre > 0.f) acc += dg[e] * wo;
+    }
+    dHq[static_cast<size_t>(j) * HO + lane] = acc;
+}
+
+// Kaporin loss, pass 1: per row tr_i = g_i^T B_i g_i and log g_ii; grid sums.
+__global__ void kaporin_sum(const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Boff,
+                            const float* __restrict__ B, const float* __restrict__ g, uint32_t n,
+                            double* parts, uint32_t* ticket, double* out) {
+    double acc[2] = {0.0, 0.0};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t k0 = Lrp[i], m = Lrp[i + 1] - k0;
+        const float* Bi = B + Boff[i];
+        double t = 0.0;
+        for (uint32_t a = 0; a < m; ++a) {
+            double s = 0.0;
+            for (uint32_t c = 0; c < m; ++c) s += static_cast<double>(Bi[a * m + c]) * g[k0 + c];
+            t += s * g[k0 + a];
+        }
+        acc[0] += t;
+        acc[1] += log(static_cast<double>(g[k0 + m - 1]));  // diagonal is last (sorted columns)
+    }
+    double tot[2];
+    if (dev::grid_reduce_last<2>(acc, parts, ticket, tot) && threadIdx.x == 0) {
+        out[0] = tot[0];
+        out[1] = tot[1];
+    }
+}
+
+// Kaporin loss, pass 2: dL/dg_i = (2/tr) B_i g_i - (2/n)/g_ii on the diagonal.
+__global__ void kaporin_grad(const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Boff,
+                             const float* __restrict__ B, const float* __restrict__ g, uint32_t n,
+                             const double* sums, float* __restrict__ dg) {
+    const double tr = sums[0];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t k0 = Lrp[i], m = Lrp[i + 1] - k0;
+        const float* Bi = B + Boff[i];
+        for (uint32_t a = 0; a < m; ++a) {
+            double s = 0.0;
+            for (uint32_t c = 0; c < m; ++c) s += static_cast<double>(Bi[a * m + c]) * g[k0 + c];
+            double d = 2.0 * s / tr;
+            if (a == m - 1) d -= 2.0 / (static_cast<double>(n) * g[k0 + a]);
+            dg[k0 + a] = static_cast<float>(d);
+        }
+    }
+}
+
+// y = G v (rows of L) or y = G^T v (rows of L^T); warp per row, FP32.
+__global__ void lspmv(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ idx,
+                      const uint32_t* __restrict__ vidx, const float* __restrict__ g,
+                      const float* __restrict__ v, float* __restrict__ y, uint32_t n) {
+    const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    float s = 0.f;
+    for (uint32_t k = rp[row] + lane; k < rp[row + 1]; k += 32) s += g[vidx ? vidx[k] : k] * v[idx[k]];
+    s = dev::warp_sum(s);
+    if (lane == 0) y[row] = s;
+}
+
+// y = A_hat v with the scaled values (ehat) on A's pattern (diagonal = 1).
+__global__ void ahat_spmv(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols,
+                          const float* __restrict__ ehat, const float* __restrict__ v, float* __restrict__ y,
+                          uint32_t n) {
+    const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    float s = 0.f;
+    for (uint32_t k = rp[row] + lane; k < rp[row + 1]; k += 32) s += ehat[k] * v[cols[k]];
+    s = dev::warp_sum(s);
+    if (lane == 0) y[row] = s;
+}
+
+// Probe loss pieces. res = v - r scaled: dv = coef * (v - r), and the sum of
+// (v - r)^2 / ||r||^2 goes to `out` through a grid sum.
+__global__ void probe_residual(const float* __restrict__ v, const float* __restrict__ r, float coef,
+                               float inv_rr, float* __restrict__ dv, uint32_t n, double* parts,
+                               uint32_t* ticket, double* out) {
+    double acc[1] = {0.0};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float d = v[i] - r[i];
+        dv[i] = coef * d;
+        acc[0] += static_cast<double>(d) * d * inv_rr;
+    }
+    double tot[1];
+    if (dev::grid_reduce_last<1>(acc, parts, ticket, tot) && threadIdx.x == 0) out[0] += tot[0];
+}
+
+// dg_ij += dv_j u_i + du_i w_j over the entries of L.
+__global__ void probe_grad(const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lcol,
+                           const float* __restrict__ dv, const float* __restrict__ u,
+                           const float* __restrict__ du, const float* __restrict__ w, float* __restrict__ dg,
+                           uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (uint32_t k = Lrp[i]; k < Lrp[i + 1]; ++k) {
+            const uint32_t j = Lcol[k];
+            dg[k] += dv[j] * u[i] + du[i] * w[j];
+        }
+}
+
+__global__ void adam_step(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                          float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1,
+                          float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// G values for the solver: g_ij = g_hat_ij / sqrt(a_jj) in L order, as FP32,
+// BF16 and FP64.
+__global__ void export_factor(const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lcol,
+                              const float* __restrict__ ghat, const double* __restrict__ dinvs,
+                              float* __restrict__ G32, __nv_bfloat16* __restrict__ G16,
+                              double* __restrict__ G64, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (uint32_t k = Lrp[i]; k < Lrp[i + 1]; ++k) {
+            const double v = static_cast<double>(ghat[k]) * dinvs[Lcol[k]];
+            G32[k] = static_cast<float>(v);
+            G16[k] = __double2bfloat16(v);
+            G64[k] = v;
+        }
+}
+
+// The same values in L^T order (rows of G^T).
+__global__ void gather_transpose(const uint32_t* __restrict__ LTidx, const float* __restrict__ G32,
+                                 const __nv_bfloat16* __restrict__ G16, const double* __restrict__ G64,
+                                 float* __restrict__ GT32, __nv_bfloat16* __restrict__ GT16,
+                                 double* __restrict__ GT64, uint32_t nnzL) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nnzL; k += gridDim.x * blockDim.x) {
+        const uint32_t s = LTidx[k];
+        GT32[k] = G32[s];
+        GT16[k] = G16[s];
+        GT64[k] = G64[s];
+    }
+}
+
+// node features f = [1, sum_{j != i} |a_hat_ij|, deg_i / 8, 0]
+__global__ void node_features(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols,
+                              const float* __restrict__ ehat, float* __restrict__ F, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float s = 0.f;
+        uint32_t deg = 0;
+        for (uint32_t k = rp[i]; k < rp[i + 1]; ++k)
+            if (cols[k] != i) {
+                s += fabsf(ehat[k]);
+                ++deg;
+            }
+        F[static_cast<size_t>(i) * NF + 0] = 1.f;
+        F[static_cast<size_t>(i) * NF + 1] = s;
+        F[static_cast<size_t>(i) * NF + 2] = deg * 0.125f;
+        F[static_cast<size_t>(i) * NF + 3] = 0.f;
+    }
+}
+
+// ------------------------------------------------------------- host side
+
+constexpr int kRows = 16;  // rows per CTA of linear_fwd / linear_bwd
+
+uint32_t nblk(size_t n, int per) { return static_cast<uint32_t>((n + per - 1) / per); }
+uint32_t warps_grid(size_t n) { return static_cast<uint32_t>((n * 32 + 255) / 256); }
+
+template <typename P>
+cudaError_t dalloc(P*& p, size_t count) {
+    return cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(P) + 16);
+}
+
+uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934665603ull) {
+    const unsigned char* c = static_cast<const unsigned char*>(data);
+    for (size_t i = 0; i < bytes; ++i) {
+        h ^= c[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+// Graph of one matrix: A's pattern with scaled values, L = tril(A), L^T,
+// the local blocks of the loss, and the exported factor.
+struct Graph {
+    uint32_t n = 0, nnz = 0, nnzL = 0;
+    size_t nB = 0;
+    const uint32_t* rp = nullptr;   // A's arrays (user memory)
+    const uint32_t* cols = nullptr;
+    float* ehat = nullptr;          // a_hat on A's pattern
+    double* dinvs = nullptr;        // 1 / sqrt(a_ii)
+    uint32_t *Lrp = nullptr, *Lcol = nullptr;
+    float* Le = nullptr;
+    uint32_t *LTrp = nullptr, *LTrow = nullptr, *LTidx = nullptr;
+    uint32_t* Boff = nullptr;
+    float* B = nullptr;
+    float* F = nullptr;
+    // activations
+    float* Hs[NL + 1] = {};
+    float *Hu[NL] = {}, *S[NL] = {}, *Au[NL] = {};
+    float *Hp = nullptr, *Hq = nullptr, *g = nullptr, *dg = nullptr;
+    float *dH = nullptr, *dHn = nullptr, *dS = nullptr, *dHu = nullptr, *dHp = nullptr, *dHq = nullptr;
+    float* part = nullptr;
+    size_t part_floats = 0;
+    float *pw = nullptr, *pu = nullptr, *pv = nullptr, *pdv = nullptr, *pdu = nullptr;
+    double* red = nullptr;  // [0..3] results, [8..] partials
+    uint32_t* ticket = nullptr;
+    // exported factor (L order) and its transpose (L^T order)
+    float *G32 = nullptr, *GT32 = nullptr;
+    __nv_bfloat16 *G16 = nullptr, *GT16 = nullptr;
+    double *G64 = nullptr, *GT64 = nullptr;
+    bool built = false;
+    int device = 0;
+
+    void release() {
+        void* ptrs[] = {ehat, dinvs, Lrp, Lcol, Le, LTrp, LTrow, LTidx, Boff, B, F, Hp, Hq, g, dg, dH, dHn, dS,
+                        dHu, dHp, dHq, part, pw, pu, pv, pdv, pdu, red, ticket, G32, GT32, G16, GT16, G64, GT64};
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+        for (int l = 0; l <= NL; ++l)
+            if (Hs[l]) cudaFree(Hs[l]);
+        for (int l = 0; l < NL; ++l) {
+            if (Hu[l]) cudaFree(Hu[l]);
+            if (S[l]) cudaFree(S[l]);
+            if (Au[l]) cudaFree(Au[l]);
+        }
+        *this = Graph();
+    }
+};
+
+}  // namespace gnn
+}  // namespace clsp
+
+using namespace clsp;
+using namespace clsp::gnn;
+
+// The learned preconditioner object: network parameters, optimiser state and
+// the graph of the matrix it was last set to.
+struct _clsparseB200Spai {
+    Offsets o;
+    float* prm = nullptr;   // FP32 master weights
+    float* grad = nullptr;
+    float* m = nullptr;
+    float* v = nullptr;
+    int step = 0;
+    int device = 0;
+    Graph gr;
+    ~_clsparseB200Spai() {
+        gr.release();
+        if (prm) cudaFree(prm);
+        if (grad) cudaFree(grad);
+        if (m) cudaFree(m);
+        if (v) cudaFree(v);
+    }
+};
+
+namespace {
+
+// Builds the graph structures of an SPD matrix A (FP64 values, sorted
+// columns, every diagonal present, at most kMaxP entries per row of tril(A)).
+clsparseStatus build_graph(_clsparseB200Spai* net, const clsparseCsrMatrix* A, clsparseControl c) {
+    Graph& gr = net->gr;
+    gr.release();
+    const uint32_t n = A->num_rows, nnz = A->num_nonzeros;
+    std::vector<uint32_t> rp(n + 1), cols(nnz);
+    std::vector<double> vals(nnz);
+    cudaStream_t s = c->stream;
+    cudaMemcpyAsync(rp.data(), dev_ptr<const uint32_t>(A->row_pointer, A->off_row_pointer), (n + 1) * 4,
+                    cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(cols.data(), dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices), size_t(nnz) * 4,
+                    cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(vals.data(), dev_ptr<const double>(A->values, A->off_values), size_t(nnz) * 8,
+                    cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return clsparseInvalidMemObject;
+    const uint32_t base = rp[0];
+    std::vector<double> dinv(n, 0.0);
+    for (uint32_t i = 0; i < n; ++i) {
+        for (uint32_t k = rp[i]; k < rp[i + 1]; ++k)
+            if (cols[k - base] == i) dinv[i] = vals[k - base];
+        if (!(dinv[i] > 0.0)) return clsparseInvalidValue;  // not SPD (missing or non-positive diagonal)
+        dinv[i] = 1.0 / std::sqrt(dinv[i]);
+    }
+    std::vector<float> ehat(nnz);
+    std::vector<uint32_t> Lrp(n + 1, 0), Lcol, Lsrc;
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t prev = 0;
+        bool first = true;
+        for (uint32_t k = rp[i]; k < rp[i + 1]; ++k) {
+            const uint32_t j = cols[k - base];
+            if (j >= n) return clsparseInvalidValue;
+            if (!first && j <= prev) return clsparseInvalidValue;  // columns must be sorted, unique
+            first = false;
+            prev = j;
+            ehat[k - base] = static_cast<float>(vals[k - base] * dinv[i] * dinv[j]);
+            if (j <= i) {
+                Lcol.push_back(j);
+                Lsrc.push_back(k - base);
+            }
+        }
+        Lrp[i + 1] = static_cast<uint32_t>(Lcol.size());
+        if (Lrp[i + 1] - Lrp[i] > static_cast<uint32_t>(kMaxP)) return clsparseInvalidValue;
+        if (Lrp[i + 1] == Lrp[i] || Lcol.back() != i) return clsparseInvalidValue;
+    }
+    const uint32_t nnzL = Lrp[n];
+    std::vector<float> Le(nnzL);
+    for (uint32_t k = 0; k < nnzL; ++k) Le[k] = ehat[Lsrc[k]];
+    // transpose of L
+    std::vector<uint32_t> LTrp(n + 1, 0), LTrow(nnzL), LTidx(nnzL);
+    for (uint32_t k = 0; k < nnzL; ++k) ++LTrp[Lcol[k] + 1];
+    for (uint32_t j = 0; j < n; ++j) LTrp[j + 1] += LTrp[j];
+    {
+        std::vector<uint32_t> fill(LTrp.begin(), LTrp.end() - 1);
+        for (uint32_t i = 0; i < n; ++i)
+            for (uint32_t k = Lrp[i]; k < Lrp[i + 1]; ++k) {
+                const uint32_t pos = fill[Lcol[k]]++;
+                LTrow[pos] = i;
+                LTidx[pos] = k;
+            }
+    }
+    // local blocks B_i = A_hat[P_i, P_i]
+    std::vector<uint32_t> Boff(n + 1, 0);
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t m = Lrp[i + 1] - Lrp[i];
+        Boff[i + 1] = Boff[i] + m * m;
+    }
+    std::vector<float> B(Boff[n]);
+    auto ahat_at = [&](uint32_t r, uint32_t col) -> float {
+        uint32_t lo = rp[r] - base, hi = rp[r + 1] - base;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (cols[mid] < col)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        return (lo < rp[r + 1] - base && cols[lo] == col) ? ehat[lo] : 0.f;
+    };
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t k0 = Lrp[i], m = Lrp[i + 1] - k0;
+        for (uint32_t a = 0; a < m; ++a)
+            for (uint32_t b2 = 0; b2 < m; ++b2) B[Boff[i] + a * m + b2] = ahat_at(Lcol[k0 + a], Lcol[k0 + b2]);
+    }
+
+    gr.n = n;
+    gr.nnz = nnz;
+    gr.nnzL = nnzL;
+    gr.nB = Boff[n];
+    gr.rp = dev_ptr<const uint32_t>(A->row_pointer, A->off_row_pointer);
+    gr.cols = dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices);
+    gr.device = c->device;
+    bool ok = dalloc(gr.ehat, nnz) == cudaSuccess && dalloc(gr.dinvs, n) == cudaSuccess &&
+              dalloc(gr.Lrp, n + 1) == cudaSuccess && dalloc(gr.Lcol, nnzL) == cudaSuccess &&
+              dalloc(gr.Le, nnzL) == cudaSuccess && dalloc(gr.LTrp, n + 1) == cudaSuccess &&
+              dalloc(gr.LTrow, nnzL) == cudaSuccess && dalloc(gr.LTidx, nnzL) == cudaSuccess &&
+              dalloc(gr.Boff, n + 1) == cudaSuccess && dalloc(gr.B, gr.nB) == cudaSuccess &&
+              dalloc(gr.F, size_t(n) * NF) == cudaSuccess;
+    const size_t nh = size_t(n) * H, nho = size_t(n) * HO;
+    for (int l = 0; l <= NL && ok; ++l) ok = dalloc(gr.Hs[l], nh) == cudaSuccess;
+    for (int l = 0; l < NL && ok; ++l)
+        ok = dalloc(gr.Hu[l], nh) == cudaSuccess && dalloc(gr.S[l], nh) == cudaSuccess &&
+             dalloc(gr.Au[l], nh) == cudaSuccess;
+    const size_t tiles = nblk(n, kRows);
+    gr.part_floats = std::max({tiles * size_t(H * 2 * H + H), size_t(n) * 2 * H, size_t(n) * kOutPart});
+    ok = ok && dalloc(gr.Hp, nho) == cudaSuccess && dalloc(gr.Hq, nho) == cudaSuccess &&
+         dalloc(gr.g, nnzL) == cudaSuccess && dalloc(gr.dg, nnzL) == cudaSuccess &&
+         dalloc(gr.dH, nh) == cudaSuccess && dalloc(gr.dHn, nh) == cudaSuccess &&
+         dalloc(gr.dS, nh) == cudaSuccess && dalloc(gr.dHu, nh) == cudaSuccess &&
+         dalloc(gr.dHp, nho) == cudaSuccess && dalloc(gr.dHq, nho) == cudaSuccess &&
+         dalloc(gr.part, gr.part_floats) == cudaSuccess && dalloc(gr.pw, n) == cudaSuccess &&
+         dalloc(gr.pu, n) == cudaSuccess && dalloc(gr.pv, n) == cudaSuccess &&
+         dalloc(gr.pdv, n) == cudaSuccess && dalloc(gr.pdu, n) == cudaSuccess &&
+         dalloc(gr.red, 8 + 2 * kMaxReduceCtas) == cudaSuccess && dalloc(gr.ticket, 4) == cudaSuccess &&
+         dalloc(gr.G32, nnzL) == cudaSuccess && dalloc(gr.GT32, nnzL) == cudaSuccess &&
+         dalloc(gr.G16, nnzL) == cudaSuccess && dalloc(gr.GT16, nnzL) == cudaSuccess &&
+         dalloc(gr.G64, nnzL) == cudaSuccess && dalloc(gr.GT64, nnzL) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        gr.release();
+        return clsparseOutOfResources;
+    }
+    cudaMemcpyAsync(gr.ehat, ehat.data(), size_t(nnz) * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(gr.dinvs, dinv.data(), size_t(n) * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(gr.Lrp, Lrp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(gr.Lcol, Lcol.data(), size_t(nnzL) * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(gr.Le, Le.data(), size_t(nnzL) * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(gr.LTrp, LTrp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(gr.LTrow, LTrow.data(), size_t(nnzL) * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(gr.LTidx, LTidx.data(), size_t(nnzL) * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(gr.Boff, Boff.data(), (n + 1) * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(gr.B, B.data(), gr.nB * 4, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(gr.ticket, 0, 16, s);
+    node_features<<<nblk(n, 256), 256, 0, s>>>(gr.rp, gr.cols, gr.ehat, gr.F, n);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return clsparseInvalidKernelExecution;
+    gr.built = true;
+    return clsparseSuccess;
+}
+
+void forward(_clsparseB200Spai* net, int bf16, cudaStream_t s) {
+    Graph& gr = net->gr;
+    const Offsets& o = net->o;
+    const float* P = net->prm;
+    const size_t n = gr.n;
+    const uint32_t tiles = nblk(n, kRows);
+    linear_fwd<H, NF, 0><<<tiles, 256, 0, s>>>(gr.F, nullptr, P + o.w_in, P + o.b_in, nullptr, gr.Hs[0],
+                                                nullptr, n, 1, bf16);
+    for (int l = 0; l < NL; ++l) {
+        linear_fwd<H, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[l], nullptr, P + o.U[l], nullptr, nullptr, gr.Hu[l],
+                                                  nullptr, n, 0, bf16);
+        message_fwd<<<warps_grid(n), 256, 0, s>>>(gr.rp, gr.cols, gr.ehat, gr.Hu[l], P + o.w[l], P + o.c[l],
+                                                  gr.S[l], gr.n, bf16);
+        linear_fwd<H, H, H><<<tiles, 256, 0, s>>>(gr.Hs[l], gr.S[l], P + o.V[l], P + o.d[l], gr.Hs[l],
+                                                  gr.Hs[l + 1], gr.Au[l], n, 1, bf16);
+    }
+    linear_fwd<HO, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[NL], nullptr, P + o.P, nullptr, nullptr, gr.Hp, nullptr,
+                                               n, 0, bf16);
+    linear_fwd<HO, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[NL], nullptr, P + o.Q, nullptr, nullptr, gr.Hq, nullptr,
+                                               n, 0, bf16);
+    output_fwd<<<warps_grid(n), 256, 0, s>>>(gr.Lrp, gr.Lcol, gr.Le, gr.Hs[NL], gr.Hp, gr.Hq, P, o, gr.g,
+                                             gr.n, bf16);
+}
+
+// Loss and dL/dg; returns the loss (host sync).
+double loss_and_dg(_clsparseB200Spai* net, const float* probes, int K, double lambda, cudaStream_t s) {
+    Graph& gr = net->gr;
+    const uint32_t n = gr.n;
+    double* parts = gr.red + 8;
+    const uint32_t rg = std::min<uint32_t>(nblk(n, 256), 1024);
+    kaporin_sum<<<rg, 256, 0, s>>>(gr.Lrp, gr.Boff, gr.B, gr.g, n, parts, gr.ticket, gr.red);
+    kaporin_grad<<<rg, 256, 0, s>>>(gr.Lrp, gr.Boff, gr.B, gr.g, n, gr.red, gr.dg);
+    cudaMemsetAsync(gr.red + 2, 0, sizeof(double), s);
+    std::vector<double> rnorm(K, 0.0);
+    if (K > 0 && lambda > 0.0) {
+        // host norms of the probes (small K)
+        std::vector<float> hp(size_t(n) * K);
+        cudaMemcpyAsync(hp.data(), probes, hp.size() * 4, cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        for (int k = 0; k < K; ++k) {
+            double a = 0.0;
+            for (uint32_t i = 0; i < n; ++i) a += double(hp[size_t(k) * n + i]) * hp[size_t(k) * n + i];
+            rnorm[k] = a;
+        }
+        for (int k = 0; k < K; ++k) {
+            if (!(rnorm[k] > 0.0)) continue;
+            const float* r = probes + size_t(k) * n;
+            ahat_spmv<<<warps_grid(n), 256, 0, s>>>(gr.rp, gr.cols, gr.ehat, r, gr.pw, n);
+            lspmv<<<warps_grid(n), 256, 0, s>>>(gr.Lrp, gr.Lcol, nullptr, gr.g, gr.pw, gr.pu, n);
+            lspmv<<<warps_grid(n), 256, 0, s>>>(gr.LTrp, gr.LTrow, gr.LTidx, gr.g, gr.pu, gr.pv, n);
+            const float coef = static_cast<float>(2.0 * lambda / (K * rnorm[k]));
+            probe_residual<<<rg, 256, 0, s>>>(gr.pv, r, coef, static_cast<float>(lambda / (K * rnorm[k])),
+                                              gr.pdv, n, parts, gr.ticket, gr.red + 2);
+            lspmv<<<warps_grid(n), 256, 0, s>>>(gr.Lrp, gr.Lcol, nullptr, gr.g, gr.pdv, gr.pdu, n);
+            probe_grad<<<rg, 256, 0, s>>>(gr.Lrp, gr.Lcol, gr.pdv, gr.pu, gr.pdu, gr.pw, gr.dg, n);
+        }
+    }
+    double h[3];
+    cudaMemcpyAsync(h, gr.red, 3 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    return std::log(h[0] / n) - 2.0 * h[1] / n + h[2];
+}
+
+void reduce_into(_clsparseB200Spai* net, int rec, int ntiles, int off_w, int off_b, int nw, cudaStream_t s) {
+    reduce_parts<<<nblk(rec, 256), 256, 0, s>>>(net->gr.part, rec, ntiles, net->grad, off_w, off_b, nw);
+}
+
+void backward(_clsparseB200Spai* net, int bf16, cudaStream_t s) {
+    Graph& gr = net->gr;
+    const Offsets& o = net->o;
+    const float* P = net->prm;
+    const size_t n = gr.n;
+    const size_t nh = n * H;
+    const uint32_t tiles = nblk(n, kRows);
+    cudaMemsetAsync(net->grad, 0, size_t(o.total) * 4, s);
+    cudaMemsetAsync(gr.dH, 0, nh * 4, s);
+    output_bwd_rows<<<warps_grid(n), 256, 0, s>>>(gr.Lrp, gr.Lcol, gr.Le, gr.Hs[NL], gr.Hp, gr.Hq, P, o, gr.dg,
+                                                  gr.dH, gr.dHp, gr.part, gr.n, bf16);
+    reduce_into(net, kOutPart, static_cast<int>(n), o.r, -1, kOutPart, s);
+    output_bwd_cols<<<warps_grid(n), 256, 0, s>>>(gr.LTrp, gr.LTrow, gr.LTidx, gr.Le, gr.Hp, gr.Hq, P, o, gr.dg,
+                                                  gr.dHq, gr.n, bf16);
+    linear_bwd<HO, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[NL], nullptr, P + o.P, nullptr, gr.dHp, gr.dH, nullptr,
+                                               gr.part, n, 0, bf16);
+    reduce_into(net, HO * H + HO, tiles, o.P, -1, HO * H, s);
+    linear_bwd<HO, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[NL], nullptr, P + o.Q, nullptr, gr.dHq, gr.dH, nullptr,
+                                               gr.part, n, 0, bf16);
+    reduce_into(net, HO * H + HO, tiles, o.Q, -1, HO * H, s);
+    // gr.dH holds dL/dH_NL; walk the layers back
+    for (int l = NL - 1; l >= 0; --l) {
+        // H_{l+1} = H_l + relu(V [H_l; S_l] + d): dH_l = dH_{l+1} + ..., dS_l = ...
+        cudaMemcpyAsync(gr.dHn, gr.dH, nh * 4, cudaMemcpyDeviceToDevice, s);
+        cudaMemsetAsync(gr.dS, 0, nh * 4, s);
+        linear_bwd<H, H, H><<<tiles, 256, 0, s>>>(gr.Hs[l], gr.S[l], P + o.V[l], gr.Au[l], gr.dH, gr.dHn, gr.dS,
+                                                  gr.part, n, 1, bf16);
+        reduce_into(net, H * 2 * H + H, tiles, o.V[l], o.d[l], H * 2 * H, s);
+        message_bwd<<<warps_grid(n), 256, 0, s>>>(gr.rp, gr.cols, gr.ehat, gr.Hu[l], P + o.w[l], P + o.c[l],
+                                                  gr.dS, gr.dHu, gr.part, gr.n, bf16);
+        reduce_into(net, 2 * H, static_cast<int>(n), o.w[l], o.c[l], H, s);
+        linear_bwd<H, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[l], nullptr, P + o.U[l], nullptr, gr.dHu, gr.dHn,
+                                                  nullptr, gr.part, n, 0, bf16);
+        reduce_into(net, H * H + H, tiles, o.U[l], -1, H * H, s);
+        std::swap(gr.dH, gr.dHn);
+    }
+    linear_bwd<H, NF, 0><<<tiles, 256, 0, s>>>(gr.F, nullptr, P + o.w_in, gr.Hs[0], gr.dH, nullptr, nullptr,
+                                               gr.part, n, 1, bf16);
+    reduce_into(net, H * NF + H, tiles, o.w_in, o.b_in, H * NF, s);
+}
+
+void export_g(_clsparseB200Spai* net, cudaStream_t s) {
+    Graph& gr = net->gr;
+    const uint32_t g = std::min<uint32_t>(nblk(gr.n, 256), 4096);
+    export_factor<<<g, 256, 0, s>>>(gr.Lrp, gr.Lcol, gr.g, gr.dinvs, gr.G32, gr.G16, gr.G64, gr.n);
+    gather_transpose<<<g, 256, 0, s>>>(gr.LTidx, gr.G32, gr.G16, gr.G64, gr.GT32, gr.GT16, gr.GT64, gr.nnzL);
+}
+
+clsparseStatus check_net(clsparseB200Spai net, clsparseControl c, bool need_graph) {
+    if (net == nullptr) return clsparseInvalidValue;
+    clsparseStatus st = check_entry(c);
+    if (st != clsparseSuccess) return st;
+    if (need_graph && !net->gr.built) return clsparseStructInvalid;
+    return clsparseSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+clsparseStatus clsparseB200SpaiCreate(clsparseB200Spai* out, cl_ulong seed) {
+    if (out == nullptr) return clsparseInvalidValue;
+    auto* net = new (std::nothrow) _clsparseB200Spai();
+    if (!net) return clsparseOutOfHostMemory;
+    net->o = layout();
+    const int P = net->o.total;
+    cudaGetDevice(&net->device);
+    if (dalloc(net->prm, P) != cudaSuccess || dalloc(net->grad, P) != cudaSuccess ||
+        dalloc(net->m, P) != cudaSuccess || dalloc(net->v, P) != cudaSuccess) {
+        cudaGetLastError();
+        delete net;
+        return clsparseOutOfResources;
+    }
+    // He-style initialisation from a fixed-seed generator
+    std::vector<float> h(P, 0.f);
+    std::mt19937_64 rng(seed);
+    auto fill = [&](int off, int rows, int cols, float gain) {
+        std::normal_distribution<float> nd(0.f, gain / std::sqrt(static_cast<float>(cols)));
+        for (int i = 0; i < rows * cols; ++i) h[off + i] = nd(rng);
+    };
+    const Offsets& o = net->o;
+    fill(o.w_in, H, NF, 1.4f);
+    for (int l = 0; l < NL; ++l) {
+        fill(o.U[l], H, H, 1.0f);
+        fill(o.w[l], 1, H, 1.0f);
+        fill(o.V[l], H, 2 * H, 0.5f);
+    }
+    fill(o.P, HO, H, 1.0f);
+    fill(o.Q, HO, H, 1.0f);
+    fill(o.r, 1, HO, 1.0f);
+    fill(o.w_o, 1, HO, 0.05f);
+    fill(o.w_d, 1, H, 0.05f);
+    h[o.b_d] = 0.5413f;  // softplus(0.5413) = 1: starts near the Jacobi factor
+    cudaMemcpy(net->prm, h.data(), size_t(P) * 4, cudaMemcpyHostToDevice);
+    cudaMemset(net->m, 0, size_t(P) * 4);
+    cudaMemset(net->v, 0, size_t(P) * 4);
+    *out = net;
+    return clsparseSuccess;
+}
+
+clsparseStatus clsparseB200SpaiRelease(clsparseB200Spai net) {
+    if (net == nullptr) return clsparseInvalidValue;
+    delete net;
+    return clsparseSuccess;
+}
+
+clsparseStatus clsparseB200SpaiSetMatrix(clsparseB200Spai net, const clsparseCsrMatrix* A,
+                                         clsparseControl control) {
+    clsparseStatus st = check_net(net, control, false);
+    if (st != clsparseSuccess) return st;
+    if (!A || A->num_rows != A->num_cols || A->num_rows == 0) return clsparseInvalidSystemSize;
+    DeviceGuard g(control->device);
+    return build_graph(net, A, control);
+}
+
+clsparseStatus clsparseB200SpaiParams(clsparseB200Spai net, cl_float* host, size_t capacity, size_t* count,
+                                      cl_int toDevice) {
+    if (net == nullptr || count == nullptr) return clsparseInvalidValue;
+    *count = static_cast<size_t>(net->o.total);
+    if (host == nullptr) return clsparseSuccess;
+    if (capacity < *count) return clsparseInsufficientMemory;
+    DeviceGuard g(net->device);
+    const cudaError_t e = toDevice ? cudaMemcpy(net->prm, host, *count * 4, cudaMemcpyHostToDevice)
+                                   : cudaMemcpy(host, net->prm, *count * 4, cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? clsparseSuccess : clsparseInvalidKernelExecution;
+}
+
+clsparseStatus clsparseB200SpaiLossGrad(clsparseB200Spai net, const cldenseVector* probes, cl_int K,
+                                        cl_double lambda, cl_int fp32Weights, cl_double* loss, cl_float* grad,
+                                        size_t capacity, clsparseControl control) {
+    clsparseStatus st = check_net(net, control, true);
+    if (st != clsparseSuccess) return st;
+    if (K > 0 && (!probes || probes->num_values < size_t(K) * net->gr.n)) return clsparseInvalidSize;
+    DeviceGuard g(control->device);
+    const int bf16 = fp32Weights ? 0 : 1;
+    forward(net, bf16, control->stream);
+    const double L = loss_and_dg(net, K > 0 ? dev_ptr<const float>(probes->values, probes->off_values) : nullptr,
+                                 K, lambda, control->stream);
+    backward(net, bf16, control->stream);
+    if (loss) *loss = L;
+    if (grad) {
+        if (capacity < size_t(net->o.total)) return clsparseInsufficientMemory;
+        cudaMemcpyAsync(grad, net->grad, size_t(net->o.total) * 4, cudaMemcpyDeviceToHost, control->stream);
+    }
+    return cudaStreamSynchronize(control->stream) == cudaSuccess ? clsparseSuccess
+                                                                 : clsparseInvalidKernelExecution;
+}
+
+clsparseStatus clsparseB200SpaiTrainStep(clsparseB200Spai net, const cldenseVector* probes, cl_int K,
+                                         cl_double lambda, cl_double lr, cl_double* loss,
+                                         clsparseControl control) {
+    clsparseStatus st = clsparseB200SpaiLossGrad(net, probes, K, lambda, 0, loss, nullptr, 0, control);
+    if (st != clsparseSuccess) return st;
+    DeviceGuard g(control->device);
+    net->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, float(net->step)), c2 = 1.f - std::pow(b2, float(net->step));
+    adam_step<<<nblk(net->o.total, 256), 256, 0, control->stream>>>(net->prm, net->grad, net->m, net->v,
+                                                                    net->o.total, float(lr), b1, b2, 1e-8f, c1,
+                                                                    c2);
+    return finish_call(control);
+}
+
+clsparseStatus clsparseB200SpaiBuild(clsparseB200Spai net, clsparseControl control) {
+    clsparseStatus st = check_net(net, control, true);
+    if (st != clsparseSuccess) return st;
+    DeviceGuard g(control->device);
+    forward(net, 1, control->stream);
+    export_g(net, control->stream);
+    return finish_call(control);
+}
+
+// Copies the exported factor (FP64, L = tril(A) order) and its pattern to the host.
+clsparseStatus clsparseB200SpaiGetFactor(clsparseB200Spai net, clsparseIdx_t* rowPtr, clsparseIdx_t* cols,
+                                         cl_double* vals, size_t capacity, size_t* nnz) {
+    if (net == nullptr || nnz == nullptr || !net->gr.built) return clsparseInvalidValue;
+    *nnz = net->gr.nnzL;
+    if (!rowPtr && !cols && !vals) return clsparseSuccess;
+    if (capacity < net->gr.nnzL) return clsparseInsufficientMemory;
+    DeviceGuard g(net->device);
+    if (rowPtr) cudaMemcpy(rowPtr, net->gr.Lrp, (net->gr.n + 1) * 4, cudaMemcpyDeviceToHost);
+    if (cols) cudaMemcpy(cols, net->gr.Lcol, size_t(net->gr.nnzL) * 4, cudaMemcpyDeviceToHost);
+    if (vals) cudaMemcpy(vals, net->gr.G64, size_t(net->gr.nnzL) * 8, cudaMemcpyDeviceToHost);
+    return cudaGetLastError() == cudaSuccess ? clsparseSuccess : clsparseInvalidKernelExecution;
+}
+
+// Checkpoint: "CLSPSPAI", version, parameter count, step, FP32 weights, Adam
+// moments, FNV-1a 64 checksum of everything before it.
+clsparseStatus clsparseB200SpaiSave(clsparseB200Spai net, const char* path) {
+    if (net == nullptr || path == nullptr) return clsparseInvalidValue;
+    DeviceGuard g(net->device);
+    const size_t P = size_t(net->o.total);
+    std::vector<float> buf(3 * P);
+    cudaMemcpy(buf.data(), net->prm, P * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(buf.data() + P, net->m, P * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(buf.data() + 2 * P, net->v, P * 4, cudaMemcpyDeviceToHost);
+    const char magic[8] = {'C', 'L', 'S', 'P', 'S', 'P', 'A', 'I'};
+    const uint32_t hdr[3] = {1u, static_cast<uint32_t>(P), static_cast<uint32_t>(net->step)};
+    uint64_t h = fnv1a(magic, 8);
+    h = fnv1a(hdr, sizeof(hdr), h);
+    h = fnv1a(buf.data(), buf.size() * 4, h);
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return clsparseInvalidFile;
+    bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(hdr, 4, 3, f) == 3 &&
+              std::fwrite(buf.data(), 4, buf.size(), f) == buf.size() && std::fwrite(&h, 8, 1, f) == 1;
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? clsparseSuccess : clsparseInvalidFile;
+}
+
+clsparseStatus clsparseB200SpaiLoad(clsparseB200Spai net, const char* path) {
+    if (net == nullptr || path == nullptr) return clsparseInvalidValue;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return clsparseInvalidFile;
+    char magic[8];
+    uint32_t hdr[3];
+    const size_t P = size_t(net->o.total);
+    std::vector<float> buf(3 * P);
+    uint64_t h_file = 0;
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "CLSPSPAI", 8) == 0 &&
+              std::fread(hdr, 4, 3, f) == 3 && hdr[0] == 1u && hdr[1] == P &&
+              std::fread(buf.data(), 4, buf.size(), f) == buf.size() && std::fread(&h_file, 8, 1, f) == 1;
+    std::fclose(f);
+    if (!ok) return clsparseInvalidFileFormat;
+    uint64_t h = fnv1a(magic, 8);
+    h = fnv1a(hdr, sizeof(hdr), h);
+    h = fnv1a(buf.data(), buf.size() * 4, h);
+    if (h != h_file) return clsparseInvalidFileFormat;
+    DeviceGuard g(net->device);
+    cudaMemcpy(net->prm, buf.data(), P * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(net->m, buf.data() + P, P * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(net->v, buf.data() + 2 * P, P * 4, cudaMemcpyHostToDevice);
+    net->step = static_cast<int>(hdr[2]);
+    return cudaGetLastError() == cudaSuccess ? clsparseSuccess : clsparseInvalidKernelExecution;
+}
+
+}  // extern "C"
+
+namespace clsp {
+
+// Views of the exported factor for the solvers (mixed.cu).
+bool spai_factor_views(clsparseB200Spai net, CsrView<__nv_bfloat16>& G16, CsrView<__nv_bfloat16>& GT16,
+                       CsrView<float>& G32, CsrView<float>& GT32, CsrView<double>& G64, CsrView<double>& GT64) {
+    if (net == nullptr || !net->gr.built) return false;
+    const Graph& gr = net->gr;
+    G16 = CsrView<__nv_bfloat16>{gr.G16, gr.Lcol, gr.Lrp, gr.n, gr.n, gr.nnzL, nullptr};
+    GT16 = CsrView<__nv_bfloat16>{gr.GT16, gr.LTrow, gr.LTrp, gr.n, gr.n, gr.nnzL, nullptr};
+    G32 = CsrView<float>{gr.G32, gr.Lcol, gr.Lrp, gr.n, gr.n, gr.nnzL, nullptr};
+    GT32 = CsrView<float>{gr.GT32, gr.LTrow, gr.LTrp, gr.n, gr.n, gr.nnzL, nullptr};
+    G64 = CsrView<double>{gr.G64, gr.Lcol, gr.Lrp, gr.n, gr.n, gr.nnzL, nullptr};
+    GT64 = CsrView<double>{gr.GT64, gr.LTrow, gr.LTrp, gr.n, gr.n, gr.nnzL, nullptr};
+    return true;
+}
+
+}  // namespace clsp

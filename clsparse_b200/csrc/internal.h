@@ -155,7 +155,7 @@ constexpr int kMaxReduceCtas = 2048;
 // Optional fused epilogue of an SpMV: per-row dot products of the result y
 // with w0 (and with y itself), reduced deterministically over the grid; the
 // last CTA to finish runs a solver-specific finaliser (spmv_epilogue_op).
-enum class EpiOp : int { None = 0, CgAlpha = 1, BicgAlpha = 2, BicgOmega = 3 };
+enum class EpiOp : int { None = 0, CgAlpha = 1, BicgAlpha = 2, BicgOmega = 3, PcgRz = 4, PcgRz0 = 5 };
 
 struct SpmvEpilogue {
     int ndots = 0;            // 0, 1 or 2
@@ -192,6 +192,17 @@ cudaError_t launch_csrmv(const CsrView<V>& A, const T* alpha, const T* beta, con
 template <typename V, typename T>
 clsparseStatus cg_solve_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
                               clSParseSolverControl sc, clsparseControl c);
+
+// PCG with the factorized preconditioner M^-1 = G^T G (solvers.cu).
+template <typename V, typename T, typename VG>
+clsparseStatus pcg_factor_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                                clSParseSolverControl sc, const CsrView<VG>& G, const CsrView<VG>& Gt,
+                                clsparseControl c);
+
+// Device views of a learned factor G (L = tril(A) order) and G^T (gnn.cu).
+bool spai_factor_views(clsparseB200Spai net, CsrView<__nv_bfloat16>& G16, CsrView<__nv_bfloat16>& GT16,
+                       CsrView<float>& G32, CsrView<float>& GT32, CsrView<double>& G64,
+                       CsrView<double>& GT64);
 
 // Host binning (meta.cpp).
 void compute_row_blocks(cl_ulong* rowBlocks, clsparseIdx_t& rowBlockSize, const clsparseIdx_t* rp,

@@ -72,10 +72,15 @@ MixedWork& work_of(clsparseControl c) {
     return *c->mixed_work;
 }
 
+// Learned factor M^-1 = G^T G for the inner solves (null: Jacobi).
+struct Factor {
+    CsrView<__nv_bfloat16> G, GT;
+};
+
 template <typename V>
 clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
                       clSParseSolverControl sc, double inner_tol, clsparseB200MixedInfo* info,
-                      clsparseControl c) {
+                      clsparseControl c, const Factor* factor = nullptr, int* fell_back = nullptr) {
     const size_t n = A->num_rows, nnz = A->num_nonzeros;
     MixedWork& w = work_of(c);
     if (w.lowvals.ensure(nnz * sizeof(V) + 256) != cudaSuccess || w.y.ensure(n * 8 + 256) != cudaSuccess ||
@@ -120,6 +125,7 @@ clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const clden
     double* hres = static_cast<double*>(w.pinned);
     const uint32_t g = grid_for(n, c->sm_count);
     clsparseStatus st = clsparseSuccess;
+    bool use_factor = factor != nullptr;
     info->converged = 0;
     for (;;) {
         SpmvEpilogue none;
@@ -153,7 +159,14 @@ clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const clden
             break;
         }
         if (inner_total >= max_inner_total) break;
-        if (res > 0.5 * prev && ++stalls >= 3) break;  // refinement no longer contracts
+        // The learned factor stalls when an outer step fails to halve the
+        // residual or its inner solve broke down: continue with Jacobi.
+        if (use_factor && outer > 0 && (res > 0.5 * prev || (inner.deviceStatus & 0x14u))) {
+            use_factor = false;
+            if (fell_back) *fell_back = 1;
+        } else if (res > 0.5 * prev && ++stalls >= 3) {
+            break;  // refinement no longer contracts
+        }
         prev = res;
         // inner solve A_low d = r / ||b||, from d = 0
         cudaMemsetAsync(w.d.ptr, 0, n * sizeof(float), s);
@@ -161,7 +174,12 @@ clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const clden
         inner.relativeTolerance = inner_tol;
         inner.absoluteTolerance = 0.0;
         inner.nIters = 0;
-        st = cg_solve_typed<V, float>(&dvec, &Alow, &rvec, &inner, c);
+        inner.deviceStatus = 0;
+        if (use_factor)
+            st = pcg_factor_typed<V, float, __nv_bfloat16>(&dvec, &Alow, &rvec, &inner, factor->G, factor->GT,
+                                                            c);
+        else
+            st = cg_solve_typed<V, float>(&dvec, &Alow, &rvec, &inner, c);
         if (st != clsparseSuccess) return st;
         inner_total += inner.nIters + 1;
         update_kernel<<<g, kThreads, 0, s>>>(x, static_cast<const float*>(w.d.ptr), bnorm, n);
@@ -200,6 +218,50 @@ clsparseStatus clsparseDcsrcgMixed(cldenseVector* x, const clsparseCsrMatrix* A,
     if (innerPrecision == 0)
         return refine<float>(x, A, b, solverControl, innerTolerance, info, control);
     return refine<__nv_bfloat16>(x, A, b, solverControl, innerTolerance, info, control);
+}
+
+clsparseStatus clsparseDcsrcgLearned(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                                     clSParseSolverControl solverControl, clsparseB200Spai spai,
+                                     cl_int innerPrecision, cl_double innerTolerance,
+                                     clsparseB200MixedInfo* info, cl_int* fellBack, clsparseControl control) {
+    clsparseStatus st = check_entry(control);
+    if (st != clsparseSuccess) return st;
+    if (solverControl == nullptr) return clsparseInvalidSolverControlObject;
+    if (!x || !A || !b || !info) return clsparseInvalidValue;
+    if (A->num_rows != A->num_cols || A->num_rows != x->num_values || A->num_cols != b->num_values)
+        return clsparseInvalidSystemSize;
+    CsrView<__nv_bfloat16> G16, GT16;
+    CsrView<float> G32, GT32;
+    CsrView<double> G64, GT64;
+    if (!spai_factor_views(spai, G16, GT16, G32, GT32, G64, GT64)) return clsparseStructInvalid;
+    if (G16.nrows != A->num_rows) return clsparseInvalidSystemSize;
+    std::memset(info, 0, sizeof(*info));
+    int fb = 0;
+    DeviceGuard g(control->device);
+    if (innerPrecision == 2) {
+        // plain FP64 PCG with M^-1 = G^T G, L2 stop test on the recursive residual
+        _solverControl sc = *solverControl;
+        sc.normType = 1;
+        sc.nIters = 0;
+        st = pcg_factor_typed<double, double, double>(x, A, b, &sc, G64, GT64, control);
+        if (st != clsparseSuccess) return st;
+        info->innerIterations = sc.nIters + 1;
+        info->trueResidual = sc.currentResidual;
+        info->initialTrueResidual = sc.initialResidual;
+        info->converged = sc.currentResidual <= solverControl->relativeTolerance ? 1 : 0;
+        solverControl->nIters = sc.nIters;
+        solverControl->currentResidual = sc.currentResidual;
+        if (fellBack) *fellBack = 0;
+        return clsparseSuccess;
+    }
+    if (innerPrecision != 0 && innerPrecision != 1) return clsparseInvalidType;
+    Factor f{G16, GT16};
+    if (innerPrecision == 0)
+        st = refine<float>(x, A, b, solverControl, innerTolerance, info, control, &f, &fb);
+    else
+        st = refine<__nv_bfloat16>(x, A, b, solverControl, innerTolerance, info, control, &f, &fb);
+    if (fellBack) *fellBack = fb;
+    return st;
 }
 
 clsparseStatus clsparseB200SolverSetNormType(clSParseSolverControl solverControl, cl_int normType) {

@@ -66,6 +66,20 @@ __device__ __forceinline__ void fin_cg_alpha(SolverState<T>* st, double yp) {
     if (!(st->yp > T(0))) st->status_bits |= kStatusCurvature;
 }
 
+// Finaliser after z = G^T (G r) with dot0 = <z, r>: new <r,z>, beta.
+template <typename T>
+__device__ __forceinline__ void fin_pcg_rz(SolverState<T>* st, double rz) {
+    st->rz_old = st->rz;
+    st->rz = static_cast<T>(rz);
+    st->beta = st->rz / st->rz_old;
+}
+
+// Finaliser of the first z = G^T (G r0): <r0, z0>.
+template <typename T>
+__device__ __forceinline__ void fin_pcg_rz0(SolverState<T>* st, double rz) {
+    st->rz = static_cast<T>(rz);
+}
+
 // Finaliser after AMp = A (M p) with dot0 = <AMp, r*>: alpha = <r*,r> / <r*,AMp>.
 template <typename T>
 __device__ __forceinline__ void fin_bicg_alpha(SolverState<T>* st, double rs_amp) {

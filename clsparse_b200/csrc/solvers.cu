@@ -390,6 +390,113 @@ __global__ void __launch_bounds__(kThreads) bicg_p_kernel(BicgArgs<T> a) {
     }
 }
 
+// ------------------------------------------ factorized-inverse PCG ----
+// M^-1 = G^T G (G lower triangular on the pattern of tril(A)), applied as two
+// SpMVs, so z is held in memory. Per iteration: q = A p with <q,p> fused
+// (alpha); x/r update with the stop test; t = G r; z = G^T t with <z,r> fused
+// (beta); p = z + beta p.
+
+template <typename T>
+struct PcgArgs {
+    T* x;
+    const T* b;
+    T* q;
+    T* r;
+    T* p;
+    T* t;
+    T* z;
+    SolverState<T>* st;
+    double* parts;
+    uint32_t* ticket;
+    size_t n;
+    unsigned long long cond;
+};
+
+// r = b - A x (q holds A x); ||b||, ||r||; initial stop test.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) pcg_init_kernel(PcgArgs<T> a) {
+    double acc[2] = {0.0, 0.0};
+    const int l2 = a.st->norm_type;
+    const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
+        const T bi = a.b[i];
+        const T ri = bi - a.q[i];
+        a.r[i] = ri;
+        acc[0] += norm_term(bi, l2);
+        acc[1] += norm_term(ri, l2);
+    }
+    double tot[2];
+    if (dev::grid_reduce_last<2>(acc, a.parts, a.ticket, tot) && threadIdx.x == 0) {
+        SolverState<T>* st = a.st;
+        st->norm_b = static_cast<T>(norm_finish(tot[0], l2));
+        if (st->norm_b == T(0)) {
+            st->zero_b = 1;
+            st->done = 1;
+            st->nIters = 0;
+            set_condition(a.cond, 0u);
+            return;
+        }
+        st->norm_r = static_cast<T>(norm_finish(tot[1], l2));
+        st->res = st->norm_r / st->norm_b;
+        st->init_res = static_cast<double>(st->res);
+        st->cur_res = st->init_res;
+        st->iteration = 0;
+        if (solver_finished(*st, st->init_res)) {
+            st->nIters = 0;
+            st->done = 1;
+            set_condition(a.cond, 0u);
+        } else {
+            set_condition(a.cond, 1u);
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) pcg_copy_kernel(PcgArgs<T> a) {
+    if (a.st->done) return;
+    const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride)
+        a.p[i] = a.z[i];
+}
+
+// x += alpha p; r -= alpha q; ||r||; stop test.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) pcg_update_kernel(PcgArgs<T> a) {
+    if (a.st->done) return;
+    const T alpha = a.st->alpha;
+    const int l2 = a.st->norm_type;
+    double acc[1] = {0.0};
+    const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
+        a.x[i] = a.x[i] + alpha * a.p[i];
+        const T ri = a.r[i] - alpha * a.q[i];
+        a.r[i] = ri;
+        acc[0] += norm_term(ri, l2);
+    }
+    double tot[1];
+    if (dev::grid_reduce_last<1>(acc, a.parts, a.ticket, tot) && threadIdx.x == 0) {
+        SolverState<T>* st = a.st;
+        st->norm_r = static_cast<T>(norm_finish(tot[0], l2));
+        st->res = st->norm_r / st->norm_b;
+        st->nIters = st->iteration;
+        st->iteration += 1;
+        st->cur_res = static_cast<double>(st->res);
+        if (!isfinite(st->cur_res)) st->status_bits |= kStatusNonFinite;
+        const bool fin = solver_finished(*st, st->cur_res);
+        st->done = fin ? 1 : 0;
+        set_condition(a.cond, fin ? 0u : 1u);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) pcg_p_kernel(PcgArgs<T> a) {
+    if (a.st->done) return;
+    const T beta = a.st->beta;
+    const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride)
+        a.p[i] = a.z[i] + beta * a.p[i];
+}
+
 // ---------------------------------------------------------- driver ----
 
 // Runs prologue / body / epilogue either as one graph with a conditional
@@ -764,7 +871,125 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
     return stt;
 }
 
+// PCG with M^-1 = G^T G; G and Gt (its transpose) are CSR with values VG.
+template <typename V, typename T, typename VG>
+clsparseStatus pcg_factor_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
+                                clSParseSolverControl sc, const CsrView<VG>& G, const CsrView<VG>& Gt,
+                                clsparseControl c) {
+    clsparseStatus stt = check_solver_args(xv, A, bv, sc, c);
+    if (stt != clsparseSuccess) return stt;
+    if (G.nrows != A->num_rows || Gt.nrows != A->num_rows) return clsparseInvalidSystemSize;
+    DeviceGuard guard(c->device);
+    const size_t n = A->num_rows;
+    if (!c->solver_cache) c->solver_cache = std::make_unique<SolverCache>();
+    SolverCache& cache = *c->solver_cache;
+    const CsrView<V> Av = view_of<V>(A);
+    const uint32_t spmv_ctas = std::max(spmv_num_ctas(Av.meta, Av.nrows, Av.nnz),
+                                        std::max(spmv_num_ctas(G.meta, G.nrows, G.nnz),
+                                                 spmv_num_ctas(Gt.meta, Gt.nrows, Gt.nnz)));
+    SolverKey key = make_key(3, sizeof(V), sizeof(T), sc, c, A, xv, bv);
+    key.ptrs[6] = G.vals;
+    key.ptrs[7] = Gt.vals;
+    bool rebuild = false;
+    stt = prepare_cache<T>(c, cache, key, 5, n, spmv_ctas, rebuild);
+    if (stt != clsparseSuccess) return stt;
+
+    const size_t vb = ((n * sizeof(T) + 255) / 256) * 256;
+    char* base = static_cast<char*>(cache.vecs.ptr);
+    PcgArgs<T> a;
+    a.x = dev_ptr<T>(xv->values, xv->off_values);
+    a.b = dev_ptr<const T>(bv->values, bv->off_values);
+    a.q = reinterpret_cast<T*>(base);
+    a.r = reinterpret_cast<T*>(base + vb);
+    a.p = reinterpret_cast<T*>(base + 2 * vb);
+    a.t = reinterpret_cast<T*>(base + 3 * vb);
+    a.z = reinterpret_cast<T*>(base + 4 * vb);
+    a.st = static_cast<SolverState<T>*>(cache.state.ptr);
+    a.parts = static_cast<double*>(cache.parts.ptr) + 1;
+    a.ticket = static_cast<uint32_t*>(cache.parts.ptr);
+    a.n = n;
+    a.cond = 0;
+
+    auto* hs = reinterpret_cast<SolverState<T>*>(c->pinned);
+    init_state(*hs, sc);
+    cudaMemcpyAsync(a.st, hs, sizeof(SolverState<T>), cudaMemcpyHostToDevice, c->stream);
+
+    const uint32_t vg = vec_grid(n, c->sm_count);
+    const bool ext = c->extended_precision;
+    SolverState<T>* st = a.st;
+    auto apply_m = [&](cudaStream_t s, const PcgArgs<T>& aa, EpiOp op) {
+        SpmvEpilogue plain;
+        plain.done = &st->done;
+        launch_csrmv<VG, T>(G, &st->one, &st->zero, aa.r, aa.t, false, plain, s);
+        SpmvEpilogue e;
+        e.ndots = 1;
+        e.w0 = aa.r;
+        e.partials = aa.parts;
+        e.ticket = aa.ticket;
+        e.op = op;
+        e.state = st;
+        e.done = &st->done;
+        launch_csrmv<VG, T>(Gt, &st->one, &st->zero, aa.t, aa.z, false, e, s);
+    };
+    auto prologue = [&](cudaStream_t s, unsigned long long h) {
+        PcgArgs<T> aa = a;
+        aa.cond = h;
+        SpmvEpilogue none;
+        launch_csrmv<V, T>(Av, &st->one, &st->zero, aa.x, aa.q, ext, none, s);
+        pcg_init_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+        apply_m(s, aa, EpiOp::PcgRz0);
+        pcg_copy_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+    };
+    auto body = [&](cudaStream_t s, unsigned long long h) {
+        PcgArgs<T> aa = a;
+        aa.cond = h;
+        SpmvEpilogue epi;
+        epi.ndots = 1;
+        epi.w0 = aa.p;
+        epi.partials = aa.parts;
+        epi.ticket = aa.ticket;
+        epi.op = EpiOp::CgAlpha;
+        epi.state = st;
+        epi.done = &st->done;
+        launch_csrmv<V, T>(Av, &st->one, &st->zero, aa.p, aa.q, ext, epi, s);
+        pcg_update_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+        apply_m(s, aa, EpiOp::PcgRz);
+        pcg_p_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+    };
+    auto epilogue = [&](cudaStream_t s) {
+        copy_if_zero_b_kernel<T><<<vg, kThreads, 0, s>>>(a.x, a.b, n, st);
+    };
+    if (n == 0) {
+        sc->nIters = 0;
+        return clsparseSuccess;
+    }
+    stt = run_solve(c, cache, rebuild, &st->done, sc->maxIters, prologue, body, epilogue);
+    if (stt != clsparseSuccess) {
+        cache.valid = false;
+        cache.drop_graph();
+        return stt;
+    }
+    return read_back<T>(c, cache, sc);
+}
+
 }  // namespace
+
+template <typename V, typename T, typename VG>
+clsparseStatus pcg_factor_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                                clSParseSolverControl sc, const CsrView<VG>& G, const CsrView<VG>& Gt,
+                                clsparseControl c) {
+    return pcg_factor_solve<V, T, VG>(x, A, b, sc, G, Gt, c);
+}
+template clsparseStatus pcg_factor_typed<float, float, __nv_bfloat16>(
+    cldenseVector*, const clsparseCsrMatrix*, const cldenseVector*, clSParseSolverControl,
+    const CsrView<__nv_bfloat16>&, const CsrView<__nv_bfloat16>&, clsparseControl);
+template clsparseStatus pcg_factor_typed<float, float, float>(cldenseVector*, const clsparseCsrMatrix*,
+                                                              const cldenseVector*, clSParseSolverControl,
+                                                              const CsrView<float>&, const CsrView<float>&,
+                                                              clsparseControl);
+template clsparseStatus pcg_factor_typed<double, double, double>(
+    cldenseVector*, const clsparseCsrMatrix*, const cldenseVector*, clSParseSolverControl,
+    const CsrView<double>&, const CsrView<double>&, clsparseControl);
 
 template <typename V, typename T>
 clsparseStatus cg_solve_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,

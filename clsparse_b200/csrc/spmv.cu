@@ -95,6 +95,8 @@ __device__ __forceinline__ void run_epilogue(RowSink<T, K>& sink, const EpiDev<T
                 auto* st = static_cast<SolverState<T>*>(e.state);
                 if (e.op == static_cast<int>(EpiOp::CgAlpha)) fin_cg_alpha(st, tot[0]);
                 if (e.op == static_cast<int>(EpiOp::BicgAlpha)) fin_bicg_alpha(st, tot[0]);
+                if (e.op == static_cast<int>(EpiOp::PcgRz)) fin_pcg_rz(st, tot[0]);
+                if (e.op == static_cast<int>(EpiOp::PcgRz0)) fin_pcg_rz0(st, tot[0]);
                 if constexpr (K >= 2) {
                     if (e.op == static_cast<int>(EpiOp::BicgOmega)) fin_bicg_omega(st, tot[0], tot[1]);
                 }

@@ -108,6 +108,61 @@ clsparseScsrcgBatched(cldenseVector* x, const clsparseCsrMatrix* A, const cldens
                       const cl_int* lanesPerRow, clSParseSolverControl solverControl,
                       clsparseB200BatchResult* result, clsparseControl control);
 
+/* ---- learned factorized sparse approximate inverse (no reference counterpart) ----
+ * A 4-layer message-passing network (hidden width 64, BF16 weights, FP32
+ * accumulation) over the graph of an SPD matrix A emits G on the pattern of
+ * tril(A) with a softplus-positive diagonal; M^-1 = G^T G is SPD. Training,
+ * inference and the optimiser run on the GPU (clsparse_b200/csrc/gnn.cu). */
+typedef struct _clsparseB200Spai* clsparseB200Spai;
+
+/* New network with weights drawn from a generator seeded with `seed`. */
+CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiCreate(clsparseB200Spai* spai, cl_ulong seed);
+CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiRelease(clsparseB200Spai spai);
+/* Prepares the graph of A (FP64 values, sorted columns, positive diagonal,
+ * at most 8 entries per row of tril(A)) for training or building G. A's
+ * arrays must stay valid while the network uses them. */
+CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiSetMatrix(clsparseB200Spai spai, const clsparseCsrMatrix* A,
+                                                         clsparseControl control);
+/* Reads (toDevice = 0) or writes (1) the flat FP32 parameter vector; *count
+ * gets its length. */
+CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiParams(clsparseB200Spai spai, cl_float* host, size_t capacity,
+                                                      size_t* count, cl_int toDevice);
+/* Loss and gradient at the current weights for the current matrix: the
+ * Kaporin bound log(tr(G A G^T)/n) - (2/n) sum log g_ii of the scaled
+ * operator plus lambda * mean_k ||G^T G A r_k - r_k||^2/||r_k||^2 over K probe
+ * vectors stored back to back in `probes` (FP32, scaled space). fp32Weights
+ * uses the FP32 master weights instead of their BF16 rounding. */
+CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiLossGrad(clsparseB200Spai spai, const cldenseVector* probes,
+                                                        cl_int K, cl_double lambda, cl_int fp32Weights,
+                                                        cl_double* loss, cl_float* grad, size_t capacity,
+                                                        clsparseControl control);
+/* One Adam step (learning rate lr) on that loss. */
+CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiTrainStep(clsparseB200Spai spai, const cldenseVector* probes,
+                                                         cl_int K, cl_double lambda, cl_double lr,
+                                                         cl_double* loss, clsparseControl control);
+/* Runs the network on the current matrix and exports G and G^T for the solver. */
+CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiBuild(clsparseB200Spai spai, clsparseControl control);
+/* Copies the exported G (FP64) and its pattern (row pointers n+1, columns). */
+CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiGetFactor(clsparseB200Spai spai, clsparseIdx_t* rowPtr,
+                                                         clsparseIdx_t* cols, cl_double* vals,
+                                                         size_t capacity, size_t* nnz);
+/* Checkpoint of weights and optimiser state: magic "CLSPSPAI", version,
+ * sizes, payload and an FNV-1a 64 checksum. */
+CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiSave(clsparseB200Spai spai, const char* path);
+CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiLoad(clsparseB200Spai spai, const char* path);
+
+/* CG preconditioned with the learned M^-1 = G^T G (after clsparseB200SpaiBuild
+ * on A). innerPrecision 0 / 1: FP64 iterative refinement with FP32 / BF16
+ * matrix values in the inner PCG (FP32 vectors, BF16 G), as
+ * clsparseDcsrcgMixed; when an outer step fails to halve the FP64 residual the
+ * remaining inner solves fall back to Jacobi (*fellBack = 1). innerPrecision
+ * 2: FP64 PCG with G in FP64, L2 stop test. */
+CLSPARSE_EXPORT clsparseStatus
+clsparseDcsrcgLearned(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                      clSParseSolverControl solverControl, clsparseB200Spai spai, cl_int innerPrecision,
+                      cl_double innerTolerance, clsparseB200MixedInfo* info, cl_int* fellBack,
+                      clsparseControl control);
+
 /* FP64 dot product r = <x, y> that allocates nothing, for callers that may
  * not call cudaMalloc (allocation-free real-time loops, applications that
  * budget every device allocation themselves, code enqueuing into streams it

@@ -1,0 +1,112 @@
+"""The learned factorized preconditioner on the GPU (clsparseB200Spai*):
+forward, loss and gradients against the float64 CPU oracle, checkpoint
+round trip, the solver it feeds, and what training gains over Jacobi."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import torch
+
+from clsparse_b200 import _lib as L
+from clsparse_b200 import api, learn, matgen
+from oracle import gnn_oracle as go
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(ctrl, m=12, seed=4):
+    rp, c, v = matgen.diffusion2d_grf(m, corr_len=0.2, sigma=1.5, seed=seed)
+    A = api.CsrMatrix.from_numpy(rp, c, v)
+    spai = api.Spai(7)
+    spai.set_matrix(A, ctrl)
+    return (rp, c, v), A, spai
+
+
+def test_gpu_loss_and_gradient_match_oracle(ctrl):
+    (rp, c, v), A, spai = _setup(ctrl)
+    gr = go.Graph(rp, c, v)
+    rng = np.random.default_rng(0)
+    p = spai.params().astype(np.float64)
+    probes = rng.normal(size=(2, gr.n))
+    Lo, go_grad = go.loss_grad(p, gr, list(probes), 0.3)
+    Lg, gg = spai.loss_grad(ctrl, torch.tensor(probes, dtype=torch.float32, device="cuda"), 0.3,
+                            fp32_weights=True)
+    assert abs(Lg - Lo) <= 1e-4 * max(1.0, abs(Lo)), (Lg, Lo)
+    rel = np.linalg.norm(gg - go_grad) / np.linalg.norm(go_grad)
+    assert rel <= 2e-3, rel
+    spai.release()
+
+
+def test_bf16_weights_close_to_fp32(ctrl):
+    (rp, c, v), A, spai = _setup(ctrl, m=16, seed=5)
+    L32, g32 = spai.loss_grad(ctrl, fp32_weights=True)
+    L16, g16 = spai.loss_grad(ctrl, fp32_weights=False)
+    assert abs(L16 - L32) <= 0.05 * max(1.0, abs(L32))
+    assert np.dot(g16, g32) > 0.9 * np.linalg.norm(g16) * np.linalg.norm(g32)
+    spai.release()
+
+
+def test_factor_pattern_and_positive_diagonal(ctrl):
+    (rp, c, v), A, spai = _setup(ctrl)
+    spai.build(ctrl)
+    frp, fcol, fval = spai.factor()
+    Aop = sp.csr_matrix((v, c.astype(np.int64), rp.astype(np.int64)))
+    T = sp.tril(Aop).tocsr()
+    assert np.array_equal(frp.astype(np.int64), T.indptr) and np.array_equal(fcol.astype(np.int64), T.indices)
+    n = len(rp) - 1
+    G = sp.csr_matrix((fval, fcol.astype(np.int64), frp.astype(np.int64)), shape=(n, n))
+    assert np.all(G.diagonal() > 0)
+    M = (G.T @ G).toarray()
+    assert np.linalg.eigvalsh(M).min() > 0
+    spai.release()
+
+
+def test_checkpoint_round_trip(ctrl, tmp_path):
+    (rp, c, v), A, spai = _setup(ctrl)
+    spai.train_step(ctrl, lr=1e-3)
+    path = tmp_path / "net.bin"
+    spai.save(path)
+    other = api.Spai(99)
+    other.load(path)
+    assert np.array_equal(other.params(), spai.params())
+    raw = bytearray(path.read_bytes())
+    raw[40] ^= 0xFF
+    path.write_bytes(bytes(raw))
+    with pytest.raises(api.ClsparseError):
+        other.load(path)
+    other.release()
+    spai.release()
+
+
+def test_training_reduces_loss_and_beats_jacobi(ctrl):
+    """The trained network's G^T G-PCG needs fewer iterations than Jacobi-CG
+    on held-out matrices of the same family (the gain the network brings)."""
+    spai, hist = learn.train(ctrl, sizes=(32, 48), seeds=range(4), steps=240, lr=3e-3)
+    assert np.mean(hist[-20:]) < np.mean(hist[:8])
+    ratios = []
+    for seed in (101, 102):
+        smp = learn.Sample(ctrl, 64, seed, with_probes=False)
+        it_l, it_j = learn.pcg_iterations(ctrl, spai, smp)
+        ratios.append(it_l / it_j)
+    assert max(ratios) < 0.85, ratios
+    spai.release()
+
+
+@pytest.mark.parametrize("inner", ["fp64", "fp32"])
+def test_learned_solver_reaches_fp64_residual(ctrl, inner):
+    spai, _ = learn.train(ctrl, sizes=(32,), seeds=range(2), steps=60, lr=3e-3)
+    smp = learn.Sample(ctrl, 48, 7, with_probes=False)
+    spai.set_matrix(smp.A, ctrl)
+    spai.build(ctrl)
+    n = smp.A.num_rows
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    sc = api.SolverControl(L.DIAGONAL, 100000, 1e-10, 0.0)
+    info = api.cg_learned(x, smp.A, smp.b, sc, spai, ctrl, inner=inner, inner_tol=1e-3)
+    sc.release()
+    rp, c, v = smp.np
+    A = sp.csr_matrix((v, c.astype(np.int64), rp.astype(np.int64)))
+    b = smp.b.cpu().numpy()
+    res = np.linalg.norm(b - A @ x.cpu().numpy()) / np.linalg.norm(b)
+    assert res <= 2e-10, (res, info)
+    spai.release()
