@@ -983,6 +983,9 @@ clsparseStatus pcg_factor_typed(cldenseVector* x, const clsparseCsrMatrix* A, co
 template clsparseStatus pcg_factor_typed<float, float, __nv_bfloat16>(
     cldenseVector*, const clsparseCsrMatrix*, const cldenseVector*, clSParseSolverControl,
     const CsrView<__nv_bfloat16>&, const CsrView<__nv_bfloat16>&, clsparseControl);
+template clsparseStatus pcg_factor_typed<__nv_bfloat16, float, __nv_bfloat16>(
+    cldenseVector*, const clsparseCsrMatrix*, const cldenseVector*, clSParseSolverControl,
+    const CsrView<__nv_bfloat16>&, const CsrView<__nv_bfloat16>&, clsparseControl);
 template clsparseStatus pcg_factor_typed<float, float, float>(cldenseVector*, const clsparseCsrMatrix*,
                                                               const cldenseVector*, clSParseSolverControl,
                                                               const CsrView<float>&, const CsrView<float>&,
