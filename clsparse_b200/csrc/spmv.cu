@@ -210,6 +210,175 @@ __device__ __forceinline__ dev::Acc<T, EXT> range_sum(const V* __restrict__ vals
 constexpr uint32_t kRpStage = kBlkSize + 1;  // row pointers of a STREAM block kept in shared memory
 constexpr uint32_t kStageRow = kBlkSize / 4 + 2;  // quads per block (+1 ragged) + 1 bank skew
 
+// What a 128-position span of a STREAM block hands to the spans after it.
+template <typename T>
+struct SpanCarry {
+    T open;          // sum from the span's last row start to its end (whole span if none)
+    T pend;          // first row end in the span: sum from the span start to it
+    int open_start;  // position of the span's last row start, -1 if none
+    int any;         // the span holds a row start
+    int has_pend;    // the span's first row end continues a row from an earlier span
+};
+
+// STREAM block without staging products: every thread keeps the products of
+// its quads (4 consecutive nonzeros each; a warp covers 128 consecutive
+// positions per span) in registers. Row starts are marked in a bitmap over the
+// block's positions; each warp runs a segmented scan over its span with warp
+// shuffles, rows ending inside the span are written by the lane that sees
+// their end, and rows crossing spans are finished from the per-span carries.
+// Summation order is fixed, so results are reproducible.
+template <typename V, typename T, int K, int NT>
+__device__ __forceinline__ void stream_segmented(const V* __restrict__ vals, const uint32_t* __restrict__ cols,
+                                                 const uint32_t* __restrict__ rp, const T* __restrict__ x,
+                                                 T alpha, uint32_t row, uint32_t nrows, uint32_t nb, uint32_t ne,
+                                                 uint32_t lo, uint32_t hi, bool vec, uint32_t* srp,
+                                                 uint32_t* bits, uint32_t* rid, SpanCarry<T>* spans,
+                                                 RowSink<T, K>& sink) {
+    constexpr int QPT = static_cast<int>(kBlkSize) / 4 / NT;
+    constexpr int NW = NT / 32;
+    constexpr int NREG = QPT * NW;  // regular spans; one more for the ragged quad
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u, warp = tid >> 5;
+    const uint32_t base = nb & ~3u;
+    const uint32_t nq = (ne - base + 3) >> 2;
+    const bool extra = nq > static_cast<uint32_t>(QPT * NT);
+
+    for (uint32_t i = tid; i < kBlkSize / 32 + 8; i += NT) bits[i] = 0u;
+    if (tid < static_cast<uint32_t>(NREG + 1)) {
+        spans[tid].has_pend = 0;
+        spans[tid].any = 0;
+        spans[tid].open = T(0);
+        spans[tid].open_start = -1;
+    }
+    Quad<T> q[QPT];
+#pragma unroll
+    for (int j = 0; j < QPT; ++j) {
+        const uint32_t g = tid + j * NT;
+        if (g < nq)
+            load_quad(vals, cols, base + 4 * g, nb, ne, lo, hi, vec, q[j]);
+        else
+            q[j].mask = 0;
+    }
+    Quad<T> qx[1];
+    qx[0].mask = 0;
+    if (extra && warp == 0 && QPT * NT + lane < nq)
+        load_quad(vals, cols, base + 4 * (QPT * NT + lane), nb, ne, lo, hi, vec, qx[0]);
+    for (uint32_t i = tid; i <= nrows; i += NT) srp[i] = dev::ld_ro(rp + row + i);
+    T xv[QPT][4];
+    gather_quads(x, q, xv);
+    T xx[1][4];
+    gather_quads(x, qx, xx);
+    __syncthreads();
+    // row starts of the non-empty rows; empty rows are final already
+    for (uint32_t r = tid; r < nrows; r += NT) {
+        const uint32_t s = srp[r] - base, e = srp[r + 1] - base;
+        if (e > s) {
+            atomicOr(&bits[s >> 5], 1u << (s & 31u));
+            rid[s] = r;
+        } else {
+            dev::Acc<T, false> z;
+            sink.template put<false>(row + r, z);
+        }
+    }
+    __syncthreads();
+    auto emit = [&](int pos, T total) {
+        dev::Acc<T, false> a;
+        a.s = total;
+        sink.template put<false>(row + rid[pos], a);
+    };
+    // segmented scan of one span; p = this lane's four products, qd its quad
+    auto span = [&](int S, uint32_t qd, const T (&p)[4]) {
+        const uint32_t pos0 = 4u * qd;
+        const uint32_t fl = (bits[pos0 >> 5] >> (pos0 & 31u)) & 0xFu;
+        T head = T(0), run = T(0);
+        int cur = -1;
+        bool seen = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (fl & (1u << k)) {
+                if (!seen) {
+                    head = run;
+                    seen = true;
+                } else {
+                    emit(cur, run);  // a row that starts and ends inside this quad
+                }
+                run = T(0);
+                cur = static_cast<int>(pos0) + k;
+            }
+            run += p[k];
+        }
+        if (!seen) head = run;
+        T v = run;
+        int f = seen ? 1 : 0;
+        int sp = seen ? cur : -1;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const T vu = __shfl_up_sync(0xffffffffu, v, off);
+            const int fu = __shfl_up_sync(0xffffffffu, f, off);
+            const int su = __shfl_up_sync(0xffffffffu, sp, off);
+            if (lane >= static_cast<uint32_t>(off)) {
+                if (!f) {
+                    v += vu;
+                    sp = su;
+                }
+                f |= fu;
+            }
+        }
+        T rp_ = __shfl_up_sync(0xffffffffu, v, 1);
+        int fp = __shfl_up_sync(0xffffffffu, f, 1);
+        int spp = __shfl_up_sync(0xffffffffu, sp, 1);
+        if (lane == 0) {
+            rp_ = T(0);
+            fp = 0;
+            spp = -1;
+        }
+        if (seen) {
+            const T total = rp_ + head;  // the row ending at this lane's first start
+            if (fp) {
+                emit(spp, total);
+            } else {
+                spans[S].pend = total;
+                spans[S].has_pend = 1;
+            }
+        }
+        if (lane == 31) {
+            spans[S].open = v;
+            spans[S].open_start = f ? sp : -1;
+            spans[S].any = f;
+        }
+    };
+#pragma unroll
+    for (int j = 0; j < QPT; ++j) {
+        T p[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            p[k] = (q[j].mask & (1u << k)) ? dev::mul_rn(alpha * q[j].v[k], xv[j][k]) : T(0);
+        span(j * NW + static_cast<int>(warp), j * NT + tid, p);
+    }
+    if (extra && warp == 0) {
+        T p[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            p[k] = (qx[0].mask & (1u << k)) ? dev::mul_rn(alpha * qx[0].v[k], xx[0][k]) : T(0);
+        span(NREG, QPT * NT + lane, p);
+    }
+    __syncthreads();
+    // rows that cross spans: the first row end of a span (and the block end)
+    const int nspans = NREG + (extra ? 1 : 0);
+    if (tid <= static_cast<uint32_t>(nspans)) {
+        const int S = static_cast<int>(tid);
+        if (S == nspans || spans[S].has_pend) {
+            T total = S < nspans ? spans[S].pend : T(0);
+            int s = S - 1;
+            while (s >= 0 && !spans[s].any) {
+                total += spans[s].open;
+                --s;
+            }
+            if (s >= 0 && spans[s].open_start >= 0) emit(spans[s].open_start, total + spans[s].open);
+        }
+    }
+}
+
 template <typename V, typename T, bool EXT, int K, int NT>
 __global__ void __launch_bounds__(NT)
     csr_adaptive_kernel(const V* __restrict__ vals, const uint32_t* __restrict__ cols,
@@ -228,6 +397,12 @@ __global__ void __launch_bounds__(NT)
     __shared__ T red_s[32];
     __shared__ T red_c[32];
     __shared__ bool lr_last;
+    // segmented STREAM reduction: row-start bitmap over the block's positions,
+    // the block row starting at each flagged position, per-span carries
+    constexpr int kSpans = static_cast<int>(kBlkSize) / 128 + 1;
+    __shared__ uint32_t seg_bits[kBlkSize / 32 + 8];
+    __shared__ uint32_t seg_row[kBlkSize + 8];
+    __shared__ SpanCarry<T> spans[kSpans];
 
     if (epi.done != nullptr && *epi.done) return;
 
@@ -249,7 +424,11 @@ __global__ void __launch_bounds__(NT)
         const uint32_t nrows = stop - row;
         const uint32_t tid = threadIdx.x;
 
-        if (nrows > kRowsForVector) {
+        if (nrows > kRowsForVector && !EXT && ne - nb <= kBlkSize && nrows < kRpStage) {
+            // ---- STREAM, segmented: products stay in registers ----
+            stream_segmented<V, T, K, NT>(vals, cols, rp, x, alpha, row, nrows, nb, ne, lo, hi, vec != 0,
+                                          srp, seg_bits, seg_row, spans, sink);
+        } else if (nrows > kRowsForVector) {
             // ---- STREAM: several short rows, <= kBlkSize nonzeros in total ----
             const uint32_t cnt = ne - nb;
             // A block from clsparseCsrMetaCreate never exceeds the staging
@@ -456,12 +635,14 @@ cudaError_t launch_vector(const CsrView<V>& A, const T* alpha, const T* beta, co
 
 #include "spmv_tma.cuh"
 
-// Adaptive kernel choice: the TMA-staged pipeline (default) or the plain
-// one-CTA-per-block kernel (CLSPARSE_B200_SPMV_KERNEL=plain).
+// Adaptive kernel choice: one CTA per row block (default) or the TMA-staged
+// persistent pipeline (CLSPARSE_B200_SPMV_KERNEL=tma), which measured slower
+// on the irregular workload (its per-block barriers leave too little work in
+// flight per SM).
 bool use_tma_kernel() {
     static bool on = [] {
         const char* e = std::getenv("CLSPARSE_B200_SPMV_KERNEL");
-        return !(e && std::string(e) == "plain");
+        return e && std::string(e) == "tma";
     }();
     return on;
 }
