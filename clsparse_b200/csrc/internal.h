@@ -94,6 +94,7 @@ struct matrix_meta {
     cl_ulong* d_rowBlocks = nullptr;    // device copy of the words
     std::vector<cl_ulong> h_rowBlocks;  // host copy (for inspection)
     uint32_t* d_word_nnz = nullptr;     // row_pointer[first row of word w], one per word
+    std::vector<uint32_t> h_word_nnz;   // host copy (static CTA partitions of the persistent solvers)
     double* d_lr_partial = nullptr;     // one partial sum per row-block word (long rows)
     uint32_t* d_lr_ticket = nullptr;    // one arrival counter per row-block word (long rows)
     int* d_error = nullptr;             // set by an SpMV whose bounded barrier wait timed out

@@ -256,6 +256,7 @@ clsparseStatus clsparseCsrMetaCreate(clsparseCsrMatrix* csrMatx, clsparseControl
     if (e == cudaSuccess) e = cudaMemsetAsync(meta->d_error, 0, sizeof(int), control->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(control->stream);
     if (e != cudaSuccess) return clsparseInvalidKernelExecution;
+    meta->h_word_nnz = std::move(word_nnz);
     csrMatx->meta = meta.release();
     return clsparseSuccess;
 }
