@@ -55,6 +55,31 @@ __device__ __forceinline__ float ld_gather(const float* p) {
 #endif
 }
 
+// Coherent gather for kernels that read a vector other CTAs of the same
+// launch wrote before a grid barrier (the persistent solvers): a plain weak
+// load, which the barrier's acquire orders, never the non-coherent
+// read-only path (whose data must not change while the kernel runs).
+__device__ __forceinline__ double ld_coherent(const double* p) {
+    double v;
+    asm volatile("ld.global.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float ld_coherent(const float* p) {
+    float v;
+    asm volatile("ld.global.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+
+// Gather of x[c]: read-only path, or coherent when COH.
+template <bool COH, typename T>
+__device__ __forceinline__ T ld_x(const T* p) {
+    if constexpr (COH) {
+        return ld_coherent(p);
+    } else {
+        return ld_gather(p);
+    }
+}
+
 // Loads one matrix value (double, float or bf16) as the arithmetic type T.
 template <typename T, typename V>
 __device__ __forceinline__ T ld_val(const V* p) {

@@ -574,8 +574,14 @@ struct Graph {
     double *G64 = nullptr, *GT64 = nullptr;
     bool built = false;
     int device = 0;
+    // CSR-Adaptive metas of the patterns of G (L) and G^T (L^T), so the
+    // solvers apply the factor with the row-block kernels
+    matrix_meta* metaL = nullptr;
+    matrix_meta* metaLT = nullptr;
 
     void release() {
+        delete metaL;
+        delete metaLT;
         void* ptrs[] = {ehat, dinvs, Lrp, Lcol, Le, LTrp, LTrow, LTidx, Boff, B, F, Hp, Hq, g, dg, dH, dHn, dS,
                         dHu, dHp, dHq, part, pw, pu, pv, pdv, pdu, red, ticket, G32, GT32, G16, GT16, G64, GT64};
         for (void* p : ptrs)
@@ -754,6 +760,20 @@ clsparseStatus build_graph(_clsparseB200Spai* net, const clsparseCsrMatrix* A, c
     cudaMemsetAsync(gr.ticket, 0, 16, s);
     node_features<<<nblk(n, 256), 256, 0, s>>>(gr.rp, gr.cols, gr.ehat, gr.F, n);
     if (cudaStreamSynchronize(s) != cudaSuccess) return clsparseInvalidKernelExecution;
+    {
+        clsparseCsrMatrix pat;
+        std::memset(&pat, 0, sizeof(pat));
+        pat.num_rows = n;
+        pat.num_cols = n;
+        pat.num_nonzeros = nnzL;
+        pat.row_pointer = gr.Lrp;
+        if (clsparseCsrMetaCreate(&pat, c) != clsparseSuccess) return clsparseOutOfResources;
+        gr.metaL = static_cast<matrix_meta*>(pat.meta);
+        pat.meta = nullptr;
+        pat.row_pointer = gr.LTrp;
+        if (clsparseCsrMetaCreate(&pat, c) != clsparseSuccess) return clsparseOutOfResources;
+        gr.metaLT = static_cast<matrix_meta*>(pat.meta);
+    }
     gr.built = true;
     return clsparseSuccess;
 }
@@ -1069,12 +1089,12 @@ bool spai_factor_views(clsparseB200Spai net, CsrView<__nv_bfloat16>& G16, CsrVie
                        CsrView<float>& G32, CsrView<float>& GT32, CsrView<double>& G64, CsrView<double>& GT64) {
     if (net == nullptr || !net->gr.built) return false;
     const Graph& gr = net->gr;
-    G16 = CsrView<__nv_bfloat16>{gr.G16, gr.Lcol, gr.Lrp, gr.n, gr.n, gr.nnzL, nullptr};
-    GT16 = CsrView<__nv_bfloat16>{gr.GT16, gr.LTrow, gr.LTrp, gr.n, gr.n, gr.nnzL, nullptr};
-    G32 = CsrView<float>{gr.G32, gr.Lcol, gr.Lrp, gr.n, gr.n, gr.nnzL, nullptr};
-    GT32 = CsrView<float>{gr.GT32, gr.LTrow, gr.LTrp, gr.n, gr.n, gr.nnzL, nullptr};
-    G64 = CsrView<double>{gr.G64, gr.Lcol, gr.Lrp, gr.n, gr.n, gr.nnzL, nullptr};
-    GT64 = CsrView<double>{gr.GT64, gr.LTrow, gr.LTrp, gr.n, gr.n, gr.nnzL, nullptr};
+    G16 = CsrView<__nv_bfloat16>{gr.G16, gr.Lcol, gr.Lrp, gr.n, gr.n, gr.nnzL, gr.metaL};
+    GT16 = CsrView<__nv_bfloat16>{gr.GT16, gr.LTrow, gr.LTrp, gr.n, gr.n, gr.nnzL, gr.metaLT};
+    G32 = CsrView<float>{gr.G32, gr.Lcol, gr.Lrp, gr.n, gr.n, gr.nnzL, gr.metaL};
+    GT32 = CsrView<float>{gr.GT32, gr.LTrow, gr.LTrp, gr.n, gr.n, gr.nnzL, gr.metaLT};
+    G64 = CsrView<double>{gr.G64, gr.Lcol, gr.Lrp, gr.n, gr.n, gr.nnzL, gr.metaL};
+    GT64 = CsrView<double>{gr.GT64, gr.LTrow, gr.LTrp, gr.n, gr.n, gr.nnzL, gr.metaLT};
     return true;
 }
 

@@ -73,7 +73,7 @@ struct _clsparseControl {
     size_t l2_bytes = 0;
     bool async = false;
     bool extended_precision = false;
-    int solver_loop_mode = 0;       // 0 graph while-loop, 1 host chunks
+    int solver_loop_mode = 0;       // 0 graph while-loop, 1 host chunks, 2 persistent kernel
     cudaEvent_t event = nullptr;    // recorded after each call
     cudaStream_t capture_stream = nullptr;  // private stream used for graph capture
     // Reduction scratch: kMaxReduceCtas doubles x 4 partial slots + a ticket.

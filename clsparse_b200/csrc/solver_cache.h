@@ -28,6 +28,8 @@ struct SolverCache {
     DeviceBuffer vecs;
     DeviceBuffer parts;
     DeviceBuffer state;
+    DeviceBuffer fused;      // persistent solver: barrier area + per-CTA word ranges
+    uint32_t fused_grid = 0; // grid the word ranges in `fused` were made for (0: none)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     void drop_graph() {

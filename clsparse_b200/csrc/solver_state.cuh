@@ -18,6 +18,7 @@ enum : int {
     kStatusCurvature = 4,
     kStatusBicgBreakdown = 8,
     kStatusNonFinite = 16,
+    kStatusBarrierTimeout = 32,  // a persistent solver's grid barrier wait ran out
 };
 
 template <typename T>

@@ -28,6 +28,7 @@
 
 #include "device_common.cuh"
 #include "internal.h"
+#include "fused.h"
 #include "solver_cache.h"
 #include "solver_state.cuh"
 
@@ -500,13 +501,13 @@ __global__ void __launch_bounds__(kThreads) pcg_p_kernel(PcgArgs<T> a) {
 // ---------------------------------------------------------- driver ----
 
 // Runs prologue / body / epilogue either as one graph with a conditional
-// WHILE node around the body (mode 0) or as host-enqueued chunks of bodies
-// that return at once after the device set done (mode 1).
+// WHILE node around the body (modes 0 and 2) or as host-enqueued chunks of
+// bodies that return at once after the device set done (mode 1).
 template <typename Pro, typename Body, typename Epi>
 clsparseStatus run_solve(clsparseControl c, SolverCache& cache, bool rebuild, const int* d_done,
                          int max_iters, Pro prologue, Body body, Epi epilogue) {
     cudaStream_t s = c->stream;
-    if (c->solver_loop_mode == 0) {
+    if (c->solver_loop_mode != 1) {
         if (rebuild || cache.exec == nullptr) {
             cache.drop_graph();
             cudaStream_t cs = c->capture_stream;
@@ -626,6 +627,7 @@ clsparseStatus read_back(clsparseControl c, SolverCache& cache, clSParseSolverCo
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return clsparseInvalidKernelExecution;
     if (c->event) cudaEventRecord(c->event, c->stream);
     sc->deviceStatus = static_cast<cl_uint>(h->status_bits);
+    if (h->status_bits & kStatusBarrierTimeout) return clsparseInvalidKernelExecution;
     if (h->zero_b) {
         // conjugate-gradients.hpp:87-95 resets the tolerances of the control
         sc->nIters = 0;
@@ -683,6 +685,64 @@ clsparseStatus prepare_cache(clsparseControl c, SolverCache& cache, const Solver
     }
     cache.key = key;
     cache.valid = true;
+    return clsparseSuccess;
+}
+
+// Whether the persistent kernel can run this solve: loop mode 2 and a
+// CSR-Adaptive meta (with its host word offsets) on every matrix it reads.
+bool fused_ok(clsparseControl c, const matrix_meta* m) {
+    return c->solver_loop_mode == 2 && m != nullptr && m->num_words >= 2 &&
+           m->h_word_nnz.size() == m->num_words;
+}
+
+size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+// Launches the persistent solver: sizes the barrier area, makes the per-CTA
+// word ranges of A (and G, Gt) when the operands or the grid changed, zeroes
+// the barrier counters and launches one cooperative kernel.
+template <typename V, typename T, typename VG>
+clsparseStatus run_fused(clsparseControl c, SolverCache& cache, bool rebuild, FusedCgArgs<V, T, VG>& fa,
+                         const CsrView<V>& Av, const CsrView<VG>* G, const CsrView<VG>* Gt, int pk) {
+    const bool ext = c->extended_precision && pk == 0;
+    // all CTAs resident, and no more CTAs than A has row-block words
+    const uint32_t words = static_cast<uint32_t>(Av.meta->num_words - 1);
+    const uint32_t grid = std::min(fused_grid<V, T, VG>(c->sm_count, ext, pk), std::max(1u, words));
+    const size_t sync_b = align256(fused_sync_bytes(grid));
+    const size_t wb = align256((static_cast<size_t>(grid) + 1) * sizeof(uint32_t));
+    if (cache.fused.ensure(sync_b + 3 * wb) != cudaSuccess) {
+        cudaGetLastError();
+        return clsparseOutOfResources;
+    }
+    char* base = static_cast<char*>(cache.fused.ptr);
+    uint32_t* wA = reinterpret_cast<uint32_t*>(base + sync_b);
+    uint32_t* wG = reinterpret_cast<uint32_t*>(base + sync_b + wb);
+    uint32_t* wGt = reinterpret_cast<uint32_t*>(base + sync_b + 2 * wb);
+    if (rebuild || cache.fused_grid != grid) {
+        std::vector<uint32_t> part;
+        const CsrView<VG>* mats[2] = {G, Gt};
+        uint32_t* dst[2] = {wG, wGt};
+        word_partition(Av.meta, grid, part);
+        cudaError_t e = cudaMemcpy(wA, part.data(), part.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+        for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+            if (!mats[k]) continue;
+            word_partition(mats[k]->meta, grid, part);
+            e = cudaMemcpy(dst[k], part.data(), part.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) {
+            cache.fused_grid = 0;
+            return clsparseInvalidKernelExecution;
+        }
+        cache.fused_grid = grid;
+    }
+    if (cudaMemsetAsync(base, 0, kFusedSyncHead, c->stream) != cudaSuccess) return clsparseInvalidKernelExecution;
+    fa.sync = fused_sync_at(base);
+    fa.A = word_mat(Av, wA);
+    if (G) fa.G = word_mat(*G, wG);
+    if (Gt) fa.Gt = word_mat(*Gt, wGt);
+    if (launch_pcg_fused<V, T, VG>(fa, grid, ext, pk, c->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return clsparseInvalidKernelExecution;
+    }
     return clsparseSuccess;
 }
 
@@ -758,7 +818,20 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
         sc->nIters = 0;
         return clsparseSuccess;
     }
-    stt = run_solve(c, cache, rebuild, &st->done, sc->maxIters, prologue, body, epilogue);
+    if (fused_ok(c, Av.meta)) {
+        FusedCgArgs<V, T, T> fa{};
+        fa.x = a.x;
+        fa.b = a.b;
+        fa.q = a.y;
+        fa.r = a.r;
+        fa.p = a.p;
+        fa.invD = a.invD ? invD : nullptr;
+        fa.st = st;
+        fa.n = static_cast<uint32_t>(n);
+        stt = run_fused<V, T, T>(c, cache, rebuild, fa, Av, nullptr, nullptr, 0);
+    } else {
+        stt = run_solve(c, cache, rebuild, &st->done, sc->maxIters, prologue, body, epilogue);
+    }
     if (stt != clsparseSuccess) {
         cache.valid = false;
         cache.drop_graph();
@@ -963,7 +1036,21 @@ clsparseStatus pcg_factor_solve(cldenseVector* xv, const clsparseCsrMatrix* A, c
         sc->nIters = 0;
         return clsparseSuccess;
     }
-    stt = run_solve(c, cache, rebuild, &st->done, sc->maxIters, prologue, body, epilogue);
+    if (fused_ok(c, Av.meta) && fused_ok(c, G.meta) && fused_ok(c, Gt.meta)) {
+        FusedCgArgs<V, T, VG> fa{};
+        fa.x = a.x;
+        fa.b = a.b;
+        fa.q = a.q;
+        fa.r = a.r;
+        fa.p = a.p;
+        fa.t = a.t;
+        fa.z = a.z;
+        fa.st = st;
+        fa.n = static_cast<uint32_t>(n);
+        stt = run_fused<V, T, VG>(c, cache, rebuild, fa, Av, &G, &Gt, 1);
+    } else {
+        stt = run_solve(c, cache, rebuild, &st->done, sc->maxIters, prologue, body, epilogue);
+    }
     if (stt != clsparseSuccess) {
         cache.valid = false;
         cache.drop_graph();

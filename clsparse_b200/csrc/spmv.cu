@@ -50,8 +50,8 @@ __global__ void __launch_bounds__(NT)
     RowSink<T, K> sink;
     sink.init(y, epi, *beta_p);
     if (blockIdx.x < nblocks)
-        adaptive_word<V, T, EXT, K, NT>(blockIdx.x, vals, cols, rp, x, alpha, words, word_nnz, lo, hi, vec,
-                                        lr_partial, lr_ticket, sm, sink);
+        adaptive_word<V, T, EXT, NT>(blockIdx.x, vals, cols, rp, DenseX<T>{x}, alpha, words, word_nnz, lo, hi,
+                                     vec, lr_partial, lr_ticket, sm, sink);
     run_epilogue<T, K>(sink, epi);
 }
 

@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(kThreads, EXT ? 1 : 2)
                 }
             } else if (d.kind == kVector) {
                 dev::Acc<T, EXT> a =
-                    range_sum<V, T, EXT, kConsumers>(vals, cols, x, alpha, d.nb, d.ne, 0u, hi, aligned != 0);
+                    range_sum<V, T, EXT, kConsumers>(vals, cols, DenseX<T>{x}, alpha, d.nb, d.ne, 0u, hi, aligned != 0);
                 a = consumer_reduce(a, red_s, red_c);
                 if (tid == 0) sink.template put<EXT>(d.row, a);
             } else if (d.kind == kLong) {
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(kThreads, EXT ? 1 : 2)
                     const uint32_t cb = d.nb + d.low * kLongChunk;
                     const uint32_t ce = min(re, cb + kLongChunk);
                     dev::Acc<T, EXT> a =
-                        range_sum<V, T, EXT, kConsumers>(vals, cols, x, alpha, cb, ce, 0u, hi, aligned != 0);
+                        range_sum<V, T, EXT, kConsumers>(vals, cols, DenseX<T>{x}, alpha, cb, ce, 0u, hi, aligned != 0);
                     a = consumer_reduce(a, red_s, red_c);
                     if (tid == 0) {
                         lr_partial[gid] = static_cast<double>(a.value());

@@ -146,21 +146,29 @@ __device__ __forceinline__ void load_quad(const V* __restrict__ vals, const uint
     }
 }
 
-template <typename T, int N>
-__device__ __forceinline__ void gather_quads(const T* __restrict__ x, const Quad<T> (&q)[N], T (&xv)[N][4]) {
+// Source of the gathered vector entries x[c]: the dense vector itself
+// (read-only path, or coherent when other CTAs of the launch wrote it).
+template <typename T, bool COH = false>
+struct DenseX {
+    const T* x;
+    __device__ __forceinline__ T operator()(uint32_t c) const { return dev::ld_x<COH>(x + c); }
+};
+
+template <int N, typename T, typename XS>
+__device__ __forceinline__ void gather_quads(const XS& xs, const Quad<T> (&q)[N], T (&xv)[N][4]) {
 #pragma unroll
     for (int j = 0; j < N; ++j)
 #pragma unroll
-        for (int k = 0; k < 4; ++k) xv[j][k] = (q[j].mask & (1u << k)) ? dev::ld_gather(x + q[j].c[k]) : T(0);
+        for (int k = 0; k < 4; ++k) xv[j][k] = (q[j].mask & (1u << k)) ? xs(q[j].c[k]) : T(0);
 }
 
 // Sum of alpha*a_j*x[col_j] over [cb, ce) by the whole CTA (VECTOR rows and
 // LONG chunks). Each round a thread has two quads (8 nonzeros) in flight
 // before it gathers x.
-template <typename V, typename T, bool EXT, int NT>
+template <typename V, typename T, bool EXT, int NT, typename XS>
 __device__ __forceinline__ dev::Acc<T, EXT> range_sum(const V* __restrict__ vals,
                                                       const uint32_t* __restrict__ cols,
-                                                      const T* __restrict__ x, T alpha, uint32_t cb,
+                                                      const XS& x, T alpha, uint32_t cb,
                                                       uint32_t ce, uint32_t lo, uint32_t hi, bool vec) {
     dev::Acc<T, EXT> a;
     const uint32_t base = cb & ~3u;
@@ -177,7 +185,7 @@ __device__ __forceinline__ dev::Acc<T, EXT> range_sum(const V* __restrict__ vals
                 q[u].mask = 0;
         }
         T xv[U][4];
-        gather_quads(x, q, xv);
+        gather_quads<U>(x, q, xv);
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
@@ -205,17 +213,18 @@ struct WordSmem {
 };
 
 // Processes row-block word `gid` (0 <= gid < number of words - 1) with the
-// whole CTA (NT threads). Every row the word finishes goes through `sink`.
-// The caller separates two calls on the same shared memory with a barrier.
-template <typename V, typename T, bool EXT, int K, int NT>
+// whole CTA (NT threads). x(c) yields the vector entry of column c; every row
+// the word finishes goes through sink.put. The caller separates two calls on
+// the same shared memory with a barrier.
+template <typename V, typename T, bool EXT, int NT, typename XS, typename Sink>
 __device__ __forceinline__ void adaptive_word(uint32_t gid, const V* __restrict__ vals,
                                               const uint32_t* __restrict__ cols,
-                                              const uint32_t* __restrict__ rp, const T* __restrict__ x,
+                                              const uint32_t* __restrict__ rp, const XS& x,
                                               T alpha, const uint64_t* __restrict__ words,
                                               const uint32_t* __restrict__ word_nnz, uint32_t lo,
                                               uint32_t hi, int vec, double* __restrict__ lr_partial,
                                               uint32_t* __restrict__ lr_ticket, WordSmem<T>& sm,
-                                              RowSink<T, K>& sink) {
+                                              Sink& sink) {
     T* stage = sm.stage;
     uint32_t* srp = sm.srp;
     // Independent loads: the block's words and the nonzero offsets of
@@ -253,7 +262,7 @@ __device__ __forceinline__ void adaptive_word(uint32_t gid, const V* __restrict_
             if (rp_staged)
                 for (uint32_t i = tid; i <= nrows; i += NT) srp[i] = dev::ld_ro(rp + row + i);
             T xv[QPT][4];
-            gather_quads(x, q, xv);
+            gather_quads<QPT>(x, q, xv);
 #pragma unroll
             for (int j = 0; j < QPT; ++j) {
                 const uint32_t e0 = base + 4 * (tid + j * NT);
@@ -267,7 +276,7 @@ __device__ __forceinline__ void adaptive_word(uint32_t gid, const V* __restrict_
                 Quad<T> r[1];
                 load_quad(vals, cols, base + 4 * g, nb, ne, lo, hi, vec != 0, r[0]);
                 T rv[1][4];
-                gather_quads(x, r, rv);
+                gather_quads<1>(x, r, rv);
 #pragma unroll
                 for (int k = 0; k < 4; ++k)
                     if (r[0].mask & (1u << k)) stage[k * kStageRow + g] = dev::mul_rn(alpha * r[0].v[k], rv[0][k]);
@@ -298,7 +307,7 @@ __device__ __forceinline__ void adaptive_word(uint32_t gid, const V* __restrict_
                         }
                     } else {
                         for (uint32_t j = nb + f + lane; j < nb + l; j += G)
-                            a.add(dev::mul_rn(alpha * dev::ld_val<T>(vals + j), dev::ld_ro(x + cols[j])));
+                            a.add(dev::mul_rn(alpha * dev::ld_val<T>(vals + j), x(cols[j])));
                     }
                 }
                 dev::group_reduce<G>(a);

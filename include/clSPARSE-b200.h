@@ -180,8 +180,11 @@ cldenseDdotNoAlloc(clsparseScalar* r, const cldenseVector* x, const cldenseVecto
 
 /* Solver loop driver: 0 = one CUDA graph per solve with a device-side
  * conditional WHILE node (no host round trip per iteration, the default);
- * 1 = host-enqueued chunks of iterations with a device done flag. Both give
- * the same iterates. */
+ * 1 = host-enqueued chunks of iterations with a device done flag (same
+ * iterates as 0); 2 = CG and factorized PCG as ONE persistent cooperative
+ * kernel per solve (grid-wide exchanges between phases; needs a
+ * CSR-Adaptive meta, otherwise and for BiCGStab the solve runs as in 0;
+ * iterates equal up to reduction order). */
 CLSPARSE_EXPORT clsparseStatus
 clsparseB200SetSolverLoopMode(clsparseControl control, cl_int mode);
 

@@ -47,17 +47,18 @@ PROBLEMS = {
 }
 
 
+@pytest.mark.parametrize("loop_mode", [0, 2], ids=["graph", "persistent"])
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
 @pytest.mark.parametrize("precond", [L.DIAGONAL, L.NOPRECOND], ids=["jacobi", "none"])
 @pytest.mark.parametrize("prob", sorted(PROBLEMS))
 @pytest.mark.parametrize("kind", ["cg", "bicgstab"])
-def test_solver_parity(ctrl, orc, kind, prob, precond, dtype):
+def test_solver_parity(ctrl, orc, kind, prob, precond, dtype, loop_mode):
     rp, col, val = PROBLEMS[prob]()
     n = len(rp) - 1
     b = np.random.default_rng(1).uniform(-1, 1, n)
     rel = 1e-10 if dtype == torch.float64 else 1e-5
     t = NP[dtype]
-    x, info, _ = run(ctrl, kind, rp, col, val, np.zeros(n), b, dtype, precond, 5000, rel, 0.0)
+    x, info, _ = run(ctrl, kind, rp, col, val, np.zeros(n), b, dtype, precond, 5000, rel, 0.0, loop_mode=loop_mode)
     xo, oi = orc.solve(kind, t, rp, col, val, np.zeros(n, t), np.asarray(b, t), precond, 5000, rel, 0.0)
     # BiCGStab's convergence history is irregular and reacts to the order of
     # the reduction sums; CG's is smooth.
@@ -80,6 +81,52 @@ def test_solver_loop_modes_agree(ctrl, kind):
                     loop_mode=1)
     assert i0 == i1
     assert np.array_equal(x0, x1)
+
+
+@pytest.mark.parametrize("ext", [False, True], ids=["plain", "extended"])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+def test_persistent_cg_matches_graph_form(ctrl, dtype, ext):
+    """Loop mode 2 (one cooperative launch per solve) against the graph form:
+    same stop decision up to reduction order, same answer to the tolerance."""
+    rp, col, val = matgen.diffusion3d_lognormal(24, sigma=1.0, seed=4)
+    n = len(rp) - 1
+    b = np.random.default_rng(6).uniform(-1, 1, n)
+    rel = 1e-10 if dtype == torch.float64 else 1e-5
+    ctrl.enable_extended_precision(ext)
+    try:
+        xg, ig, _ = run(ctrl, "cg", rp, col, val, np.zeros(n), b, dtype, L.DIAGONAL, 5000, rel, 0.0, loop_mode=0)
+        xp, ip, _ = run(ctrl, "cg", rp, col, val, np.zeros(n), b, dtype, L.DIAGONAL, 5000, rel, 0.0, loop_mode=2)
+    finally:
+        ctrl.enable_extended_precision(False)
+    assert abs(ip["nIters"] - ig["nIters"]) <= max(2, int(0.02 * ig["nIters"]))
+    assert ip["initialResidual"] == pytest.approx(ig["initialResidual"], rel=1e-6)
+    assert ip["currentResidual"] <= rel
+    tol = 1e-7 if dtype == torch.float64 else 1e-2
+    assert np.linalg.norm(xp - xg) <= tol * np.linalg.norm(xg)
+
+
+def test_persistent_cg_long_rows(ctrl, orc):
+    """An SPD arrow matrix whose first row and column are dense (the row
+    becomes LONG row-block words): the persistent solver's long-row merge."""
+    n = 40000
+    rng = np.random.default_rng(8)
+    import scipy.sparse as sp
+    off = sp.random(n, n, density=3.0 / n, random_state=3, format="csr")
+    arrow = sp.lil_matrix((n, n))
+    arrow[0, 1:] = rng.uniform(-1, 1, n - 1) * 1e-3
+    arrow = arrow.tocsr()
+    S = off + off.T + arrow + arrow.T
+    S = S.tocsr()
+    d = np.asarray(abs(S).sum(axis=1)).ravel() + 1.0
+    S = (S + sp.diags(d)).tocsr()
+    S.sort_indices()
+    rp, col, val = S.indptr.astype(np.uint32), S.indices.astype(np.uint32), S.data
+    b = rng.uniform(-1, 1, n)
+    x, info, _ = run(ctrl, "cg", rp, col, val, np.zeros(n), b, torch.float64, L.DIAGONAL, 2000, 1e-10, 0.0,
+                     loop_mode=2)
+    _, oi = orc.solve("cg", np.float64, rp, col, val, np.zeros(n), b, 1, 2000, 1e-10, 0.0)
+    assert abs(info["nIters"] - oi.nIters) <= 3
+    assert l1_residual(rp, col, val, x, b) <= 1e-9
 
 
 @pytest.mark.parametrize("kind", ["cg", "bicgstab"])

@@ -93,8 +93,10 @@ def test_training_reduces_loss_and_beats_jacobi(ctrl):
     spai.release()
 
 
+@pytest.mark.parametrize("loop_mode", [0, 2], ids=["graph", "persistent"])
 @pytest.mark.parametrize("inner", ["fp64", "fp32"])
-def test_learned_solver_reaches_fp64_residual(ctrl, inner):
+def test_learned_solver_reaches_fp64_residual(ctrl, inner, loop_mode):
+    ctrl.set_solver_loop_mode(loop_mode)
     spai, _ = learn.train(ctrl, sizes=(32,), seeds=range(2), steps=60, lr=3e-3)
     smp = learn.Sample(ctrl, 48, 7, with_probes=False)
     spai.set_matrix(smp.A, ctrl)
