@@ -188,17 +188,28 @@ template <typename V, typename T>
 cudaError_t launch_csrmv(const CsrView<V>& A, const T* alpha, const T* beta, const T* x, T* y,
                          bool extended, const SpmvEpilogue& epi, cudaStream_t s);
 
+// Continuation of an inner solve of the mixed-precision refinement: with
+// `warm`, the solve starts from x == 0 with r = b (the replaced residual) and
+// keeps the previous solve's search direction p, forming
+// p = z + (<r,z> / rz) p; on return rz holds the denominator for the next
+// continuation. The previous solve must have run on the same operands and
+// control.
+struct WarmStart {
+    bool warm = false;
+    double rz = 0.0;
+};
+
 // CG with matrix values of type V and vectors in T (solvers.cu); the drop-in
 // entry points use V == T, the mixed-precision refinement uses float / bf16.
 template <typename V, typename T>
 clsparseStatus cg_solve_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
-                              clSParseSolverControl sc, clsparseControl c);
+                              clSParseSolverControl sc, clsparseControl c, WarmStart* ws = nullptr);
 
 // PCG with the factorized preconditioner M^-1 = G^T G (solvers.cu).
 template <typename V, typename T, typename VG>
 clsparseStatus pcg_factor_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
                                 clSParseSolverControl sc, const CsrView<VG>& G, const CsrView<VG>& Gt,
-                                clsparseControl c);
+                                clsparseControl c, WarmStart* ws = nullptr);
 
 // Device views of a learned factor G (L = tril(A) order) and G^T (gnn.cu).
 bool spai_factor_views(clsparseB200Spai net, CsrView<__nv_bfloat16>& G16, CsrView<__nv_bfloat16>& GT16,

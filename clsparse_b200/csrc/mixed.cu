@@ -3,11 +3,18 @@
 //
 // Outer loop, all in FP64 on the device: r = b - A x with the FP64 matrix,
 // ||r||_2 / ||b||_2 is the stop test. Inner solve: Jacobi-PCG (the library's
-// own CG, in the graph/while-loop form) on A d = r / ||b||_2 with the matrix
-// values rounded to FP32 or BF16 (column indices, row pointers and the
-// CSR-Adaptive meta are shared with the FP64 matrix) and FP32 vectors,
-// accumulated in FP32. Then x += ||b||_2 * d in FP64. The inner tolerance is
-// relative (L2) to the inner right-hand side.
+// own CG) on A d = r / ||b||_2 with the matrix values rounded to FP32 or BF16
+// (column indices, row pointers and the CSR-Adaptive meta are shared with the
+// FP64 matrix) and FP32 vectors, accumulated in FP32. Then x += ||b||_2 * d
+// in FP64. The inner tolerance is relative (L2) to the inner right-hand side.
+//
+// The inner solves are not restarts: after the first, each continues the
+// previous one's search direction with only the residual replaced by the new
+// FP64 true residual ("reliable updates" / residual replacement: G. Sleijpen
+// and H. van der Vorst, Computing 56 (1996); H. van der Vorst and Q. Ye, SIAM
+// J. Sci. Comput. 22 (2000)). A restarted CG throws away its Krylov space at
+// every refinement step and, on ill-conditioned systems, needs about twice
+// the FP64 iteration count; the continued one stays close to it.
 #include <cmath>
 #include <cstring>
 
@@ -122,6 +129,10 @@ clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const clden
     const int max_inner_total = sc->maxIters;
     double bnorm = -1.0, res = 0.0, prev = 1e300;
     int outer = 0, inner_total = 0, stalls = 0;
+    WarmStart ws;              // continuation of the previous inner solve
+    bool have_prev = false;    // an inner solve ran whose direction can be continued
+    bool prev_factor = false;  // ... and it used the learned factor
+    double predicted = 0.0;    // true residual the last inner solve's recursion promises
     double* hres = static_cast<double*>(w.pinned);
     const uint32_t g = grid_for(n, c->sm_count);
     clsparseStatus st = clsparseSuccess;
@@ -161,7 +172,8 @@ clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const clden
         if (inner_total >= max_inner_total) break;
         // The learned factor stalls when an outer step fails to halve the
         // residual or its inner solve broke down: continue with Jacobi.
-        if (use_factor && outer > 0 && (res > 0.5 * prev || (inner.deviceStatus & 0x14u))) {
+        const bool breakdown = (inner.deviceStatus & 0x14u) != 0;
+        if (use_factor && outer > 0 && (res > 0.5 * prev || breakdown)) {
             use_factor = false;
             if (fell_back) *fell_back = 1;
         } else if (res > 0.5 * prev && ++stalls >= 3) {
@@ -173,14 +185,23 @@ clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const clden
         inner.maxIters = max_inner_total - inner_total;
         inner.relativeTolerance = inner_tol;
         inner.absoluteTolerance = 0.0;
+        // Continue the previous direction only while the recursion is
+        // trustworthy: same method, no breakdown, the inner solve reached its
+        // tolerance, and the FP64 true residual is within 2x of what the
+        // inner recursive residual predicted. Otherwise restart (p = M r):
+        // the residual-replacement criterion of van der Vorst and Ye.
+        ws.warm = have_prev && prev_factor == use_factor && !breakdown && res <= 2.0 * predicted;
         inner.nIters = 0;
         inner.deviceStatus = 0;
         if (use_factor)
             st = pcg_factor_typed<V, float, __nv_bfloat16>(&dvec, &Alow, &rvec, &inner, factor->G, factor->GT,
-                                                            c);
+                                                            c, &ws);
         else
-            st = cg_solve_typed<V, float>(&dvec, &Alow, &rvec, &inner, c);
+            st = cg_solve_typed<V, float>(&dvec, &Alow, &rvec, &inner, c, &ws);
         if (st != clsparseSuccess) return st;
+        have_prev = inner.currentResidual <= inner_tol;
+        prev_factor = use_factor;
+        predicted = res * inner.currentResidual;
         inner_total += inner.nIters + 1;
         update_kernel<<<g, kThreads, 0, s>>>(x, static_cast<const float*>(w.d.ptr), bnorm, n);
         ++outer;

@@ -15,6 +15,7 @@ struct SolverKey {
     int precond = 0;
     int ext = 0;
     int loop_mode = 0;
+    int warm = 0;       // continues the previous solve's search direction
     const void* ptrs[8] = {};  // vals, cols, rowptr, x, b, meta, preconditioner factors
     uint32_t n = 0, nnz = 0;
     size_t meta_words = 0;

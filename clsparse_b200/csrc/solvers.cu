@@ -119,10 +119,15 @@ struct CgArgs {
     uint32_t* ticket;
     size_t n;
     unsigned long long cond;
+    int warm;  // x == 0 and p holds the previous solve's direction
 };
 
 // r = b - A x (y holds A x), z = M r, p = z; ||b||_1, ||r||_1, <r,z>; initial
 // stop test (conjugate-gradients.hpp:73-148).
+// Warm start (x == 0, r = b): p is kept; beta = <r,z> / rz_old with rz_old
+// preset from the previous solve, and cg_p_kernel then forms p = z + beta p,
+// so the solve continues the previous search direction with the residual
+// replaced (reliable updates of the mixed-precision refinement).
 template <typename T>
 __global__ void __launch_bounds__(kThreads) cg_init_kernel(CgArgs<T> a) {
     double acc[3] = {0.0, 0.0, 0.0};
@@ -130,10 +135,10 @@ __global__ void __launch_bounds__(kThreads) cg_init_kernel(CgArgs<T> a) {
     const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
     for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
         const T bi = a.b[i];
-        const T ri = bi - a.y[i];
+        const T ri = a.warm ? bi : bi - a.y[i];
         const T zi = apply_m(a.invD, i, ri);
         a.r[i] = ri;
-        a.p[i] = zi;
+        if (!a.warm) a.p[i] = zi;
         acc[0] += norm_term(bi, l2);
         acc[1] += norm_term(ri, l2);
         acc[2] += static_cast<double>(ri) * static_cast<double>(zi);
@@ -154,6 +159,7 @@ __global__ void __launch_bounds__(kThreads) cg_init_kernel(CgArgs<T> a) {
         st->init_res = static_cast<double>(st->res);
         st->cur_res = st->init_res;
         st->rz = static_cast<T>(tot[2]);
+        if (a.warm) st->beta = st->rz / st->rz_old;
         st->iteration = 0;
         // The stop test sees the iteration count the solver control held
         // before this solve, as the reference's does.
@@ -411,9 +417,11 @@ struct PcgArgs {
     uint32_t* ticket;
     size_t n;
     unsigned long long cond;
+    int warm;  // x == 0 and p holds the previous solve's direction
 };
 
-// r = b - A x (q holds A x); ||b||, ||r||; initial stop test.
+// r = b - A x (q holds A x; warm start: x == 0, r = b); ||b||, ||r||; initial
+// stop test.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) pcg_init_kernel(PcgArgs<T> a) {
     double acc[2] = {0.0, 0.0};
@@ -421,7 +429,7 @@ __global__ void __launch_bounds__(kThreads) pcg_init_kernel(PcgArgs<T> a) {
     const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
     for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
         const T bi = a.b[i];
-        const T ri = bi - a.q[i];
+        const T ri = a.warm ? bi : bi - a.q[i];
         a.r[i] = ri;
         acc[0] += norm_term(bi, l2);
         acc[1] += norm_term(ri, l2);
@@ -746,9 +754,17 @@ clsparseStatus run_fused(clsparseControl c, SolverCache& cache, bool rebuild, Fu
     return clsparseSuccess;
 }
 
+// Whether a warm start may continue the cached solve: the cached work
+// vectors belong to the same operands.
+bool can_continue(const SolverCache& cache, SolverKey key) {
+    if (!cache.valid) return false;
+    key.warm = cache.key.warm;
+    return cache.key == key;
+}
+
 template <typename V, typename T>
 clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
-                        clSParseSolverControl sc, clsparseControl c) {
+                        clSParseSolverControl sc, clsparseControl c, WarmStart* ws = nullptr) {
     clsparseStatus stt = check_solver_args(xv, A, bv, sc, c);
     if (stt != clsparseSuccess) return stt;
     DeviceGuard guard(c->device);
@@ -757,7 +773,10 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
     SolverCache& cache = *c->solver_cache;
     const CsrView<V> Av = view_of<V>(A);
     const uint32_t spmv_ctas = spmv_num_ctas(Av.meta, Av.nrows, Av.nnz);
-    const SolverKey key = make_key(1, sizeof(V), sizeof(T), sc, c, A, xv, bv);
+    SolverKey key = make_key(1, sizeof(V), sizeof(T), sc, c, A, xv, bv);
+    const bool warm = ws && ws->warm;
+    key.warm = warm ? 1 : 0;
+    if (warm && !can_continue(cache, key)) return clsparseInvalidValue;
     bool rebuild = false;
     stt = prepare_cache<T>(c, cache, key, 4, n, spmv_ctas, rebuild);
     if (stt != clsparseSuccess) return stt;
@@ -777,9 +796,11 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
     a.ticket = static_cast<uint32_t*>(cache.parts.ptr);
     a.n = n;
     a.cond = 0;
+    a.warm = warm ? 1 : 0;
 
     auto* hs = reinterpret_cast<SolverState<T>*>(c->pinned);
     init_state(*hs, sc);
+    if (warm) hs->rz_old = static_cast<T>(ws->rz);
     cudaMemcpyAsync(a.st, hs, sizeof(SolverState<T>), cudaMemcpyHostToDevice, c->stream);
 
     const uint32_t vg = vec_grid(n, c->sm_count);
@@ -789,12 +810,15 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
     auto prologue = [&](cudaStream_t s, unsigned long long h) {
         CgArgs<T> aa = a;
         aa.cond = h;
-        if (aa.invD)
+        if (aa.invD && !aa.warm)
             extract_inv_diag_kernel<V, T><<<vg, kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
                                                                   invD, st);
-        SpmvEpilogue none;
-        launch_csrmv<V, T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
+        if (!aa.warm) {
+            SpmvEpilogue none;
+            launch_csrmv<V, T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
+        }
         cg_init_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+        if (aa.warm) cg_p_kernel<T><<<vg, kThreads, 0, s>>>(aa);
     };
     auto body = [&](cudaStream_t s, unsigned long long h) {
         CgArgs<T> aa = a;
@@ -818,7 +842,7 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
         sc->nIters = 0;
         return clsparseSuccess;
     }
-    if (fused_ok(c, Av.meta)) {
+    if (fused_ok(c, Av.meta) && !warm) {
         FusedCgArgs<V, T, T> fa{};
         fa.x = a.x;
         fa.b = a.b;
@@ -838,6 +862,8 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
         return stt;
     }
     stt = read_back<T>(c, cache, sc);
+    if (ws && stt == clsparseSuccess)
+        ws->rz = static_cast<double>(reinterpret_cast<SolverState<T>*>(static_cast<char*>(c->pinned) + 2048)->rz_old);
     sc->printSummary(stt);
     return stt;
 }
@@ -948,7 +974,7 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
 template <typename V, typename T, typename VG>
 clsparseStatus pcg_factor_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
                                 clSParseSolverControl sc, const CsrView<VG>& G, const CsrView<VG>& Gt,
-                                clsparseControl c) {
+                                clsparseControl c, WarmStart* ws = nullptr) {
     clsparseStatus stt = check_solver_args(xv, A, bv, sc, c);
     if (stt != clsparseSuccess) return stt;
     if (G.nrows != A->num_rows || Gt.nrows != A->num_rows) return clsparseInvalidSystemSize;
@@ -963,6 +989,9 @@ clsparseStatus pcg_factor_solve(cldenseVector* xv, const clsparseCsrMatrix* A, c
     SolverKey key = make_key(3, sizeof(V), sizeof(T), sc, c, A, xv, bv);
     key.ptrs[6] = G.vals;
     key.ptrs[7] = Gt.vals;
+    const bool warm = ws && ws->warm;
+    key.warm = warm ? 1 : 0;
+    if (warm && !can_continue(cache, key)) return clsparseInvalidValue;
     bool rebuild = false;
     stt = prepare_cache<T>(c, cache, key, 5, n, spmv_ctas, rebuild);
     if (stt != clsparseSuccess) return stt;
@@ -982,9 +1011,11 @@ clsparseStatus pcg_factor_solve(cldenseVector* xv, const clsparseCsrMatrix* A, c
     a.ticket = static_cast<uint32_t*>(cache.parts.ptr);
     a.n = n;
     a.cond = 0;
+    a.warm = warm ? 1 : 0;
 
     auto* hs = reinterpret_cast<SolverState<T>*>(c->pinned);
     init_state(*hs, sc);
+    if (warm) hs->rz = static_cast<T>(ws->rz);
     cudaMemcpyAsync(a.st, hs, sizeof(SolverState<T>), cudaMemcpyHostToDevice, c->stream);
 
     const uint32_t vg = vec_grid(n, c->sm_count);
@@ -1007,6 +1038,13 @@ clsparseStatus pcg_factor_solve(cldenseVector* xv, const clsparseCsrMatrix* A, c
     auto prologue = [&](cudaStream_t s, unsigned long long h) {
         PcgArgs<T> aa = a;
         aa.cond = h;
+        if (aa.warm) {
+            // r = b; z = G^T G r; beta = <z,r> / rz (preset); p = z + beta p
+            pcg_init_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+            apply_m(s, aa, EpiOp::PcgRz);
+            pcg_p_kernel<T><<<vg, kThreads, 0, s>>>(aa);
+            return;
+        }
         SpmvEpilogue none;
         launch_csrmv<V, T>(Av, &st->one, &st->zero, aa.x, aa.q, ext, none, s);
         pcg_init_kernel<T><<<vg, kThreads, 0, s>>>(aa);
@@ -1036,7 +1074,7 @@ clsparseStatus pcg_factor_solve(cldenseVector* xv, const clsparseCsrMatrix* A, c
         sc->nIters = 0;
         return clsparseSuccess;
     }
-    if (fused_ok(c, Av.meta) && fused_ok(c, G.meta) && fused_ok(c, Gt.meta)) {
+    if (fused_ok(c, Av.meta) && fused_ok(c, G.meta) && fused_ok(c, Gt.meta) && !warm) {
         FusedCgArgs<V, T, VG> fa{};
         fa.x = a.x;
         fa.b = a.b;
@@ -1056,7 +1094,10 @@ clsparseStatus pcg_factor_solve(cldenseVector* xv, const clsparseCsrMatrix* A, c
         cache.drop_graph();
         return stt;
     }
-    return read_back<T>(c, cache, sc);
+    stt = read_back<T>(c, cache, sc);
+    if (ws && stt == clsparseSuccess)
+        ws->rz = static_cast<double>(reinterpret_cast<SolverState<T>*>(static_cast<char*>(c->pinned) + 2048)->rz);
+    return stt;
 }
 
 }  // namespace
@@ -1064,37 +1105,37 @@ clsparseStatus pcg_factor_solve(cldenseVector* xv, const clsparseCsrMatrix* A, c
 template <typename V, typename T, typename VG>
 clsparseStatus pcg_factor_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
                                 clSParseSolverControl sc, const CsrView<VG>& G, const CsrView<VG>& Gt,
-                                clsparseControl c) {
-    return pcg_factor_solve<V, T, VG>(x, A, b, sc, G, Gt, c);
+                                clsparseControl c, WarmStart* ws) {
+    return pcg_factor_solve<V, T, VG>(x, A, b, sc, G, Gt, c, ws);
 }
 template clsparseStatus pcg_factor_typed<float, float, __nv_bfloat16>(
     cldenseVector*, const clsparseCsrMatrix*, const cldenseVector*, clSParseSolverControl,
-    const CsrView<__nv_bfloat16>&, const CsrView<__nv_bfloat16>&, clsparseControl);
+    const CsrView<__nv_bfloat16>&, const CsrView<__nv_bfloat16>&, clsparseControl, WarmStart*);
 template clsparseStatus pcg_factor_typed<__nv_bfloat16, float, __nv_bfloat16>(
     cldenseVector*, const clsparseCsrMatrix*, const cldenseVector*, clSParseSolverControl,
-    const CsrView<__nv_bfloat16>&, const CsrView<__nv_bfloat16>&, clsparseControl);
+    const CsrView<__nv_bfloat16>&, const CsrView<__nv_bfloat16>&, clsparseControl, WarmStart*);
 template clsparseStatus pcg_factor_typed<float, float, float>(cldenseVector*, const clsparseCsrMatrix*,
                                                               const cldenseVector*, clSParseSolverControl,
                                                               const CsrView<float>&, const CsrView<float>&,
-                                                              clsparseControl);
+                                                              clsparseControl, WarmStart*);
 template clsparseStatus pcg_factor_typed<double, double, double>(
     cldenseVector*, const clsparseCsrMatrix*, const cldenseVector*, clSParseSolverControl,
-    const CsrView<double>&, const CsrView<double>&, clsparseControl);
+    const CsrView<double>&, const CsrView<double>&, clsparseControl, WarmStart*);
 
 template <typename V, typename T>
 clsparseStatus cg_solve_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
-                              clSParseSolverControl sc, clsparseControl c) {
-    return cg_solve<V, T>(x, A, b, sc, c);
+                              clSParseSolverControl sc, clsparseControl c, WarmStart* ws) {
+    return cg_solve<V, T>(x, A, b, sc, c, ws);
 }
 template clsparseStatus cg_solve_typed<double, double>(cldenseVector*, const clsparseCsrMatrix*,
                                                        const cldenseVector*, clSParseSolverControl,
-                                                       clsparseControl);
+                                                       clsparseControl, WarmStart*);
 template clsparseStatus cg_solve_typed<float, float>(cldenseVector*, const clsparseCsrMatrix*,
                                                      const cldenseVector*, clSParseSolverControl,
-                                                     clsparseControl);
+                                                     clsparseControl, WarmStart*);
 template clsparseStatus cg_solve_typed<__nv_bfloat16, float>(cldenseVector*, const clsparseCsrMatrix*,
-                                                             const cldenseVector*,
-                                                             clSParseSolverControl, clsparseControl);
+                                                             const cldenseVector*, clSParseSolverControl,
+                                                             clsparseControl, WarmStart*);
 
 }  // namespace clsp
 
