@@ -12,6 +12,10 @@ L2 (126 MB), so every step streams it from HBM.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+After the SpMV line's timing, rank 0 (N=1) also measures CG time-to-solution
+(key "cg": C1 against the CPU oracle, C3 mixed FP32 vs FP64, C5 learned+mixed
+and mixed vs FP64 Jacobi-CG); --no-cg skips it.
+
 N>1 (torchrun): each rank runs its own replica of the workload on its own GPU
 (no data-path collective; weak scaling); the timing is the max over ranks.
 --impl reference times the reference algorithm's CPU restatement (the oracle
@@ -125,6 +129,157 @@ def cpu_baseline(rp, col, val, seconds=12.0):
     return {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
             "sample": f"{reps} full FP64 SpMVs of the same 2M-row matrix ({el:.1f} s, "
                       f"row ranges balanced by nnz over {threads} threads)"}
+
+
+def _timed(fn, reps=2):
+    """Device-synchronised wall time of the last of `reps` calls (the first
+    builds the cached solver graph)."""
+    import torch
+    r = None
+    t = 0.0
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+    return t, r
+
+
+def cg_section(ctrl, with_cpu: bool):
+    """Time-to-solution of the solver configurations the headline metric names.
+
+    C1  2D Poisson 512^2, FP64 Jacobi-CG with the reference's L1 stop test at
+        1e-10 (clsparseDcsrcg) -- beside it the oracle restatement of the
+        reference CG on one host core.
+    C3  3D 7-point log-normal diffusion 128^3 (sigma 1.5): FP64 Jacobi-CG vs
+        the FP64 refinement around FP32 CG (clsparseDcsrcgMixed), both to a
+        relative L2 true residual of 1e-10.
+    C5  2D GRF diffusion 1024^2 (corr 0.05, sigma 2): FP64 Jacobi-CG vs
+        mixed FP32 and vs learned (G^T G, BF16 factor) + mixed FP32
+        (clsparseDcsrcgLearned); the network is trained on the GPU by the
+        library's kernels on 128^2 matrices of the family (different seeds)
+        before the timed solves; training time is reported separately.
+    Each solve is timed on its second call (the first captures the graph)."""
+    import torch
+    from clsparse_b200 import _lib as L
+    from clsparse_b200 import api, learn, matgen
+
+    out = {}
+
+    def fp64_cg(A, b, x, l2=True, max_iters=200000):
+        def run():
+            x.zero_()
+            sc = api.SolverControl(L.DIAGONAL, max_iters, 1e-10, 0.0)
+            if l2:
+                sc.set_norm(2)
+            info = api.solve("cg", x, A, b, sc, ctrl)
+            sc.release()
+            return info
+        return _timed(run)
+
+    def true_res(np_mat, x, b):
+        import scipy.sparse as sp
+        rp, col, val = np_mat
+        n = len(rp) - 1
+        M = sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64)), shape=(n, n))
+        bb = b.cpu().numpy()
+        return float(np.linalg.norm(bb - M @ x.cpu().numpy()) / np.linalg.norm(bb))
+
+    # C1
+    c1 = matgen.poisson2d(512)
+    A = api.CsrMatrix.from_numpy(*c1)
+    A.create_meta(ctrl)
+    n = A.num_rows
+    b = torch.tensor(np.random.default_rng(1).uniform(-1, 1, n), device="cuda")
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    t, info = fp64_cg(A, b, x, l2=False)
+    c1_out = {"workload": "2D Poisson 512x512 (n=262,144), FP64 Jacobi-CG, L1 stop test 1e-10",
+              "gpu_s": round(t, 5), "iterations": info["nIters"]}
+    if with_cpu:
+        import oracle
+        rp, col, val = c1
+        t0 = time.perf_counter()
+        _, oi = oracle.solve("cg", np.float64, rp, col, val, np.zeros(n), b.cpu().numpy(), 1, 200000, 1e-10, 0.0)
+        tc = time.perf_counter() - t0
+        c1_out["cpu_baseline"] = {"s": round(tc, 3), "iterations": oi.nIters, "cores": 1, "kind": "port",
+                                  "sample": "the whole solve, oracle restatement of the reference CG"}
+        c1_out["speedup_vs_cpu"] = round(tc / t, 1)
+    out["C1"] = c1_out
+    del A
+
+    # C3
+    c3 = matgen.diffusion3d_lognormal(128, sigma=1.5, seed=3)
+    A = api.CsrMatrix.from_numpy(*c3)
+    A.create_meta(ctrl)
+    n = A.num_rows
+    b = torch.tensor(np.random.default_rng(1).uniform(-1, 1, n), device="cuda")
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    t64, i64 = fp64_cg(A, b, x)
+    r64 = true_res(c3, x, b)
+
+    def mixed():
+        x.zero_()
+        sc = api.SolverControl(L.DIAGONAL, 200000, 1e-10, 0.0)
+        r = api.cg_mixed(x, A, b, sc, ctrl, inner="fp32", inner_tol=0.1)
+        sc.release()
+        return r
+    tm, im = _timed(mixed)
+    out["C3"] = {"workload": "3D 7-point log-normal diffusion 128^3 (n=2,097,152, sigma 1.5), rel. L2 residual 1e-10",
+                 "fp64_jacobi": {"s": round(t64, 5), "iterations": i64["nIters"] + 1, "true_residual": r64},
+                 "mixed_fp32": {"s": round(tm, 5), "inner_iterations": im["innerIterations"],
+                                "refinements": im["outerIterations"], "true_residual": true_res(c3, x, b)},
+                 "speedup": round(t64 / tm, 3)}
+    del A
+
+    # C5
+    t0 = time.perf_counter()
+    spai, hist = learn.train(ctrl, sizes=(128,), seeds=range(6), steps=300, lr=3e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    c5 = matgen.diffusion2d_grf(1024, corr_len=0.05, sigma=2.0, seed=1005)
+    A = api.CsrMatrix.from_numpy(*c5)
+    A.create_meta(ctrl)
+    n = A.num_rows
+    b = torch.tensor(np.random.default_rng(1).uniform(-1, 1, n), device="cuda")
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    t64, i64 = fp64_cg(A, b, x)
+    r64 = true_res(c5, x, b)
+
+    def mixed5():
+        x.zero_()
+        sc = api.SolverControl(L.DIAGONAL, 200000, 1e-10, 0.0)
+        r = api.cg_mixed(x, A, b, sc, ctrl, inner="fp32", inner_tol=0.1)
+        sc.release()
+        return r
+    tm, im = _timed(mixed5)
+    rm = true_res(c5, x, b)
+    tb0 = time.perf_counter()
+    spai.set_matrix(A, ctrl)
+    spai.build(ctrl)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - tb0
+
+    def learned():
+        x.zero_()
+        sc = api.SolverControl(L.DIAGONAL, 200000, 1e-10, 0.0)
+        r = api.cg_learned(x, A, b, sc, spai, ctrl, inner="fp32", inner_tol=0.1)
+        sc.release()
+        return r
+    tl, il = _timed(learned)
+    rl = true_res(c5, x, b)
+    spai.release()
+    out["C5"] = {"workload": "2D GRF diffusion 1024^2 (n=1,048,576, corr 0.05, sigma 2), rel. L2 residual 1e-10",
+                 "fp64_jacobi": {"s": round(t64, 5), "iterations": i64["nIters"] + 1, "true_residual": r64},
+                 "mixed_fp32": {"s": round(tm, 5), "inner_iterations": im["innerIterations"],
+                                "refinements": im["outerIterations"], "true_residual": rm,
+                                "speedup": round(t64 / tm, 3)},
+                 "learned_mixed_fp32": {"s": round(tl, 5), "inner_iterations": il["innerIterations"],
+                                        "refinements": il["outerIterations"], "true_residual": rl,
+                                        "fell_back_to_jacobi": il["fell_back"], "factor_build_s": round(build_s, 3),
+                                        "speedup": round(t64 / tl, 3)},
+                 "train_s": round(train_s, 2), "train_loss_first_last": [hist[0], hist[-1]]}
+    return out
 
 
 def make_matrix():
@@ -269,6 +424,11 @@ def run_ours(args, rank, world, local_rank):
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(rp, col, val)
+    if world == 1 and not args.no_cg:
+        del A
+        with torch.cuda.stream(stream):
+            ctrl.enable_async(False)
+            line["cg"] = cg_section(ctrl, with_cpu=not args.no_cpu_baseline)
     print(json.dumps(line), flush=True)
     ctrl.release()
 
@@ -280,6 +440,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cg", action="store_true", help="skip the CG time-to-solution section")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
