@@ -178,6 +178,7 @@ SIGNATURES = {
     "clsparseB200ComputeRowBlocksHost": (clsparseStatus, [P(clsparseIdx_t), clsparseIdx_t, P(cl_ulong),
                                                           C.c_size_t, P(clsparseIdx_t)]),
     "clsparseB200CsrMetaGetRowBlocks": (clsparseStatus, [_M, P(cl_ulong), C.c_size_t, P(C.c_size_t)]),
+    "clsparseB200CsrMetaCreateTuned": (clsparseStatus, [_M, cl_uint, cl_uint, cl_uint, cl_uint, _V]),
     "clsparseB200SolverGetInfo": (clsparseStatus, [_V, P(cl_int), P(C.c_double), P(C.c_double)]),
     "clsparseB200SolverGetDeviceStatus": (clsparseStatus, [_V, P(cl_uint)]),
     "clsparseB200SetSolverLoopMode": (clsparseStatus, [_V, cl_int]),

@@ -130,8 +130,18 @@ class CsrMatrix:
         check(r.status, "clsparseCsrMetaSize")
         return int(r.metaSize)
 
-    def create_meta(self, ctrl: Control):
-        check(lib().clsparseCsrMetaCreate(C.byref(self.s), ctrl.handle), "clsparseCsrMetaCreate")
+    def create_meta(self, ctrl: Control, shape=None):
+        """CSR-Adaptive meta; shape = (blk_size, blk_multiplier, rows_for_vector,
+        cta_threads) for clsparseB200CsrMetaCreateTuned, None for the
+        reference's shape (clsparseCsrMetaCreate)."""
+        if shape is None:
+            check(lib().clsparseCsrMetaCreate(C.byref(self.s), ctrl.handle), "clsparseCsrMetaCreate")
+        else:
+            if self.s.meta:
+                self.delete_meta()
+            blk, mult, rfv, nt = (int(v) for v in shape)
+            check(lib().clsparseB200CsrMetaCreateTuned(C.byref(self.s), blk, mult, rfv, nt, ctrl.handle),
+                  "clsparseB200CsrMetaCreateTuned")
 
     def delete_meta(self):
         check(lib().clsparseCsrMetaDelete(C.byref(self.s)), "clsparseCsrMetaDelete")

@@ -176,12 +176,15 @@ struct DotSink {
 };
 
 // Runs this CTA's words of M through adaptive_word.
+// (Metas of the reference's row-block shape only.)
 template <typename V, typename T, bool EXT, int NT, typename XS, typename Sink>
 __device__ __forceinline__ void spmv_phase(const WordMat<V>& M, const XS& xs, Sink& sink, WordSmem<T>& sm) {
     const uint32_t wb = M.cta_words[blockIdx.x], we = M.cta_words[blockIdx.x + 1];
+    const WordShape shape{kRowsForVector, kLongChunk};
     for (uint32_t w = wb; w < we; ++w) {
-        adaptive_word<V, T, EXT, NT>(w, M.vals, M.cols, M.rp, xs, T(1), M.words, M.word_nnz, M.lo, M.hi, M.vec,
-                                     M.lr_partial, M.lr_ticket, sm, sink);
+        adaptive_word<V, T, EXT, NT, static_cast<int>(kBlkSize)>(w, M.vals, M.cols, M.rp, xs, T(1), M.words,
+                                                                 M.word_nnz, M.lo, M.hi, M.vec, M.lr_partial,
+                                                                 M.lr_ticket, shape, sm, sink);
         __syncthreads();
     }
 }

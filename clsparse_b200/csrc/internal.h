@@ -103,8 +103,22 @@ struct matrix_meta {
     uint32_t nnz_lo = 0;                // row_pointer[0]
     uint32_t nnz_hi = 0;                // row_pointer[num_rows]
     int device = 0;
+    // Row-block shape the words were made with (the reference's constants by
+    // default; clsparseB200CsrMetaCreateTuned sets others) and the CTA width
+    // of the adaptive kernel.
+    uint32_t blk_size = clsp::kBlkSize;
+    uint32_t blk_mult = clsp::kBlockMultiplier;
+    uint32_t rows_for_vector = clsp::kRowsForVector;
+    int cta_threads = 128;
     ~matrix_meta();
 };
+
+// True when a meta has the reference's row-block shape (the only one the
+// persistent solver and the TMA variant are built for).
+inline bool meta_is_default_shape(const matrix_meta* m) {
+    return m->blk_size == clsp::kBlkSize && m->blk_mult == clsp::kBlockMultiplier &&
+           m->rows_for_vector == clsp::kRowsForVector;
+}
 
 // Solver control (reference solvers/solver-control.hpp:37-128).
 struct _solverControl {
@@ -215,6 +229,13 @@ clsparseStatus pcg_factor_typed(cldenseVector* x, const clsparseCsrMatrix* A, co
 bool spai_factor_views(clsparseB200Spai net, CsrView<__nv_bfloat16>& G16, CsrView<__nv_bfloat16>& GT16,
                        CsrView<float>& G32, CsrView<float>& GT32, CsrView<double>& G64,
                        CsrView<double>& GT64);
+
+// Builds the meta of a matrix with the given row-block shape and adaptive
+// kernel CTA width (meta.cpp); clsparseCsrMetaCreate uses the reference's
+// shape and default_cta_threads().
+clsparseStatus create_meta(clsparseCsrMatrix* csrMatx, clsparseControl control, uint32_t blk, uint32_t mult,
+                           uint32_t rfv, int nt);
+int default_cta_threads();
 
 // Host binning (meta.cpp).
 void compute_row_blocks(cl_ulong* rowBlocks, clsparseIdx_t& rowBlockSize, const clsparseIdx_t* rp,

@@ -12,6 +12,7 @@
 //   bits 23..0   chunk index inside a long row, or for a block of several short
 //                rows the number of threads the reference reduced each row with
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "internal.h"
@@ -202,6 +203,31 @@ clsparseMetaSizeResult clsparseCsrMetaSize(clsparseCsrMatrix* csrMatx, clsparseC
 }
 
 clsparseStatus clsparseCsrMetaCreate(clsparseCsrMatrix* csrMatx, clsparseControl control) {
+    return clsp::create_meta(csrMatx, control, kBlkSize, kBlockMultiplier, kRowsForVector, clsp::default_cta_threads());
+}
+
+clsparseStatus clsparseB200CsrMetaCreateTuned(clsparseCsrMatrix* csrMatx, cl_uint blkSize, cl_uint blkMultiplier,
+                                              cl_uint rowsForVector, cl_uint ctaThreads, clsparseControl control) {
+    if (!((blkSize == 512 && ctaThreads == 128) || ((blkSize == 1024 || blkSize == 2048) && (ctaThreads == 128 || ctaThreads == 256))))
+        return clsparseInvalidValue;
+    if (blkMultiplier < 1 || blkMultiplier > 64 || rowsForVector < 1 || rowsForVector > 256) return clsparseInvalidValue;
+    return clsp::create_meta(csrMatx, control, blkSize, blkMultiplier, rowsForVector, static_cast<int>(ctaThreads));
+}
+
+}  // extern "C"
+
+namespace clsp {
+
+int default_cta_threads() {
+    static int nt = [] {
+        const char* e = std::getenv("CLSPARSE_B200_SPMV_NT");
+        return (e && std::atoi(e) == 256) ? 256 : 128;
+    }();
+    return nt;
+}
+
+clsparseStatus create_meta(clsparseCsrMatrix* csrMatx, clsparseControl control, uint32_t blk, uint32_t mult,
+                           uint32_t rfv, int nt) {
     clsparseStatus st = check_entry(control);
     if (st != clsparseSuccess) return st;
     if (csrMatx == nullptr) return clsparseInvalidValue;
@@ -220,13 +246,15 @@ clsparseStatus clsparseCsrMetaCreate(clsparseCsrMatrix* csrMatx, clsparseControl
     meta->device = control->device;
     meta->num_rows = csrMatx->num_rows;
     meta->num_nonzeros = csrMatx->num_nonzeros;
+    meta->blk_size = blk;
+    meta->blk_mult = mult;
+    meta->rows_for_vector = rfv;
+    meta->cta_threads = nt;
     clsparseIdx_t dry = 0;
-    compute_row_blocks(nullptr, dry, rp.data(), csrMatx->num_rows, kBlkSize, kBlockMultiplier,
-                       kRowsForVector, false);
+    compute_row_blocks(nullptr, dry, rp.data(), csrMatx->num_rows, blk, mult, rfv, false);
     meta->h_rowBlocks.assign(dry / 2 + 1, 0);
     clsparseIdx_t used = dry;
-    compute_row_blocks(meta->h_rowBlocks.data(), used, rp.data(), csrMatx->num_rows, kBlkSize,
-                       kBlockMultiplier, kRowsForVector, true);
+    compute_row_blocks(meta->h_rowBlocks.data(), used, rp.data(), csrMatx->num_rows, blk, mult, rfv, true);
     meta->rowBlockSize = used;
     meta->num_words = used / 2;
     meta->h_rowBlocks.resize(meta->num_words);
@@ -260,6 +288,10 @@ clsparseStatus clsparseCsrMetaCreate(clsparseCsrMatrix* csrMatx, clsparseControl
     csrMatx->meta = meta.release();
     return clsparseSuccess;
 }
+
+}  // namespace clsp
+
+extern "C" {
 
 clsparseStatus clsparseCsrMetaCompute(clsparseCsrMatrix* csrMatx, clsparseControl control) {
     return clsparseCsrMetaCreate(csrMatx, control);

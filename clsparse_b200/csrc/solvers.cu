@@ -700,7 +700,7 @@ clsparseStatus prepare_cache(clsparseControl c, SolverCache& cache, const Solver
 // CSR-Adaptive meta (with its host word offsets) on every matrix it reads.
 bool fused_ok(clsparseControl c, const matrix_meta* m) {
     return c->solver_loop_mode == 2 && m != nullptr && m->num_words >= 2 &&
-           m->h_word_nnz.size() == m->num_words;
+           m->h_word_nnz.size() == m->num_words && meta_is_default_shape(m);
 }
 
 size_t align256(size_t b) { return (b + 255) / 256 * 256; }

@@ -35,23 +35,23 @@ namespace {
 
 constexpr int kThreads = 256;
 
-template <typename V, typename T, bool EXT, int K, int NT>
+template <typename V, typename T, bool EXT, int K, int NT, int BLK>
 __global__ void __launch_bounds__(NT)
     csr_adaptive_kernel(const V* __restrict__ vals, const uint32_t* __restrict__ cols,
                         const uint32_t* __restrict__ rp, const T* __restrict__ x, T* __restrict__ y,
                         const T* __restrict__ alpha_p, const T* __restrict__ beta_p,
                         const uint64_t* __restrict__ words, const uint32_t* __restrict__ word_nnz,
                         uint32_t nblocks, uint32_t lo, uint32_t hi, int vec,
-                        double* __restrict__ lr_partial, uint32_t* __restrict__ lr_ticket,
+                        double* __restrict__ lr_partial, uint32_t* __restrict__ lr_ticket, WordShape shape,
                         EpiDev<T> epi) {
-    __shared__ WordSmem<T> sm;
+    __shared__ WordSmem<T, BLK> sm;
     if (epi.done != nullptr && *epi.done) return;
     const T alpha = *alpha_p;
     RowSink<T, K> sink;
     sink.init(y, epi, *beta_p);
     if (blockIdx.x < nblocks)
-        adaptive_word<V, T, EXT, NT>(blockIdx.x, vals, cols, rp, DenseX<T>{x}, alpha, words, word_nnz, lo, hi,
-                                     vec, lr_partial, lr_ticket, sm, sink);
+        adaptive_word<V, T, EXT, NT, BLK>(blockIdx.x, vals, cols, rp, DenseX<T>{x}, alpha, words, word_nnz, lo,
+                                          hi, vec, lr_partial, lr_ticket, shape, sm, sink);
     run_epilogue<T, K>(sink, epi);
 }
 
@@ -141,9 +141,9 @@ cudaError_t launch_vector(const CsrView<V>& A, const T* alpha, const T* beta, co
 #include "spmv_tma.cuh"
 
 // Adaptive kernel choice: one CTA per row block (default) or the TMA-staged
-// persistent pipeline (CLSPARSE_B200_SPMV_KERNEL=tma), which measured slower
-// on the irregular workload (its per-block barriers leave too little work in
-// flight per SM).
+// persistent pipeline (CLSPARSE_B200_SPMV_KERNEL=tma, default row-block shape
+// only), which measured slower on the irregular workload (its per-block
+// barriers leave too little work in flight per SM).
 bool use_tma_kernel() {
     static bool on = [] {
         const char* e = std::getenv("CLSPARSE_B200_SPMV_KERNEL");
@@ -181,38 +181,47 @@ cudaError_t launch_tma(const CsrView<V>& A, const T* alpha, const T* beta, const
     return cudaGetLastError();
 }
 
-// Threads per CTA of the adaptive kernel (128 or 256); CLSPARSE_B200_SPMV_NT
-// overrides the default for tuning.
-int adaptive_threads() {
-    static int nt = [] {
-        const char* e = std::getenv("CLSPARSE_B200_SPMV_NT");
-        const int v = e ? std::atoi(e) : 128;
-        return v == 256 ? 256 : 128;
-    }();
-    return nt;
+template <typename V, typename T, bool EXT, int K, int NT, int BLK>
+void launch_adaptive(const CsrView<V>& A, const T* alpha, const T* beta, const T* x, T* y, const EpiDev<T>& e,
+                     uint32_t grid, uint32_t nblocks, int vec, cudaStream_t s) {
+    const matrix_meta* m = A.meta;
+    const WordShape shape{m->rows_for_vector, m->blk_size * m->blk_mult};
+    csr_adaptive_kernel<V, T, EXT, K, NT, BLK><<<grid, NT, 0, s>>>(
+        A.vals, A.cols, A.rp, x, y, alpha, beta, m->d_rowBlocks, m->d_word_nnz, nblocks, m->nnz_lo, m->nnz_hi,
+        vec, m->d_lr_partial, m->d_lr_ticket, shape, e);
 }
 
 template <typename V, typename T, bool EXT, int K>
 cudaError_t launch_kind(const CsrView<V>& A, const T* alpha, const T* beta, const T* x, T* y,
                         const EpiDev<T>& e, cudaStream_t s) {
     if (A.meta == nullptr) return launch_vector<V, T, EXT, K>(A, alpha, beta, x, y, e, s);
-    const uint32_t nblocks = static_cast<uint32_t>(A.meta->num_words - 1);
+    const matrix_meta* m = A.meta;
+    const uint32_t nblocks = static_cast<uint32_t>(m->num_words - 1);
     uint32_t grid = nblocks;
     if (grid == 0) {
         if (K == 0) return cudaSuccess;
         grid = 1;  // one idle CTA still finishes the fused reduction
     }
-    if (use_tma_kernel()) return launch_tma<V, T, EXT, K>(A, alpha, beta, x, y, e, s, A.meta->d_error);
+    if (use_tma_kernel() && meta_is_default_shape(m))
+        return launch_tma<V, T, EXT, K>(A, alpha, beta, x, y, e, s, m->d_error);
     const int vec = ((reinterpret_cast<uintptr_t>(A.vals) | reinterpret_cast<uintptr_t>(A.cols)) & 15u) == 0;
-    const matrix_meta* m = A.meta;
-    if (adaptive_threads() == 256)
-        csr_adaptive_kernel<V, T, EXT, K, 256><<<grid, 256, 0, s>>>(
-            A.vals, A.cols, A.rp, x, y, alpha, beta, m->d_rowBlocks, m->d_word_nnz, nblocks, m->nnz_lo,
-            m->nnz_hi, vec, m->d_lr_partial, m->d_lr_ticket, e);
-    else
-        csr_adaptive_kernel<V, T, EXT, K, 128><<<grid, 128, 0, s>>>(
-            A.vals, A.cols, A.rp, x, y, alpha, beta, m->d_rowBlocks, m->d_word_nnz, nblocks, m->nnz_lo,
-            m->nnz_hi, vec, m->d_lr_partial, m->d_lr_ticket, e);
+    // Row-block shapes with kernels: BLKSIZE 512 (128 threads), 1024 and 2048
+    // (128 or 256 threads); meta creation accepts no other.
+    const int nt = m->cta_threads;
+    switch (m->blk_size) {
+        case 512: launch_adaptive<V, T, EXT, K, 128, 512>(A, alpha, beta, x, y, e, grid, nblocks, vec, s); break;
+        case 2048:
+            if (nt == 256)
+                launch_adaptive<V, T, EXT, K, 256, 2048>(A, alpha, beta, x, y, e, grid, nblocks, vec, s);
+            else
+                launch_adaptive<V, T, EXT, K, 128, 2048>(A, alpha, beta, x, y, e, grid, nblocks, vec, s);
+            break;
+        default:
+            if (nt == 256)
+                launch_adaptive<V, T, EXT, K, 256, 1024>(A, alpha, beta, x, y, e, grid, nblocks, vec, s);
+            else
+                launch_adaptive<V, T, EXT, K, 128, 1024>(A, alpha, beta, x, y, e, grid, nblocks, vec, s);
+    }
     return cudaGetLastError();
 }
 

@@ -23,7 +23,7 @@
 namespace clsp {
 namespace {
 
-constexpr uint32_t kLongChunk = kBlkSize * kBlockMultiplier;  // 3072 nonzeros per CTA
+constexpr uint32_t kLongChunk = kBlkSize * kBlockMultiplier;  // 3072 nonzeros per CTA (default shape)
 
 template <typename T>
 struct EpiDev {
@@ -195,12 +195,20 @@ __device__ __forceinline__ dev::Acc<T, EXT> range_sum(const V* __restrict__ vals
     return a;
 }
 
-constexpr uint32_t kRpStage = kBlkSize + 1;  // row pointers of a STREAM block kept in shared memory
-constexpr uint32_t kStageRow = kBlkSize / 4 + 2;  // quads per block (+1 ragged) + 1 bank skew
+// Row-block shape of a meta: BLK (the reference's BLKSIZE) is a template
+// parameter of the kernels (shared-memory staging and per-thread quads are
+// sized by it); ROWS_FOR_VECTOR and the long-row chunk
+// (BLOCK_MULTIPLIER * BLKSIZE) are runtime values.
+struct WordShape {
+    uint32_t rows_for_vector;
+    uint32_t chunk;
+};
 
 // Shared memory of one word's processing.
-template <typename T>
+template <typename T, int BLK = static_cast<int>(kBlkSize)>
 struct WordSmem {
+    static constexpr uint32_t kRpStage = BLK + 1;     // row pointers of a STREAM block
+    static constexpr uint32_t kStageRow = BLK / 4 + 2;  // quads per block (+1 ragged) + 1 bank skew
     // Products of a STREAM block, quad-transposed: element e (counted from the
     // block's 16-byte-aligned start) lives at stage[(e & 3) * kStageRow + e / 4],
     // so a warp's stores of one quad slot are contiguous and the row
@@ -216,15 +224,18 @@ struct WordSmem {
 // whole CTA (NT threads). x(c) yields the vector entry of column c; every row
 // the word finishes goes through sink.put. The caller separates two calls on
 // the same shared memory with a barrier.
-template <typename V, typename T, bool EXT, int NT, typename XS, typename Sink>
+template <typename V, typename T, bool EXT, int NT, int BLK, typename XS, typename Sink>
 __device__ __forceinline__ void adaptive_word(uint32_t gid, const V* __restrict__ vals,
                                               const uint32_t* __restrict__ cols,
                                               const uint32_t* __restrict__ rp, const XS& x,
                                               T alpha, const uint64_t* __restrict__ words,
                                               const uint32_t* __restrict__ word_nnz, uint32_t lo,
                                               uint32_t hi, int vec, double* __restrict__ lr_partial,
-                                              uint32_t* __restrict__ lr_ticket, WordSmem<T>& sm,
-                                              Sink& sink) {
+                                              uint32_t* __restrict__ lr_ticket, WordShape shape,
+                                              WordSmem<T, BLK>& sm, Sink& sink) {
+    constexpr uint32_t kRpStage = WordSmem<T, BLK>::kRpStage;
+    constexpr uint32_t kStageRow = WordSmem<T, BLK>::kStageRow;
+    static_assert(BLK / 4 / NT >= 1, "a block needs at least one quad per thread");
     T* stage = sm.stage;
     uint32_t* srp = sm.srp;
     // Independent loads: the block's words and the nonzero offsets of
@@ -238,18 +249,18 @@ __device__ __forceinline__ void adaptive_word(uint32_t gid, const V* __restrict_
     const uint32_t low = static_cast<uint32_t>(w0 & ((1u << kWgBits) - 1u));
     const uint32_t nrows = stop - row;
     const uint32_t tid = threadIdx.x;
-    if (nrows > kRowsForVector) {
-        // ---- STREAM: several short rows, <= kBlkSize nonzeros in total ----
+    if (nrows > shape.rows_for_vector) {
+        // ---- STREAM: several short rows, <= BLK nonzeros in total ----
         const uint32_t cnt = ne - nb;
         // A block from clsparseCsrMetaCreate never exceeds the staging
         // buffer; if the row pointers changed after the meta was made, the
         // rows are summed straight from global memory instead.
-        const bool staged = cnt <= kBlkSize;
+        const bool staged = cnt <= static_cast<uint32_t>(BLK);
         const bool rp_staged = nrows < kRpStage;
         if (staged) {
-            constexpr int QPT = static_cast<int>(kBlkSize) / 4 / NT;
+            constexpr int QPT = BLK / 4 / NT;
             const uint32_t base = nb & ~3u;
-            const uint32_t nq = (ne - base + 3) >> 2;  // <= kBlkSize/4 + 1
+            const uint32_t nq = (ne - base + 3) >> 2;  // <= BLK/4 + 1
             Quad<T> q[QPT];
 #pragma unroll
             for (int j = 0; j < QPT; ++j) {
@@ -322,20 +333,26 @@ __device__ __forceinline__ void adaptive_word(uint32_t gid, const V* __restrict_
             case 16: reduce_rows(std::integral_constant<int, 16>{}); break;
             default: reduce_rows(std::integral_constant<int, 32>{}); break;
         }
-    } else if (nrows == 1 && low == 0) {
-        // ---- VECTOR: one row, the whole CTA ----
-        dev::Acc<T, EXT> a = range_sum<V, T, EXT, NT>(vals, cols, x, alpha, nb, ne, lo, hi, vec != 0);
-        a = dev::block_reduce_acc(a, sm.red_s, sm.red_c);
-        if (tid == 0) sink.template put<EXT>(row, a);
+    } else if (nrows >= 1 && low == 0) {
+        // ---- VECTOR: up to ROWS_FOR_VECTOR rows, one at a time, the whole CTA
+        // (the reference's CSR-Vector branch, csrmv_adaptive.cl:517-610) ----
+        for (uint32_t rr = 0; rr < nrows; ++rr) {
+            const uint32_t rb = rr == 0 ? nb : dev::ld_ro(rp + row + rr);
+            const uint32_t re = rr + 1 == nrows ? ne : dev::ld_ro(rp + row + rr + 1);
+            dev::Acc<T, EXT> a = range_sum<V, T, EXT, NT>(vals, cols, x, alpha, rb, re, lo, hi, vec != 0);
+            a = dev::block_reduce_acc(a, sm.red_s, sm.red_c);
+            if (tid == 0) sink.template put<EXT>(row + rr, a);
+        }
     } else {
         // ---- LONG: chunk `low` of a row split over several CTAs ----
         const uint32_t re = dev::ld_ro(rp + row + 1);
         const uint32_t len = re - nb;
-        const uint32_t nchunks = (len + kLongChunk - 1) / kLongChunk;
+        const uint32_t chunk = shape.chunk;
+        const uint32_t nchunks = (len + chunk - 1) / chunk;
         if (nchunks >= 2 && low < nchunks) {
             const uint32_t first = gid - low;
-            const uint32_t cb = nb + low * kLongChunk;
-            const uint32_t ce = min(re, cb + kLongChunk);
+            const uint32_t cb = nb + low * chunk;
+            const uint32_t ce = min(re, cb + chunk);
             dev::Acc<T, EXT> a = range_sum<V, T, EXT, NT>(vals, cols, x, alpha, cb, ce, lo, hi, vec != 0);
             a = dev::block_reduce_acc(a, sm.red_s, sm.red_c);
             if (tid == 0) {

@@ -33,6 +33,21 @@ clsparseB200ComputeRowBlocksHost(const clsparseIdx_t* rowPointer, clsparseIdx_t 
                                  cl_ulong* rowBlocks, size_t capacity,
                                  clsparseIdx_t* rowBlockSize);
 
+/* clsparseCsrMetaCreate with a chosen row-block shape, the knobs the
+ * autotuner sweeps: blkSize (the reference's BLKSIZE, 512, 1024 or 2048),
+ * blkMultiplier (long rows are cut into blkMultiplier * blkSize chunks,
+ * 1..64), rowsForVector (blocks of at most this many rows are reduced one row
+ * at a time by the whole CTA, 1..256) and ctaThreads (threads per CTA of the
+ * adaptive kernel: 128, or 256 for blkSize >= 1024). The reference hard-codes
+ * these (src/library/include/clSPARSE-private.hpp:46-50) and passes them to
+ * ComputeRowBlocks (src/library/internal/data-types/csr-meta.hpp:52-269);
+ * clsparseCsrMetaCreate uses them unchanged. Any shape gives the same SpMV
+ * results up to summation order; the persistent solver (loop mode 2) needs
+ * the default shape and otherwise runs as loop mode 0. */
+CLSPARSE_EXPORT clsparseStatus
+clsparseB200CsrMetaCreateTuned(clsparseCsrMatrix* csrMatx, cl_uint blkSize, cl_uint blkMultiplier,
+                               cl_uint rowsForVector, cl_uint ctaThreads, clsparseControl control);
+
 /* Copies the row-block words of an existing meta to host memory. *count gets
  * the number of words (rowBlockSize / 2). */
 CLSPARSE_EXPORT clsparseStatus

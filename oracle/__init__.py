@@ -71,31 +71,45 @@ def ref_lib():
         L.ref_row_blocks_size.argtypes = [_u32p, C.c_uint32]
         L.ref_row_blocks.restype = C.c_uint32
         L.ref_row_blocks.argtypes = [_u32p, C.c_uint32, _u64p, C.c_uint32]
+        L.ref_row_blocks_shape_size.restype = C.c_uint32
+        L.ref_row_blocks_shape_size.argtypes = [_u32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
+        L.ref_row_blocks_shape.restype = C.c_uint32
+        L.ref_row_blocks_shape.argtypes = [_u32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _u64p,
+                                           C.c_uint32]
         _ref = L
     return _ref
 
 
-def row_blocks(rp: np.ndarray):
-    """Row-block words and rowBlockSize of the oracle restatement."""
+def row_blocks(rp: np.ndarray, shape=(1024, 3, 1)):
+    """Row-block words and rowBlockSize of the oracle restatement; shape =
+    (BLKSIZE, BLOCK_MULTIPLIER, ROWS_FOR_VECTOR), the reference's by default."""
     rp = np.ascontiguousarray(rp, dtype=np.uint32)
     n = len(rp) - 1
     L = lib()
-    dry = L.oracle_row_blocks(rp, n, 1024, 3, 1, None)
+    blk, mult, rfv = (int(v) for v in shape[:3])
+    dry = L.oracle_row_blocks(rp, n, blk, mult, rfv, None)
     words = np.zeros(dry // 2 + 1, dtype=np.uint64)
-    size = L.oracle_row_blocks(rp, n, 1024, 3, 1, words.ctypes.data)
+    size = L.oracle_row_blocks(rp, n, blk, mult, rfv, words.ctypes.data)
     return words[: size // 2].copy(), size, dry
 
 
-def ref_row_blocks(rp: np.ndarray):
-    """Row-block words and rowBlockSize of the reference's own ComputeRowBlocks."""
+def ref_row_blocks(rp: np.ndarray, shape=None):
+    """Row-block words and rowBlockSize of the reference's own ComputeRowBlocks
+    (its compiled-in shape, or shape = (BLKSIZE, BLOCK_MULTIPLIER, ROWS_FOR_VECTOR))."""
     L = ref_lib()
     if L is None:
         raise RuntimeError("oracle/_ref/librefbins.so not built (reference tree absent)")
     rp = np.ascontiguousarray(rp, dtype=np.uint32)
     n = len(rp) - 1
-    dry = L.ref_row_blocks_size(rp, n)
-    words = np.zeros(dry // 2 + 1, dtype=np.uint64)
-    size = L.ref_row_blocks(rp, n, words, dry // 2 + 1)
+    if shape is None:
+        dry = L.ref_row_blocks_size(rp, n)
+        words = np.zeros(dry // 2 + 1, dtype=np.uint64)
+        size = L.ref_row_blocks(rp, n, words, dry // 2 + 1)
+    else:
+        blk, mult, rfv = (int(v) for v in shape[:3])
+        dry = L.ref_row_blocks_shape_size(rp, n, blk, mult, rfv)
+        words = np.zeros(dry // 2 + 1, dtype=np.uint64)
+        size = L.ref_row_blocks_shape(rp, n, blk, mult, rfv, words, dry // 2 + 1)
     return words[: size // 2].copy(), size, dry
 
 

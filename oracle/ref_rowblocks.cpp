@@ -22,4 +22,19 @@ unsigned int ref_row_blocks(const unsigned int* rp, unsigned int n, unsigned lon
     return size;
 }
 
+// Same with a chosen row-block shape (blkSize, blkMultiplier, rows_for_vector
+// are parameters of the reference's ComputeRowBlocks; the library's
+// clsparseB200CsrMetaCreateTuned must reproduce these words).
+unsigned int ref_row_blocks_shape_size(const unsigned int* rp, unsigned int n, unsigned int blk, unsigned int mult,
+                                       unsigned int rfv) {
+    return static_cast<unsigned int>(ComputeRowBlocksSize(rp, n, blk, mult, rfv));
+}
+
+unsigned int ref_row_blocks_shape(const unsigned int* rp, unsigned int n, unsigned int blk, unsigned int mult,
+                                  unsigned int rfv, unsigned long long* words, unsigned int capacity_words) {
+    clsparseIdx_t size = capacity_words * 2;
+    ComputeRowBlocks(reinterpret_cast<cl_ulong*>(words), size, rp, n, blk, mult, rfv, true);
+    return size;
+}
+
 }

@@ -19,6 +19,10 @@ sys.path.insert(0, str(ROOT))
 import oracle  # noqa: E402
 
 
+# (BLKSIZE, BLOCK_MULTIPLIER, ROWS_FOR_VECTOR) shapes pinned besides the default
+SHAPES = [(512, 1, 1), (512, 8, 4), (2048, 3, 1), (2048, 1, 4), (1024, 8, 2)]
+
+
 def cases():
     """Row-length patterns covering every branch of the binning."""
     rng = np.random.default_rng(20251203)
@@ -63,6 +67,20 @@ def main():
     dst = Path(__file__).resolve().parent / "rowblocks.npz"
     np.savez_compressed(dst, **arrays)
     print(f"wrote {dst} ({len(arrays) // 3} cases)")
+    # the same cases under the non-default row-block shapes the tuner sweeps
+    shaped = {}
+    for shape in SHAPES:
+        tag = "x".join(str(v) for v in shape)
+        for name, lens in cases().items():
+            lens = np.asarray(lens, dtype=np.int64)
+            rp = np.zeros(len(lens) + 1, dtype=np.uint32)
+            rp[1:] = np.cumsum(lens)
+            words, size, dry = oracle.ref_row_blocks(rp, shape)
+            shaped[f"{tag}__{name}__words"] = words
+            shaped[f"{tag}__{name}__size"] = np.array([size, dry], dtype=np.uint32)
+    dst = Path(__file__).resolve().parent / "rowblocks_shapes.npz"
+    np.savez_compressed(dst, **shaped)
+    print(f"wrote {dst} ({len(shaped) // 2} cases)")
 
 
 if __name__ == "__main__":

@@ -42,6 +42,29 @@ def test_library_host_binning_matches_reference(libso, name, rp, words, size):
     np.testing.assert_array_equal(out[: size[0] // 2], words)
 
 
+GOLD_SHAPES = Path(__file__).resolve().parent / "golden" / "rowblocks_shapes.npz"
+
+
+def _shape_cases():
+    rps = np.load(GOLD)
+    d = np.load(GOLD_SHAPES)
+    out = []
+    for key in sorted(k for k in d.files if k.endswith("__words")):
+        tag, name, _ = key.split("__")
+        shape = tuple(int(v) for v in tag.split("x"))
+        out.append((f"{tag}-{name}", shape, rps[f"{name}__rp"], d[key], d[f"{tag}__{name}__size"]))
+    return out
+
+
+@pytest.mark.parametrize("cid,shape,rp,words,size", _shape_cases(), ids=[c[0] for c in _shape_cases()])
+def test_oracle_row_blocks_shapes_match_reference(orc, cid, shape, rp, words, size):
+    """Non-default row-block shapes (the autotuner's knobs) against the
+    reference's ComputeRowBlocks called with the same shape."""
+    w, s, dry = orc.row_blocks(rp, shape)
+    assert s == size[0] and dry == size[1]
+    np.testing.assert_array_equal(w, words)
+
+
 def test_probe_case_layout():
     """Rows {3,3,2000,4}: one stream block of 2 rows (128 threads/row), one
     vector row, one trailing row -- the layout of csr-meta.hpp:70-90."""

@@ -110,6 +110,61 @@ def test_meta_words_equal_reference_binning(ctrl, orc):
         np.testing.assert_array_equal(A.row_blocks(), orc.ref_row_blocks(rp)[0])
 
 
+TUNED_SHAPES = [(512, 1, 1, 128), (512, 8, 4, 128), (2048, 3, 1, 256), (2048, 1, 4, 128), (1024, 8, 2, 256),
+                (1024, 3, 1, 256)]
+
+
+@pytest.mark.parametrize("shape", TUNED_SHAPES, ids=["x".join(map(str, s)) for s in TUNED_SHAPES])
+def test_tuned_meta_words_match_reference(ctrl, shape):
+    """clsparseB200CsrMetaCreateTuned's words against the reference's
+    ComputeRowBlocks with the same shape (tests/golden/rowblocks_shapes.npz)."""
+    from pathlib import Path
+    gold = Path(__file__).resolve().parent / "golden"
+    rps = np.load(gold / "rowblocks.npz")
+    d = np.load(gold / "rowblocks_shapes.npz")
+    tag = "x".join(str(v) for v in shape[:3])
+    names = sorted({k.split("__")[1] for k in d.files if k.startswith(tag + "__")})
+    if not names:
+        pytest.skip("shape not in the golden set")
+    for name in names:
+        rp = rps[f"{name}__rp"]
+        if len(rp) < 2 or int(rp[-1]) == 0:
+            continue
+        n = len(rp) - 1
+        col = np.zeros(int(rp[-1]), dtype=np.uint32)
+        A = api.CsrMatrix.from_numpy(rp, col, np.ones(int(rp[-1])), num_cols=1)
+        A.create_meta(ctrl, shape=shape)
+        np.testing.assert_array_equal(A.row_blocks(), d[f"{tag}__{name}__words"], err_msg=name)
+        assert n == A.num_rows
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+@pytest.mark.parametrize("shape", TUNED_SHAPES, ids=["x".join(map(str, s)) for s in TUNED_SHAPES])
+@pytest.mark.parametrize("case", ["threshold_rows", "long_rows_between_short", "lognormal", "many_short"])
+def test_spmv_tuned_shapes(ctrl, orc, dtype, shape, case):
+    """SpMV parity for every row-block shape the autotuner may pick."""
+    lens = EDGE_LENGTHS[case]
+    ncols = 60_000
+    rp, col, val = matgen.random_lengths(lens, ncols, seed=len(lens))
+    x, y0 = vecs(len(lens), ncols, 5)
+    A = api.CsrMatrix.from_numpy(rp, col, val, num_cols=ncols, dtype=dtype)
+    A.create_meta(ctrl, shape=shape)
+    xt = torch.tensor(x, dtype=dtype, device="cuda")
+    for alpha, beta in ((1.0, 0.0), (2.5, -1.5)):
+        yt = torch.tensor(y0, dtype=dtype, device="cuda")
+        api.csrmv(torch.tensor([alpha], dtype=dtype, device="cuda"), A, xt,
+                  torch.tensor([beta], dtype=dtype, device="cuda"), yt, ctrl)
+        assert_parity(orc, rp, col, val, x, y0, alpha, beta, yt.cpu().numpy(), dtype)
+
+
+def test_tuned_meta_rejects_bad_shapes(ctrl):
+    rp, col, val = matgen.poisson2d(8)
+    A = api.CsrMatrix.from_numpy(rp, col, val)
+    for bad in ((256, 3, 1, 128), (512, 3, 1, 256), (1024, 0, 1, 128), (1024, 3, 0, 128), (1024, 3, 1, 64)):
+        with pytest.raises(api.ClsparseError):
+            A.create_meta(ctrl, shape=bad)
+
+
 def test_spmv_beta_zero_does_not_read_y(ctrl):
     rp, col, val = matgen.random_lengths([3, 0, 5000, 40, 12000, 1], 20_000, seed=2)
     for meta in (True, False):
