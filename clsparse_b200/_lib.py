@@ -184,6 +184,7 @@ SIGNATURES = {
     "clsparseB200SetSolverLoopMode": (clsparseStatus, [_V, cl_int]),
     "clsparseB200SolverSetNormType": (clsparseStatus, [_V, cl_int]),
     "clsparseDcsrcgMixed": (clsparseStatus, [_D, _M, _D, _V, cl_int, C.c_double, P(clsparseB200MixedInfo), _V]),
+    "clsparseDcsrbicgStabMixed": (clsparseStatus, [_D, _M, _D, _V, cl_int, C.c_double, P(clsparseB200MixedInfo), _V]),
 }
 
 _lib = None

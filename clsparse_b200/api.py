@@ -230,6 +230,17 @@ def cg_mixed(x: torch.Tensor, A: CsrMatrix, b: torch.Tensor, sc: SolverControl, 
     return {f[0]: getattr(info, f[0]) for f in info._fields_}
 
 
+def bicgstab_mixed(x: torch.Tensor, A: CsrMatrix, b: torch.Tensor, sc: SolverControl, ctrl: Control,
+                   inner: str = "fp32", inner_tol: float = 1e-4) -> dict:
+    """FP64 iterative refinement with an FP32- or BF16-valued inner BiCGStab
+    (clsparseDcsrbicgStabMixed); returns the refinement statistics."""
+    info = L.clsparseB200MixedInfo()
+    prec = {"fp32": 0, "bf16": 1}[inner]
+    check(lib().clsparseDcsrbicgStabMixed(C.byref(vector(x)), C.byref(A.s), C.byref(vector(b)), sc.handle, prec,
+                                          inner_tol, C.byref(info), ctrl.handle), "clsparseDcsrbicgStabMixed")
+    return {f[0]: getattr(info, f[0]) for f in info._fields_}
+
+
 def blas1(name: str, *args, ctrl: Control):
     """Calls a cldense* entry point; tensors become vectors, 1-element tensors
     passed as ('s', t) become scalars."""

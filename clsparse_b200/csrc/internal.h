@@ -219,6 +219,11 @@ template <typename V, typename T>
 clsparseStatus cg_solve_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
                               clSParseSolverControl sc, clsparseControl c, WarmStart* ws = nullptr);
 
+// BiCGStab with matrix values of type V and vectors in T (solvers.cu).
+template <typename V, typename T>
+clsparseStatus bicg_solve_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                                clSParseSolverControl sc, clsparseControl c);
+
 // PCG with the factorized preconditioner M^-1 = G^T G (solvers.cu).
 template <typename V, typename T, typename VG>
 clsparseStatus pcg_factor_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,

@@ -1,5 +1,6 @@
-// Mixed-precision iterative refinement around CG (clsparseDcsrcgMixed), a
-// project extension with no reference counterpart.
+// Mixed-precision iterative refinement around CG (clsparseDcsrcgMixed) and
+// BiCGStab (clsparseDcsrbicgStabMixed), project extensions with no reference
+// counterpart.
 //
 // Outer loop, all in FP64 on the device: r = b - A x with the FP64 matrix,
 // ||r||_2 / ||b||_2 is the stop test. Inner solve: Jacobi-PCG (the library's
@@ -84,10 +85,13 @@ struct Factor {
     CsrView<__nv_bfloat16> G, GT;
 };
 
+enum class Inner { Cg, BiCgStab };
+
 template <typename V>
 clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
                       clSParseSolverControl sc, double inner_tol, clsparseB200MixedInfo* info,
-                      clsparseControl c, const Factor* factor = nullptr, int* fell_back = nullptr) {
+                      clsparseControl c, const Factor* factor = nullptr, int* fell_back = nullptr,
+                      Inner method = Inner::Cg) {
     const size_t n = A->num_rows, nnz = A->num_nonzeros;
     MixedWork& w = work_of(c);
     if (w.lowvals.ensure(nnz * sizeof(V) + 256) != cudaSuccess || w.y.ensure(n * 8 + 256) != cudaSuccess ||
@@ -193,7 +197,9 @@ clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const clden
         ws.warm = have_prev && prev_factor == use_factor && !breakdown && res <= 2.0 * predicted;
         inner.nIters = 0;
         inner.deviceStatus = 0;
-        if (use_factor)
+        if (method == Inner::BiCgStab)  // restarted every refinement step
+            st = bicg_solve_typed<V, float>(&dvec, &Alow, &rvec, &inner, c);
+        else if (use_factor)
             st = pcg_factor_typed<V, float, __nv_bfloat16>(&dvec, &Alow, &rvec, &inner, factor->G, factor->GT,
                                                             c, &ws);
         else
@@ -239,6 +245,27 @@ clsparseStatus clsparseDcsrcgMixed(cldenseVector* x, const clsparseCsrMatrix* A,
     if (innerPrecision == 0)
         return refine<float>(x, A, b, solverControl, innerTolerance, info, control);
     return refine<__nv_bfloat16>(x, A, b, solverControl, innerTolerance, info, control);
+}
+
+clsparseStatus clsparseDcsrbicgStabMixed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                                         clSParseSolverControl solverControl, cl_int innerPrecision,
+                                         cl_double innerTolerance, clsparseB200MixedInfo* info,
+                                         clsparseControl control) {
+    clsparseStatus st = check_entry(control);
+    if (st != clsparseSuccess) return st;
+    if (solverControl == nullptr) return clsparseInvalidSolverControlObject;
+    if (!x || !A || !b || !info) return clsparseInvalidValue;
+    if (A->num_rows != A->num_cols || A->num_rows != x->num_values || A->num_cols != b->num_values)
+        return clsparseInvalidSystemSize;
+    if (innerPrecision != 0 && innerPrecision != 1) return clsparseInvalidType;
+    std::memset(info, 0, sizeof(*info));
+    if (A->num_rows == 0) return clsparseSuccess;
+    DeviceGuard g(control->device);
+    if (innerPrecision == 0)
+        return refine<float>(x, A, b, solverControl, innerTolerance, info, control, nullptr, nullptr,
+                             Inner::BiCgStab);
+    return refine<__nv_bfloat16>(x, A, b, solverControl, innerTolerance, info, control, nullptr, nullptr,
+                                 Inner::BiCgStab);
 }
 
 clsparseStatus clsparseDcsrcgLearned(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,

@@ -868,7 +868,7 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
     return stt;
 }
 
-template <typename T>
+template <typename V, typename T>
 clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
                           clSParseSolverControl sc, clsparseControl c) {
     clsparseStatus stt = check_solver_args(xv, A, bv, sc, c);
@@ -877,9 +877,9 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
     const size_t n = A->num_rows;
     if (!c->solver_cache) c->solver_cache = std::make_unique<SolverCache>();
     SolverCache& cache = *c->solver_cache;
-    const CsrView<T> Av = view_of<T>(A);
+    const CsrView<V> Av = view_of<V>(A);
     const uint32_t spmv_ctas = spmv_num_ctas(Av.meta, Av.nrows, Av.nnz);
-    const SolverKey key = make_key(2, sizeof(T), sizeof(T), sc, c, A, xv, bv);
+    const SolverKey key = make_key(2, sizeof(V), sizeof(T), sc, c, A, xv, bv);
     bool rebuild = false;
     stt = prepare_cache<T>(c, cache, key, 11, n, spmv_ctas, rebuild);
     if (stt != clsparseSuccess) return stt;
@@ -920,10 +920,10 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
         BicgArgs<T> aa = a;
         aa.cond = h;
         if (aa.invD)
-            extract_inv_diag_kernel<T, T><<<vg, kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
+            extract_inv_diag_kernel<V, T><<<vg, kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
                                                                   invD, st);
         SpmvEpilogue none;
-        launch_csrmv<T, T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
+        launch_csrmv<V, T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
         bicg_init_kernel<T><<<vg, kThreads, 0, s>>>(aa);
     };
     auto body = [&](cudaStream_t s, unsigned long long h) {
@@ -937,7 +937,7 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
         e1.op = EpiOp::BicgAlpha;
         e1.state = st;
         e1.done = &st->done;
-        launch_csrmv<T, T>(Av, &st->one, &st->zero, aa.Mp, aa.AMp, ext, e1, s);
+        launch_csrmv<V, T>(Av, &st->one, &st->zero, aa.Mp, aa.AMp, ext, e1, s);
         bicg_s_kernel<T><<<vg, kThreads, 0, s>>>(aa);
         SpmvEpilogue e2;
         e2.ndots = 2;
@@ -948,7 +948,7 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
         e2.op = EpiOp::BicgOmega;
         e2.state = st;
         e2.done = &st->done;
-        launch_csrmv<T, T>(Av, &st->one, &st->zero, aa.Ms, aa.AMs, ext, e2, s);
+        launch_csrmv<V, T>(Av, &st->one, &st->zero, aa.Ms, aa.AMs, ext, e2, s);
         bicg_x_kernel<T><<<vg, kThreads, 0, s>>>(aa);
         bicg_p_kernel<T><<<vg, kThreads, 0, s>>>(aa);
     };
@@ -1123,6 +1123,18 @@ template clsparseStatus pcg_factor_typed<double, double, double>(
     const CsrView<double>&, const CsrView<double>&, clsparseControl, WarmStart*);
 
 template <typename V, typename T>
+clsparseStatus bicg_solve_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                                clSParseSolverControl sc, clsparseControl c) {
+    return bicg_solve<V, T>(x, A, b, sc, c);
+}
+template clsparseStatus bicg_solve_typed<float, float>(cldenseVector*, const clsparseCsrMatrix*,
+                                                       const cldenseVector*, clSParseSolverControl,
+                                                       clsparseControl);
+template clsparseStatus bicg_solve_typed<__nv_bfloat16, float>(cldenseVector*, const clsparseCsrMatrix*,
+                                                               const cldenseVector*, clSParseSolverControl,
+                                                               clsparseControl);
+
+template <typename V, typename T>
 clsparseStatus cg_solve_typed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
                               clSParseSolverControl sc, clsparseControl c, WarmStart* ws) {
     return cg_solve<V, T>(x, A, b, sc, c, ws);
@@ -1156,13 +1168,13 @@ clsparseStatus clsparseDcsrcg(cldenseVector* x, const clsparseCsrMatrix* A, cons
 clsparseStatus clsparseScsrbicgStab(cldenseVector* x, const clsparseCsrMatrix* A,
                                     const cldenseVector* b, clSParseSolverControl solverControl,
                                     clsparseControl control) {
-    return bicg_solve<float>(x, A, b, solverControl, control);
+    return bicg_solve<float, float>(x, A, b, solverControl, control);
 }
 
 clsparseStatus clsparseDcsrbicgStab(cldenseVector* x, const clsparseCsrMatrix* A,
                                     const cldenseVector* b, clSParseSolverControl solverControl,
                                     clsparseControl control) {
-    return bicg_solve<double>(x, A, b, solverControl, control);
+    return bicg_solve<double, double>(x, A, b, solverControl, control);
 }
 
 }  // extern "C"

@@ -97,6 +97,17 @@ clsparseDcsrcgMixed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseV
                     cl_double innerTolerance, clsparseB200MixedInfo* info,
                     clsparseControl control);
 
+/* The same FP64 refinement around BiCGStab (reference
+ * src/library/solvers/biconjugate-gradients-stabilized.hpp:41-268, run on
+ * the FP32- or BF16-valued copy with FP32 vectors). No symmetry needed. The
+ * inner BiCGStab restarts at every refinement step (the short recurrences of
+ * BiCGStab have no residual-replacement continuation here). Project
+ * extension, no reference counterpart. */
+CLSPARSE_EXPORT clsparseStatus
+clsparseDcsrbicgStabMixed(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                          clSParseSolverControl solverControl, cl_int innerPrecision,
+                          cl_double innerTolerance, clsparseB200MixedInfo* info, clsparseControl control);
+
 /* Per-system results of a batched solve. The two arrays are optional (NULL) or
  * hold numSystems entries each. */
 typedef struct clsparseB200BatchResult_

@@ -73,3 +73,37 @@ def test_l2_norm_option_matches_oracle_residual(ctrl):
     sc.release()
     assert info["currentResidual"] <= 1e-10
     assert true_residual(rp, col, val, x.cpu().numpy(), b) <= 2e-10
+
+
+def convection_diffusion(m, peclet=0.4):
+    """2D 5-point diffusion plus first-order upwind convection in x: a
+    nonsymmetric, diagonally dominant operator (a BiCGStab case)."""
+    rp, col, val = matgen.poisson2d(m)
+    A = sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64)))
+    n = m * m
+    i = np.arange(n)
+    west = (i % m) != 0
+    C = sp.csr_matrix((np.full(west.sum(), -peclet), (i[west], i[west] - 1)), shape=(n, n)) + \
+        sp.diags(np.where(west, peclet, 0.0))
+    M = (A + C).tocsr()
+    M.sort_indices()
+    return M.indptr.astype(np.uint32), M.indices.astype(np.uint32), M.data
+
+
+@pytest.mark.parametrize("inner", ["fp32", "bf16"])
+def test_mixed_bicgstab_reaches_fp64_residual(ctrl, inner):
+    rp, col, val = convection_diffusion(40)
+    n = len(rp) - 1
+    b = np.random.default_rng(3).uniform(-1, 1, n)
+    A = api.CsrMatrix.from_numpy(rp, col, val)
+    A.create_meta(ctrl)
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    sc = api.SolverControl(L.DIAGONAL, 20000, 1e-10, 0.0)
+    info = api.bicgstab_mixed(x, A, torch.tensor(b, device="cuda"), sc, ctrl, inner=inner, inner_tol=1e-3)
+    sc.release()
+    res = true_residual(rp, col, val, x.cpu().numpy(), b)
+    assert info["converged"] == 1, info
+    assert res <= 1.5e-10, (res, info)
+    import scipy.sparse.linalg as spla
+    xd = spla.spsolve(sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64))).tocsc(), b)
+    assert np.linalg.norm(x.cpu().numpy() - xd) / np.linalg.norm(xd) <= 1e-8
