@@ -121,6 +121,80 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// Tensor-core form of linear_fwd for the BF16 forward pass (weights and
+// input activations rounded to BF16, FP32 accumulation): warp-level
+// mma.sync m16n8k16 BF16 tiles. A persistent CTA (4 warps) stages the M x K
+// weight tile once, then walks 64-row tiles of X: each warp multiplies 16
+// rows by all M outputs; bias, ReLU and the residual are applied in the
+// epilogue. K must be a multiple of 16, M of 8.
+template <int M, int K1, int K2>
+__global__ void __launch_bounds__(128)
+    linear_fwd_tc(const float* __restrict__ X1, const float* __restrict__ X2, const float* __restrict__ W,
+                  const float* __restrict__ b, const float* __restrict__ R, float* __restrict__ Y,
+                  float* __restrict__ A, size_t n, int act) {
+    constexpr int K = K1 + K2;
+    constexpr int KP = K + 8;  // padded row length (bf16): fragment loads hit distinct banks
+    constexpr int TR = 64;     // rows per tile
+    static_assert(K % 16 == 0 && M % 8 == 0, "tile shape");
+    __shared__ __align__(16) __nv_bfloat16 sw[M * KP];
+    __shared__ __align__(16) __nv_bfloat16 sx[TR * KP];
+    __shared__ float sb[M];
+    for (int i = threadIdx.x; i < M * K; i += 128) sw[(i / K) * KP + (i % K)] = __float2bfloat16_rn(W[i]);
+    for (int i = threadIdx.x; i < M; i += 128) sb[i] = b ? b[i] : 0.f;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int rw = warp * 16;
+    const size_t ntiles = (n + TR - 1) / TR;
+    for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const size_t r0 = tile * TR;
+        __syncthreads();  // weights staged; the previous tile's fragments read
+        for (int i = threadIdx.x; i < TR * K; i += 128) {
+            const int rr = i / K, kk = i % K;
+            const size_t row = r0 + rr;
+            float v = 0.f;
+            if (row < n) v = kk < K1 ? X1[row * K1 + kk] : X2[row * K2 + (kk - K1)];
+            sx[rr * KP + kk] = __float2bfloat16_rn(v);
+        }
+        __syncthreads();
+        float acc[M / 8][4];
+#pragma unroll
+        for (int t = 0; t < M / 8; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
+#pragma unroll
+        for (int k0 = 0; k0 < K; k0 += 16) {
+            const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&sx[(rw + g) * KP + k0 + 2 * t4]);
+            const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&sx[(rw + g + 8) * KP + k0 + 2 * t4]);
+            const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&sx[(rw + g) * KP + k0 + 8 + 2 * t4]);
+            const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&sx[(rw + g + 8) * KP + k0 + 8 + 2 * t4]);
+#pragma unroll
+            for (int t = 0; t < M / 8; ++t) {
+                const int col = t * 8 + g;
+                const uint32_t b0 = *reinterpret_cast<const uint32_t*>(&sw[col * KP + k0 + 2 * t4]);
+                const uint32_t b1 = *reinterpret_cast<const uint32_t*>(&sw[col * KP + k0 + 8 + 2 * t4]);
+                asm volatile(
+                    "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+                    "{%8,%9}, {%0,%1,%2,%3};"
+                    : "+f"(acc[t][0]), "+f"(acc[t][1]), "+f"(acc[t][2]), "+f"(acc[t][3])
+                    : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < M / 8; ++t)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const size_t row = r0 + rw + g + 8 * h;
+                if (row >= n) continue;
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const int m = t * 8 + 2 * t4 + j;
+                    const float z = acc[t][2 * h + j] + sb[m];
+                    const float a = act ? fmaxf(z, 0.f) : z;
+                    if (A) A[row * M + m] = a;
+                    Y[row * M + m] = R ? R[row * M + m] + a : a;
+                }
+            }
+    }
+}
+
 // Backward of linear_fwd. dZ = dY * act'(A); dX1 += dZ W1, dX2 += dZ W2 (when
 // given); per-CTA partial sums of dW (M x K) and db (M) go to `part` at
 // blockIdx * (M*K + M).
@@ -786,18 +860,36 @@ void forward(_clsparseB200Spai* net, int bf16, cudaStream_t s) {
     const uint32_t tiles = nblk(n, kRows);
     linear_fwd<H, NF, 0><<<tiles, 256, 0, s>>>(gr.F, nullptr, P + o.w_in, P + o.b_in, nullptr, gr.Hs[0],
                                                 nullptr, n, 1, bf16);
+    // BF16 forward: the dense layers on tensor cores; FP32 weights (gradient
+    // checks): CUDA-core FMAs.
+    const uint32_t tc_grid = static_cast<uint32_t>(std::min<size_t>((n + 63) / 64, 1184));
     for (int l = 0; l < NL; ++l) {
-        linear_fwd<H, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[l], nullptr, P + o.U[l], nullptr, nullptr, gr.Hu[l],
-                                                  nullptr, n, 0, bf16);
+        if (bf16)
+            linear_fwd_tc<H, H, 0><<<tc_grid, 128, 0, s>>>(gr.Hs[l], nullptr, P + o.U[l], nullptr, nullptr,
+                                                           gr.Hu[l], nullptr, n, 0);
+        else
+            linear_fwd<H, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[l], nullptr, P + o.U[l], nullptr, nullptr, gr.Hu[l],
+                                                      nullptr, n, 0, bf16);
         message_fwd<<<warps_grid(n), 256, 0, s>>>(gr.rp, gr.cols, gr.ehat, gr.Hu[l], P + o.w[l], P + o.c[l],
                                                   gr.S[l], gr.n, bf16);
-        linear_fwd<H, H, H><<<tiles, 256, 0, s>>>(gr.Hs[l], gr.S[l], P + o.V[l], P + o.d[l], gr.Hs[l],
-                                                  gr.Hs[l + 1], gr.Au[l], n, 1, bf16);
+        if (bf16)
+            linear_fwd_tc<H, H, H><<<tc_grid, 128, 0, s>>>(gr.Hs[l], gr.S[l], P + o.V[l], P + o.d[l], gr.Hs[l],
+                                                           gr.Hs[l + 1], gr.Au[l], n, 1);
+        else
+            linear_fwd<H, H, H><<<tiles, 256, 0, s>>>(gr.Hs[l], gr.S[l], P + o.V[l], P + o.d[l], gr.Hs[l],
+                                                      gr.Hs[l + 1], gr.Au[l], n, 1, bf16);
     }
-    linear_fwd<HO, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[NL], nullptr, P + o.P, nullptr, nullptr, gr.Hp, nullptr,
-                                               n, 0, bf16);
-    linear_fwd<HO, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[NL], nullptr, P + o.Q, nullptr, nullptr, gr.Hq, nullptr,
-                                               n, 0, bf16);
+    if (bf16) {
+        linear_fwd_tc<HO, H, 0><<<tc_grid, 128, 0, s>>>(gr.Hs[NL], nullptr, P + o.P, nullptr, nullptr, gr.Hp,
+                                                        nullptr, n, 0);
+        linear_fwd_tc<HO, H, 0><<<tc_grid, 128, 0, s>>>(gr.Hs[NL], nullptr, P + o.Q, nullptr, nullptr, gr.Hq,
+                                                        nullptr, n, 0);
+    } else {
+        linear_fwd<HO, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[NL], nullptr, P + o.P, nullptr, nullptr, gr.Hp,
+                                                   nullptr, n, 0, bf16);
+        linear_fwd<HO, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[NL], nullptr, P + o.Q, nullptr, nullptr, gr.Hq,
+                                                   nullptr, n, 0, bf16);
+    }
     output_fwd<<<warps_grid(n), 256, 0, s>>>(gr.Lrp, gr.Lcol, gr.Le, gr.Hs[NL], gr.Hp, gr.Hq, P, o, gr.g,
                                              gr.n, bf16);
 }
