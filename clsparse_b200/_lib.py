@@ -34,6 +34,8 @@ clsparseInvalidSize = -1021
 clsparseInvalidMemObj = -1020
 clsparseInsufficientMemory = -1019
 clsparseInvalidControlObject = -1018
+clsparseInvalidFile = -1017
+clsparseInvalidFileFormat = -1016
 clsparseInvalidKernelExecution = -1015
 clsparseInvalidSolverControlObject = -2048
 clsparseInvalidSystemSize = -2047
@@ -132,6 +134,9 @@ SIGNATURES = {
     "clsparseDCooMatrixfromFile": (clsparseStatus, [P(clsparseCooMatrix), C.c_char_p, _V, cl_bool]),
     "clsparseSCsrMatrixfromFile": (clsparseStatus, [_M, C.c_char_p, _V, cl_bool]),
     "clsparseDCsrMatrixfromFile": (clsparseStatus, [_M, C.c_char_p, _V, cl_bool]),
+    "clsparseB200ReadMatrixMarketHost": (clsparseStatus, [C.c_char_p, cl_bool, P(clsparseIdx_t), P(clsparseIdx_t),
+                                                          P(clsparseIdx_t), P(clsparseIdx_t), P(clsparseIdx_t),
+                                                          P(C.c_double), C.c_size_t]),
     "clsparseCsrMetaSize": (clsparseMetaSizeResult, [_M, _V]),
     "clsparseCsrMetaCreate": (clsparseStatus, [_M, _V]),
     "clsparseCsrMetaDelete": (clsparseStatus, [_M]),

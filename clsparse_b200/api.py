@@ -113,6 +113,23 @@ class CsrMatrix:
         t_val = torch.from_numpy(np.asarray(val)).to(device=device, dtype=dtype)
         return cls(t_rp, t_col, t_val, ncols)
 
+    @classmethod
+    def from_file(cls, path, ctrl: "Control", dtype=torch.float64, read_explicit_zeroes: bool = False):
+        """clsparseHeaderfromFile + clsparse{S,D}CsrMatrixfromFile into new
+        device tensors (allocated with the header's sizes)."""
+        nnz, nr, nc = L.clsparseIdx_t(), L.clsparseIdx_t(), L.clsparseIdx_t()
+        check(lib().clsparseHeaderfromFile(C.byref(nnz), C.byref(nr), C.byref(nc), str(path).encode()),
+              "clsparseHeaderfromFile")
+        rp = torch.zeros(nr.value + 1, dtype=torch.int32, device="cuda")
+        col = torch.zeros(max(nnz.value, 1), dtype=torch.int32, device="cuda")
+        val = torch.zeros(max(nnz.value, 1), dtype=dtype, device="cuda")
+        m = cls(rp, col, val, nc.value)
+        fn = "clsparseDCsrMatrixfromFile" if dtype == torch.float64 else "clsparseSCsrMatrixfromFile"
+        check(getattr(lib(), fn)(C.byref(m.s), str(path).encode(), ctrl.handle, 1 if read_explicit_zeroes else 0), fn)
+        k = m.s.num_nonzeros
+        m.col, m.val = m.col[:k], m.val[:k]
+        return m
+
     @property
     def num_rows(self):
         return self.s.num_rows
@@ -239,6 +256,24 @@ def bicgstab_mixed(x: torch.Tensor, A: CsrMatrix, b: torch.Tensor, sc: SolverCon
     check(lib().clsparseDcsrbicgStabMixed(C.byref(vector(x)), C.byref(A.s), C.byref(vector(b)), sc.handle, prec,
                                           inner_tol, C.byref(info), ctrl.handle), "clsparseDcsrbicgStabMixed")
     return {f[0]: getattr(info, f[0]) for f in info._fields_}
+
+
+def read_mtx_host(path, read_explicit_zeroes: bool = False):
+    """A Matrix Market file as host CSR (rp, col, val) via
+    clsparseB200ReadMatrixMarketHost (no GPU)."""
+    nr, nc, nnz = L.clsparseIdx_t(), L.clsparseIdx_t(), L.clsparseIdx_t()
+    p = str(path).encode()
+    z = 1 if read_explicit_zeroes else 0
+    check(lib().clsparseB200ReadMatrixMarketHost(p, z, C.byref(nr), C.byref(nc), C.byref(nnz), None, None, None, 0),
+          "clsparseB200ReadMatrixMarketHost")
+    rp = np.zeros(nr.value + 1, dtype=np.uint32)
+    col = np.zeros(max(nnz.value, 1), dtype=np.uint32)
+    val = np.zeros(max(nnz.value, 1), dtype=np.float64)
+    check(lib().clsparseB200ReadMatrixMarketHost(
+        p, z, C.byref(nr), C.byref(nc), C.byref(nnz), rp.ctypes.data_as(C.POINTER(L.clsparseIdx_t)),
+        col.ctypes.data_as(C.POINTER(L.clsparseIdx_t)), val.ctypes.data_as(C.POINTER(C.c_double)), len(col)),
+        "clsparseB200ReadMatrixMarketHost")
+    return rp, col[: nnz.value], val[: nnz.value], nc.value
 
 
 def blas1(name: str, *args, ctrl: Control):

@@ -271,21 +271,6 @@ clsparseStatus clsparseB200SolverGetDeviceStatus(clSParseSolverControl s, cl_uin
 
 // ---- declared, outside the accelerated path ----
 
-clsparseStatus clsparseHeaderfromFile(clsparseIdx_t*, clsparseIdx_t*, clsparseIdx_t*, const char*) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseSCooMatrixfromFile(clsparseCooMatrix*, const char*, clsparseControl, cl_bool) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseDCooMatrixfromFile(clsparseCooMatrix*, const char*, clsparseControl, cl_bool) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseSCsrMatrixfromFile(clsparseCsrMatrix*, const char*, clsparseControl, cl_bool) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseDCsrMatrixfromFile(clsparseCsrMatrix*, const char*, clsparseControl, cl_bool) {
-    return clsparseNotImplemented;
-}
 clsparseStatus clsparseScoomv(const clsparseScalar*, const clsparseCooMatrix*, const cldenseVector*,
                               const clsparseScalar*, cldenseVector*, const clsparseControl) {
     return clsparseNotImplemented;

@@ -48,6 +48,17 @@ CLSPARSE_EXPORT clsparseStatus
 clsparseB200CsrMetaCreateTuned(clsparseCsrMatrix* csrMatx, cl_uint blkSize, cl_uint blkMultiplier,
                                cl_uint rowsForVector, cl_uint ctaThreads, clsparseControl control);
 
+/* Reads a Matrix Market file into HOST CSR arrays, with the same rules as
+ * clsparseDCsrMatrixfromFile (no GPU needed). With rowPointer, colIndices or
+ * values NULL only the sizes are returned; otherwise rowPointer needs
+ * numRows + 1 entries and colIndices / values `capacity` >= numNonzeros
+ * entries (clsparseInsufficientMemory if smaller). Project extension, no
+ * reference counterpart. */
+CLSPARSE_EXPORT clsparseStatus
+clsparseB200ReadMatrixMarketHost(const char* filePath, cl_bool read_explicit_zeroes, clsparseIdx_t* numRows,
+                                 clsparseIdx_t* numCols, clsparseIdx_t* numNonzeros, clsparseIdx_t* rowPointer,
+                                 clsparseIdx_t* colIndices, cl_double* values, size_t capacity);
+
 /* Copies the row-block words of an existing meta to host memory. *count gets
  * the number of words (rowBlockSize / 2). */
 CLSPARSE_EXPORT clsparseStatus

@@ -156,7 +156,14 @@ CLSPARSE_EXPORT clsparseStatus
 clsparseDcsrbicgStab(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
                      clSParseSolverControl solverControl, clsparseControl control); /* :480-482 */
 
-/* ---- Matrix Market I/O (reference clSPARSE.h:508-611): not implemented ---- */
+/* ---- Matrix Market input (reference clSPARSE.h:508-611, reader
+ * src/library/io/mm-reader.cpp:140-760): coordinate real / integer / pattern
+ * files with a ".mtx" path; symmetric files mirrored; explicit zeros dropped
+ * unless read_explicit_zeroes; entries sorted by (row, column). The device
+ * buffers are allocated by the caller with the sizes clsparseHeaderfromFile
+ * reports (nnz is an upper bound for symmetric files); the struct's sizes are
+ * set from the file. Pattern entries get seeded pseudo-random values in
+ * [0, 5) (the reference used rand()). ---- */
 CLSPARSE_EXPORT clsparseStatus
 clsparseHeaderfromFile(clsparseIdx_t* nnz, clsparseIdx_t* row, clsparseIdx_t* col,
                        const char* filePath);                                       /* :508-509 */
