@@ -72,6 +72,11 @@ class clsparseCooMatrix(C.Structure):
     ]
 
 
+# cldenseMajor (clSPARSE-xx.h)
+rowMajor = 1
+columnMajor = 2
+
+
 class cldenseMatrix(C.Structure):
     _fields_ = [
         ("num_rows", clsparseIdx_t), ("num_cols", clsparseIdx_t), ("lead_dim", clsparseIdx_t),

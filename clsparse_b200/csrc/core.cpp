@@ -279,14 +279,6 @@ clsparseStatus clsparseDcoomv(const clsparseScalar*, const clsparseCooMatrix*, c
                               const clsparseScalar*, cldenseVector*, const clsparseControl) {
     return clsparseNotImplemented;
 }
-clsparseStatus clsparseScsrmm(const clsparseScalar*, const clsparseCsrMatrix*, const cldenseMatrix*,
-                              const clsparseScalar*, cldenseMatrix*, const clsparseControl) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseDcsrmm(const clsparseScalar*, const clsparseCsrMatrix*, const cldenseMatrix*,
-                              const clsparseScalar*, cldenseMatrix*, const clsparseControl) {
-    return clsparseNotImplemented;
-}
 clsparseStatus clsparseScsrSpGemm(const clsparseCsrMatrix*, const clsparseCsrMatrix*,
                                   clsparseCsrMatrix*, const clsparseControl) {
     return clsparseNotImplemented;

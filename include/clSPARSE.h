@@ -280,7 +280,9 @@ clsparseDcoomv(const clsparseScalar* alpha, const clsparseCooMatrix* matx,
                const cldenseVector* x, const clsparseScalar* beta,
                cldenseVector* y, const clsparseControl control);                    /* :1126-1132 */
 
-/* ---- sparse BLAS-3 and conversions (reference clSPARSE.h:1159-1326): not implemented ---- */
+/* ---- sparse BLAS-3 (reference clSPARSE.h:1159-1187): C = alpha*A*B + beta*C,
+ * B and C dense (row-major as the reference indexes them; column-major ones
+ * are honoured too). SpGEMM and the conversions below are not implemented. ---- */
 CLSPARSE_EXPORT clsparseStatus
 clsparseScsrmm(const clsparseScalar* alpha, const clsparseCsrMatrix* sparseMatA,
                const cldenseMatrix* denseMatB, const clsparseScalar* beta,

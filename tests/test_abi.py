@@ -109,7 +109,7 @@ def test_out_of_path_entries_not_implemented(libso):
     libso.clsparseSetup()
     m = L.clsparseCooMatrix()
     assert libso.clsparseScoomv(None, C.byref(m), None, None, None, None) == L.clsparseNotImplemented
-    assert libso.clsparseScsrmm(None, None, None, None, None, None) == L.clsparseNotImplemented
+    assert libso.clsparseScsrSpGemm(None, None, None, None) == L.clsparseNotImplemented
     assert libso.clsparseHeaderfromFile(None, None, None, b"x.mtx") == L.clsparseInvalidValue
 
 
