@@ -271,40 +271,8 @@ clsparseStatus clsparseB200SolverGetDeviceStatus(clSParseSolverControl s, cl_uin
 
 // ---- declared, outside the accelerated path ----
 
-clsparseStatus clsparseScoomv(const clsparseScalar*, const clsparseCooMatrix*, const cldenseVector*,
-                              const clsparseScalar*, cldenseVector*, const clsparseControl) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseDcoomv(const clsparseScalar*, const clsparseCooMatrix*, const cldenseVector*,
-                              const clsparseScalar*, cldenseVector*, const clsparseControl) {
-    return clsparseNotImplemented;
-}
 clsparseStatus clsparseScsrSpGemm(const clsparseCsrMatrix*, const clsparseCsrMatrix*,
                                   clsparseCsrMatrix*, const clsparseControl) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseScsr2coo(const clsparseCsrMatrix*, clsparseCooMatrix*, const clsparseControl) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseDcsr2coo(const clsparseCsrMatrix*, clsparseCooMatrix*, const clsparseControl) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseScoo2csr(const clsparseCooMatrix*, clsparseCsrMatrix*, const clsparseControl) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseDcoo2csr(const clsparseCooMatrix*, clsparseCsrMatrix*, const clsparseControl) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseScsr2dense(const clsparseCsrMatrix*, cldenseMatrix*, const clsparseControl) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseDcsr2dense(const clsparseCsrMatrix*, cldenseMatrix*, clsparseControl) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseSdense2csr(const cldenseMatrix*, clsparseCsrMatrix*, const clsparseControl) {
-    return clsparseNotImplemented;
-}
-clsparseStatus clsparseDdense2csr(const cldenseMatrix*, clsparseCsrMatrix*, const clsparseControl) {
     return clsparseNotImplemented;
 }
 

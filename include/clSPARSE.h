@@ -270,7 +270,9 @@ CLSPARSE_EXPORT clsparseStatus
 clsparseDcsrmv(const clsparseScalar* alpha, const clsparseCsrMatrix* matx,
                const cldenseVector* x, const clsparseScalar* beta,
                cldenseVector* y, const clsparseControl control);                    /* :1085-1091 */
-/* Declared but never defined by the reference (clSPARSE.h:1106-1132). */
+/* Declared but never defined by the reference (clSPARSE.h:1106-1132). Here:
+ * y = alpha*A*x + beta*y like csrmv, for a COO matrix sorted by row
+ * (duplicates summed); beta == 0 overwrites y without reading it. */
 CLSPARSE_EXPORT clsparseStatus
 clsparseScoomv(const clsparseScalar* alpha, const clsparseCooMatrix* matx,
                const cldenseVector* x, const clsparseScalar* beta,

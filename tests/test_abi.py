@@ -107,8 +107,6 @@ def test_solver_control_lifecycle(libso):
 def test_out_of_path_entries_not_implemented(libso):
     from clsparse_b200 import _lib as L
     libso.clsparseSetup()
-    m = L.clsparseCooMatrix()
-    assert libso.clsparseScoomv(None, C.byref(m), None, None, None, None) == L.clsparseNotImplemented
     assert libso.clsparseScsrSpGemm(None, None, None, None) == L.clsparseNotImplemented
     assert libso.clsparseHeaderfromFile(None, None, None, b"x.mtx") == L.clsparseInvalidValue
 
