@@ -35,8 +35,23 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Resident CTAs per SM the register allocator is held to: the gathers of x
+// are latency-bound, so more CTAs in flight pay (measured on the irregular,
+// 3D and 2D workloads); FP32 accumulators need fewer registers than FP64.
+// CLSP_SPMV_MIN_BLOCKS overrides it at build time (1 leaves it free).
+// The fused-dot variants the solvers launch (K > 0) keep more registers;
+// the compensated (extended-precision) ones are left free.
+template <typename T, bool EXT, int K, int NT>
+constexpr int spmv_min_blocks() {
+#ifdef CLSP_SPMV_MIN_BLOCKS
+    return CLSP_SPMV_MIN_BLOCKS * NT <= 2048 ? CLSP_SPMV_MIN_BLOCKS : 1;
+#else
+    return EXT ? 1 : (K == 0 ? 12 : (sizeof(T) == 8 ? 10 : 12)) * 128 / NT;
+#endif
+}
+
 template <typename V, typename T, bool EXT, int K, int NT, int BLK>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, spmv_min_blocks<T, EXT, K, NT>())
     csr_adaptive_kernel(const V* __restrict__ vals, const uint32_t* __restrict__ cols,
                         const uint32_t* __restrict__ rp, const T* __restrict__ x, T* __restrict__ y,
                         const T* __restrict__ alpha_p, const T* __restrict__ beta_p,
