@@ -148,6 +148,35 @@ def _timed(fn, reps=2):
     return t, r
 
 
+# Inner tolerance of the refinement: each inner solve (continued across
+# refinements) reduces its residual by this factor before the FP64 residual
+# is recomputed and replaced.
+INNER_TOL = 0.3
+
+
+def cg_profile(iters: int):
+    """A short FP64 Jacobi-CG on the C5 matrix with the solver loop in host
+    chunks (loop mode 1), so every kernel of an iteration is an ordinary
+    stream launch a profiler lists (graph nodes of the default loop are not)."""
+    import torch
+    from clsparse_b200 import _lib as L
+    from clsparse_b200 import api, matgen
+    api.setup()
+    ctrl = api.Control()
+    ctrl.set_solver_loop_mode(1)
+    A = api.CsrMatrix.from_numpy(*matgen.diffusion2d_grf(1024, corr_len=0.05, sigma=2.0, seed=1005))
+    A.create_meta(ctrl)
+    n = A.num_rows
+    b = torch.tensor(np.random.default_rng(1).uniform(-1, 1, n), device="cuda")
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    sc = api.SolverControl(L.DIAGONAL, iters, 0.0, 0.0)
+    sc.set_norm(2)
+    info = api.solve("cg", x, A, b, sc, ctrl)
+    sc.release()
+    print(json.dumps({"cg_profile_iterations": info["nIters"]}), flush=True)
+    ctrl.release()
+
+
 def cg_section(ctrl, with_cpu: bool):
     """Time-to-solution of the solver configurations the headline metric names.
 
@@ -223,7 +252,7 @@ def cg_section(ctrl, with_cpu: bool):
     def mixed():
         x.zero_()
         sc = api.SolverControl(L.DIAGONAL, 200000, 1e-10, 0.0)
-        r = api.cg_mixed(x, A, b, sc, ctrl, inner="fp32", inner_tol=0.1)
+        r = api.cg_mixed(x, A, b, sc, ctrl, inner="fp32", inner_tol=INNER_TOL)
         sc.release()
         return r
     tm, im = _timed(mixed)
@@ -274,7 +303,7 @@ def cg_section(ctrl, with_cpu: bool):
     def mixed5():
         x.zero_()
         sc = api.SolverControl(L.DIAGONAL, 200000, 1e-10, 0.0)
-        r = api.cg_mixed(x, A, b, sc, ctrl, inner="fp32", inner_tol=0.1)
+        r = api.cg_mixed(x, A, b, sc, ctrl, inner="fp32", inner_tol=INNER_TOL)
         sc.release()
         return r
     tm, im = _timed(mixed5)
@@ -288,7 +317,7 @@ def cg_section(ctrl, with_cpu: bool):
     def learned():
         x.zero_()
         sc = api.SolverControl(L.DIAGONAL, 200000, 1e-10, 0.0)
-        r = api.cg_learned(x, A, b, sc, spai, ctrl, inner="fp32", inner_tol=0.1)
+        r = api.cg_learned(x, A, b, sc, spai, ctrl, inner="fp32", inner_tol=INNER_TOL)
         sc.release()
         return r
     tl, il = _timed(learned)
@@ -480,8 +509,14 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cg", action="store_true", help="skip the CG time-to-solution section")
+    ap.add_argument("--cg-profile", type=int, default=0, metavar="ITERS",
+                    help="only run ITERS iterations of FP64 Jacobi-CG on the C5 matrix with directly launched "
+                         "kernels (for a profiler's launch list), then exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.cg_profile:
+        cg_profile(args.cg_profile)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -254,5 +254,66 @@ __device__ __forceinline__ bool grid_reduce_last(const U (&v)[K], U* partials, u
     return true;
 }
 
+// Two-level form of grid_reduce_last for launches of many CTAs (the SpMV
+// epilogue runs one CTA per row-block word, tens of thousands): the CTAs are
+// split into at most kTreeGroups contiguous groups with a counter each; the
+// last CTA of a group adds the group's partials in CTA order and arrives at
+// the top counter; the last group adds the group sums in order. Arrivals on
+// any one counter drop from the grid size to a group's size, and the result
+// is still independent of timing.
+// tickets: 1 + kTreeGroups zeroed counters (left at zero); partials:
+// K * (gridDim.x + kTreeGroups) slots.
+constexpr uint32_t kTreeGroups = 256;
+
+template <int K, typename U = double>
+__device__ __forceinline__ bool grid_reduce_tree(const U (&v)[K], U* partials, uint32_t* tickets, U (&out)[K]) {
+    __shared__ U red[32];
+    __shared__ int stage;
+    U tot[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) tot[k] = block_sum(v[k], red);
+    const uint32_t G = gridDim.x;
+    const uint32_t gs = (G + kTreeGroups - 1) / kTreeGroups;  // CTAs per group
+    const uint32_t ngroups = (G + gs - 1) / gs;
+    const uint32_t g = blockIdx.x / gs;
+    const uint32_t g0 = g * gs, g1 = min(G, g0 + gs);
+    U* gpart = partials + static_cast<size_t>(K) * G;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) partials[(size_t)k * G + blockIdx.x] = tot[k];
+        __threadfence();
+        const uint32_t t = atomicAdd(tickets + 1 + g, 1u);
+        stage = (t == g1 - g0 - 1) ? 1 : 0;
+    }
+    __syncthreads();
+    if (stage == 0) return false;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        U a = U(0);
+        for (uint32_t i = g0 + threadIdx.x; i < g1; i += blockDim.x) a += __ldcg(partials + (size_t)k * G + i);
+        tot[k] = block_sum(a, red);
+    }
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) gpart[(size_t)k * kTreeGroups + g] = tot[k];
+        tickets[1 + g] = 0u;
+        __threadfence();
+        const uint32_t t = atomicAdd(tickets, 1u);
+        stage = (t == ngroups - 1) ? 2 : 0;
+    }
+    __syncthreads();
+    if (stage != 2) return false;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        U a = U(0);
+        for (uint32_t i = threadIdx.x; i < ngroups; i += blockDim.x) a += __ldcg(gpart + (size_t)k * kTreeGroups + i);
+        out[k] = block_sum(a, red);
+    }
+    if (threadIdx.x == 0) *tickets = 0u;
+    return true;
+}
+
 }  // namespace dev
 }  // namespace clsp

@@ -176,8 +176,8 @@ struct SpmvEpilogue {
     int ndots = 0;            // 0, 1 or 2
     const void* w0 = nullptr; // dot0 = sum y_i * w0_i
     bool dot1_self = false;   // dot1 = sum y_i * y_i
-    double* partials = nullptr;   // [ndots][num_ctas]
-    uint32_t* ticket = nullptr;
+    double* partials = nullptr;   // [ndots][num_ctas + 256] (two-level reduction)
+    uint32_t* ticket = nullptr;   // 257 zeroed counters
     EpiOp op = EpiOp::None;
     void* state = nullptr;    // solver state the finaliser updates
     unsigned long long cond = 0;  // graph conditional handle (0 = none)

@@ -36,6 +36,7 @@ namespace clsp {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr size_t kTicketBytes = 2048;  // reduction counters at the head of the solver's partials buffer
 
 uint32_t vec_grid(size_t n, int sms) {
     size_t ctas = (n + kThreads * 4 - 1) / (kThreads * 4);
@@ -678,9 +679,11 @@ clsparseStatus prepare_cache(clsparseControl c, SolverCache& cache, const Solver
                              size_t n, uint32_t spmv_ctas, bool& rebuild) {
     rebuild = !(cache.valid && cache.key == key);
     const size_t vec_bytes = ((n * sizeof(T) + 255) / 256) * 256;
-    const size_t parts_doubles = std::max<size_t>(3 * kMaxReduceCtas, 2 * static_cast<size_t>(spmv_ctas));
+    // [tickets: kTicketBytes][partials]: the SpMV epilogue's two-level
+    // reduction needs 2 x (CTAs + 256) partials and 257 counters
+    const size_t parts_doubles = std::max<size_t>(3 * kMaxReduceCtas, 2 * (static_cast<size_t>(spmv_ctas) + 256));
     if (cache.vecs.ensure(vec_bytes * nvec + 256) != cudaSuccess ||
-        cache.parts.ensure(parts_doubles * sizeof(double) + 256) != cudaSuccess ||
+        cache.parts.ensure(parts_doubles * sizeof(double) + kTicketBytes + 256) != cudaSuccess ||
         cache.state.ensure(sizeof(SolverState<T>) + 256) != cudaSuccess) {
         cudaGetLastError();
         cache.valid = false;
@@ -792,7 +795,7 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
     T* invD = reinterpret_cast<T*>(base + 3 * vb);
     a.invD = key.precond ? invD : nullptr;
     a.st = static_cast<SolverState<T>*>(cache.state.ptr);
-    a.parts = static_cast<double*>(cache.parts.ptr) + 1;
+    a.parts = reinterpret_cast<double*>(static_cast<char*>(cache.parts.ptr) + kTicketBytes);
     a.ticket = static_cast<uint32_t*>(cache.parts.ptr);
     a.n = n;
     a.cond = 0;
@@ -903,7 +906,7 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
     a.Ms = pre ? vec(9) : a.s;
     a.invD = pre ? invD : nullptr;
     a.st = static_cast<SolverState<T>*>(cache.state.ptr);
-    a.parts = static_cast<double*>(cache.parts.ptr) + 1;
+    a.parts = reinterpret_cast<double*>(static_cast<char*>(cache.parts.ptr) + kTicketBytes);
     a.ticket = static_cast<uint32_t*>(cache.parts.ptr);
     a.n = n;
     a.cond = 0;
@@ -1007,7 +1010,7 @@ clsparseStatus pcg_factor_solve(cldenseVector* xv, const clsparseCsrMatrix* A, c
     a.t = reinterpret_cast<T*>(base + 3 * vb);
     a.z = reinterpret_cast<T*>(base + 4 * vb);
     a.st = static_cast<SolverState<T>*>(cache.state.ptr);
-    a.parts = static_cast<double*>(cache.parts.ptr) + 1;
+    a.parts = reinterpret_cast<double*>(static_cast<char*>(cache.parts.ptr) + kTicketBytes);
     a.ticket = static_cast<uint32_t*>(cache.parts.ptr);
     a.n = n;
     a.cond = 0;
