@@ -38,6 +38,15 @@ namespace {
 constexpr int kThreads = 256;
 constexpr size_t kTicketBytes = 2048;  // reduction counters at the head of the solver's partials buffer
 
+// Jacobi extraction runs a warp per row: enough CTAs that each warp walks
+// only a few rows (the walk is a chain of dependent loads).
+uint32_t diag_grid(size_t n, int sms) {
+    size_t ctas = (n + (kThreads / 32) - 1) / (kThreads / 32);
+    const size_t cap = static_cast<size_t>(sms) * 64;
+    if (ctas > cap) ctas = cap;
+    return static_cast<uint32_t>(ctas ? ctas : 1);
+}
+
 uint32_t vec_grid(size_t n, int sms) {
     size_t ctas = (n + kThreads * 4 - 1) / (kThreads * 4);
     size_t cap = static_cast<size_t>(sms) * 8;
@@ -814,7 +823,7 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
         CgArgs<T> aa = a;
         aa.cond = h;
         if (aa.invD && !aa.warm)
-            extract_inv_diag_kernel<V, T><<<vg, kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
+            extract_inv_diag_kernel<V, T><<<diag_grid(n, c->sm_count), kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
                                                                   invD, st);
         if (!aa.warm) {
             SpmvEpilogue none;
@@ -923,7 +932,7 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
         BicgArgs<T> aa = a;
         aa.cond = h;
         if (aa.invD)
-            extract_inv_diag_kernel<V, T><<<vg, kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
+            extract_inv_diag_kernel<V, T><<<diag_grid(n, c->sm_count), kThreads, 0, s>>>(Av.rp, Av.cols, Av.vals, Av.nrows,
                                                                   invD, st);
         SpmvEpilogue none;
         launch_csrmv<V, T>(Av, &st->one, &st->zero, aa.x, aa.y, ext, none, s);
