@@ -336,6 +336,34 @@ def cg_section(ctrl, with_cpu: bool):
     return out
 
 
+def spmv_fp32(api, ctrl, stream, rp, col, val, steps, peak):
+    """The same irregular matrix with FP32 values and vectors
+    (clsparseScsrmv): per-launch CUDA-event time, GB/s over the FP32 byte
+    count 4*(nnz + nrows) + 4*(nnz + 2*nrows)."""
+    import torch
+    n = len(rp) - 1
+    nbytes = 4 * (len(col) + n) + 4 * (len(col) + 2 * n)
+    with torch.cuda.stream(stream):
+        A = api.CsrMatrix.from_numpy(rp, col, val, dtype=torch.float32)
+        A.create_meta(ctrl)
+        x = torch.tensor(np.random.default_rng(3).uniform(-1, 1, n), dtype=torch.float32, device="cuda")
+        y = torch.zeros(n, dtype=torch.float32, device="cuda")
+        one = torch.ones(1, dtype=torch.float32, device="cuda")
+        zero = torch.zeros(1, dtype=torch.float32, device="cuda")
+        for _ in range(5):
+            api.csrmv(one, A, x, zero, y, ctrl)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for s, e in ev:
+            s.record(stream)
+            api.csrmv(one, A, x, zero, y, ctrl)
+            e.record(stream)
+        torch.cuda.synchronize()
+    ms = float(np.mean([s.elapsed_time(e) for s, e in ev]))
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    return {"value": round(gbs, 2), "unit": "GB/s", "us_per_launch": round(1e3 * ms, 2), "bytes_per_step": nbytes,
+            "roofline_frac": round(gbs / peak, 4), "kernel": "csr_adaptive_kernel<float,false,0>"}
+
+
 def make_matrix():
     from clsparse_b200 import matgen
     return matgen.irregular(2_000_000, mu=2.5, sigma=1.2, n_dense=50, dense_len=200_000, seed=7)
@@ -490,6 +518,8 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks,
         "gflops": round(2 * nnz * args.steps / (total_ms * 1e-3) / 1e9, 2),
     }
+    if world == 1:
+        line["fp32"] = spmv_fp32(api, ctrl, stream, rp, col, val, args.steps, peak)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(rp, col, val)
     if world == 1 and not args.no_cg:
