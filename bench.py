@@ -177,6 +177,31 @@ def cg_profile(iters: int):
     ctrl.release()
 
 
+def gnn_profile(builds: int):
+    """BF16 factor builds of the learned preconditioner on the C5 matrix
+    (1,048,576 rows): the network's forward pass with its dense layers on the
+    tcgen05 tensor cores (linear_fwd_umma), then the factor export. Prints the
+    median build time; for profiler launch lists and captures."""
+    import torch
+    from clsparse_b200 import api, matgen
+    api.setup()
+    ctrl = api.Control()
+    A = api.CsrMatrix.from_numpy(*matgen.diffusion2d_grf(1024, corr_len=0.05, sigma=2.0, seed=1005))
+    spai = api.Spai(3)
+    spai.set_matrix(A, ctrl)
+    ts = []
+    for _ in range(builds):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        spai.build(ctrl)
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    spai.release()
+    ctrl.release()
+    print(json.dumps({"gnn_profile_builds": builds, "median_build_ms": round(1e3 * float(np.median(ts)), 3)}),
+          flush=True)
+
+
 def cg_section(ctrl, with_cpu: bool):
     """Time-to-solution of the solver configurations the headline metric names.
 
@@ -539,11 +564,16 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cg", action="store_true", help="skip the CG time-to-solution section")
+    ap.add_argument("--gnn-profile", type=int, default=0, metavar="BUILDS",
+                    help="only run BUILDS learned-factor builds on the C5 matrix (profiling)")
     ap.add_argument("--cg-profile", type=int, default=0, metavar="ITERS",
                     help="only run ITERS iterations of FP64 Jacobi-CG on the C5 matrix with directly launched "
                          "kernels (for a profiler's launch list), then exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.gnn_profile:
+        gnn_profile(args.gnn_profile)
+        return
     if args.cg_profile:
         cg_profile(args.cg_profile)
         return

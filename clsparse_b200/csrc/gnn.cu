@@ -19,7 +19,10 @@
 //   g_hat_ij = w_o . relu(P h_i + Q h_j + a_hat_ij r + t) + b_o   (j < i, a_ij != 0)
 // Weights are kept in FP32 for the optimiser and used as BF16 in the
 // forward and backward passes (products accumulated in FP32); a debug switch
-// uses the FP32 copies instead (gradient checks).
+// uses the FP32 copies instead (gradient checks). In the BF16 forward pass the
+// dense layers U_l, V_l, P and Q run on the tcgen05 tensor cores
+// (linear_fwd_umma: BF16 operands in shared memory, FP32 accumulator in
+// tensor memory).
 //
 // Loss: the Kaporin condition-number bound of G_hat A_hat G_hat^T,
 //   L_K = log(tr(G_hat A_hat G_hat^T) / n) - (2/n) sum_i log g_hat_ii,
@@ -36,6 +39,7 @@
 
 #include "device_common.cuh"
 #include "internal.h"
+#include "pipeline.cuh"
 
 namespace clsp {
 namespace gnn {
@@ -121,77 +125,186 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// Tensor-core form of linear_fwd for the BF16 forward pass (weights and
-// input activations rounded to BF16, FP32 accumulation): warp-level
-// mma.sync m16n8k16 BF16 tiles. A persistent CTA (4 warps) stages the M x K
-// weight tile once, then walks 64-row tiles of X: each warp multiplies 16
-// rows by all M outputs; bias, ReLU and the residual are applied in the
-// epilogue. K must be a multiple of 16, M of 8.
+// ---- tcgen05 tensor-core form of the dense layers (BF16 inference) ----
+//
+// Y[n x M] = act(X W^T + b) (+ R) with X = [X1 | X2] and W rounded to BF16 and
+// FP32 accumulation, on the sm_100 tensor cores: one 128 x M x 16 UMMA
+// (tcgen05.mma, kind::f16) per 16 columns of K, issued by one thread, the
+// 128 x M FP32 accumulator in tensor memory. A persistent CTA of 4 warps
+// stages the weights once, then per 128-row tile of X: stages the tile as
+// BF16 in shared memory, issues the MMAs, waits on their commit barrier, and
+// each warp reads its 32 accumulator rows (TMEM lanes) for the epilogue (bias,
+// ReLU, residual). Operands are K-major without swizzle: core matrices of
+// 8 rows x 16 bytes, stored contiguously, the 8-row groups K*16 bytes apart
+// (SBO) and the two K-halves of one MMA 128 bytes apart (LBO).
+namespace umma {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor (no swizzle, descriptor version 1).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
+           (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: D FP32, A and B BF16, both K-major.
+template <int TM, int TN>
+__host__ __device__ constexpr uint32_t idesc_bf16() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(TN >> 3) << 17) |
+           (static_cast<uint32_t>(TM >> 4) << 24);
+}
+
+// Element offset of (row, k) in the K-major core-matrix layout of a BF16
+// operand with K columns.
+template <int K>
+__device__ __forceinline__ int core_off(int row, int k) {
+    return (row >> 3) * (K * 8) + (k >> 3) * 64 + (row & 7) * 8 + (k & 7);
+}
+
+template <int M, int K>
+__host__ __device__ constexpr size_t smem_bytes() {
+    return static_cast<size_t>(128 * K + M * K) * 2 + M * 4 + 16;
+}
+
+}  // namespace umma
+
+__device__ int g_umma_error;  // set when a commit-barrier wait ran out
+
 template <int M, int K1, int K2>
 __global__ void __launch_bounds__(128)
-    linear_fwd_tc(const float* __restrict__ X1, const float* __restrict__ X2, const float* __restrict__ W,
-                  const float* __restrict__ b, const float* __restrict__ R, float* __restrict__ Y,
-                  float* __restrict__ A, size_t n, int act) {
+    linear_fwd_umma(const float* __restrict__ X1, const float* __restrict__ X2, const float* __restrict__ W,
+                    const float* __restrict__ b, const float* __restrict__ R, float* __restrict__ Y,
+                    float* __restrict__ A, size_t n, int act) {
     constexpr int K = K1 + K2;
-    constexpr int KP = K + 8;  // padded row length (bf16): fragment loads hit distinct banks
-    constexpr int TR = 64;     // rows per tile
-    static_assert(K % 16 == 0 && M % 8 == 0, "tile shape");
-    __shared__ __align__(16) __nv_bfloat16 sw[M * KP];
-    __shared__ __align__(16) __nv_bfloat16 sx[TR * KP];
-    __shared__ float sb[M];
-    for (int i = threadIdx.x; i < M * K; i += 128) sw[(i / K) * KP + (i % K)] = __float2bfloat16_rn(W[i]);
-    for (int i = threadIdx.x; i < M; i += 128) sb[i] = b ? b[i] : 0.f;
+    constexpr int TR = 128;                            // rows per tile = UMMA M
+    constexpr uint32_t kCols = M < 32 ? 32 : M;        // TMEM columns: a power of two >= 32
+    static_assert(K % 16 == 0 && M % 16 == 0 && M >= 16 && M <= 256 && (M & (M - 1)) == 0, "UMMA shape");
+    extern __shared__ __align__(1024) unsigned char dsm[];
+    __nv_bfloat16* sa = reinterpret_cast<__nv_bfloat16*>(dsm);  // TR x K
+    __nv_bfloat16* sw = sa + TR * K;                             // M x K
+    float* sbias = reinterpret_cast<float*>(sw + M * K);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sbias + M);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int g = lane >> 2, t4 = lane & 3;
-    const int rw = warp * 16;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         umma::smem_u32(tmem_slot)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        pipe::mbar_init(bar, 1);
+        pipe::fence_barrier_init();
+    }
+    for (int i = threadIdx.x; i < M * K; i += TR) sw[umma::core_off<K>(i / K, i % K)] = __float2bfloat16_rn(W[i]);
+    static_assert(K1 % 8 == 0 && K2 % 8 == 0, "a core-matrix row never straddles X1 and X2");
+    constexpr int C = K / 8;  // 16-byte core-matrix rows per tile row
+    for (int i = threadIdx.x; i < M; i += TR) sbias[i] = b ? b[i] : 0.f;
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t sa_addr = umma::smem_u32(sa), sw_addr = umma::smem_u32(sw);
+    constexpr uint32_t idesc = umma::idesc_bf16<TR, M>();
     const size_t ntiles = (n + TR - 1) / TR;
+    uint32_t phase = 0;
+    bool issued = false;  // an MMA commit may still be pending on the barrier
     for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const size_t r0 = tile * TR;
-        __syncthreads();  // weights staged; the previous tile's fragments read
-        for (int i = threadIdx.x; i < TR * K; i += 128) {
-            const int rr = i / K, kk = i % K;
+        // one 16-byte core-matrix row (8 columns) per thread and pass; eight
+        // consecutive threads fill the 8 rows of one core matrix (128
+        // contiguous bytes, no bank conflict)
+        for (int idx = threadIdx.x; idx < TR * C; idx += TR) {
+            const int chunk = (idx >> 3) % C;
+            const int rr = (idx & 7) + 8 * ((idx >> 3) / C);
             const size_t row = r0 + rr;
-            float v = 0.f;
-            if (row < n) v = kk < K1 ? X1[row * K1 + kk] : X2[row * K2 + (kk - K1)];
-            sx[rr * KP + kk] = __float2bfloat16_rn(v);
-        }
-        __syncthreads();
-        float acc[M / 8][4];
-#pragma unroll
-        for (int t = 0; t < M / 8; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
-#pragma unroll
-        for (int k0 = 0; k0 < K; k0 += 16) {
-            const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&sx[(rw + g) * KP + k0 + 2 * t4]);
-            const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&sx[(rw + g + 8) * KP + k0 + 2 * t4]);
-            const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&sx[(rw + g) * KP + k0 + 8 + 2 * t4]);
-            const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&sx[(rw + g + 8) * KP + k0 + 8 + 2 * t4]);
-#pragma unroll
-            for (int t = 0; t < M / 8; ++t) {
-                const int col = t * 8 + g;
-                const uint32_t b0 = *reinterpret_cast<const uint32_t*>(&sw[col * KP + k0 + 2 * t4]);
-                const uint32_t b1 = *reinterpret_cast<const uint32_t*>(&sw[col * KP + k0 + 8 + 2 * t4]);
-                asm volatile(
-                    "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-                    "{%8,%9}, {%0,%1,%2,%3};"
-                    : "+f"(acc[t][0]), "+f"(acc[t][1]), "+f"(acc[t][2]), "+f"(acc[t][3])
-                    : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+            const int k0 = chunk * 8;
+            float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
+            if (row < n) {
+                const float* src = k0 < K1 ? X1 + row * K1 + k0 : X2 + row * K2 + (k0 - K1);
+                lo = *reinterpret_cast<const float4*>(src);
+                hi = *reinterpret_cast<const float4*>(src + 4);
             }
+            __nv_bfloat162 q[4] = {__floats2bfloat162_rn(lo.x, lo.y), __floats2bfloat162_rn(lo.z, lo.w),
+                                   __floats2bfloat162_rn(hi.x, hi.y), __floats2bfloat162_rn(hi.z, hi.w)};
+            *reinterpret_cast<uint4*>(sa + (rr >> 3) * (K * 8) + chunk * 64 + (rr & 7) * 8) =
+                *reinterpret_cast<const uint4*>(q);
         }
+        // the generic-proxy stores must be visible to the tensor core's reads
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-        for (int t = 0; t < M / 8; ++t)
+            for (int s = 0; s < K / 16; ++s) {
+                const uint64_t ad = umma::smem_desc(sa_addr + s * 256, 128, K * 16);
+                const uint64_t bd = umma::smem_desc(sw_addr + s * 256, 128, K * 16);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(s)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             umma::smem_u32(bar))
+                         : "memory");
+        }
+        issued = true;
+        const bool waited = pipe::mbar_wait(bar, phase, nullptr);
+        if (__syncthreads_or(!waited)) {  // the whole CTA leaves together
+            if (threadIdx.x == 0) atomicExch(&g_umma_error, 1);
+            break;
+        }
+        issued = false;
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const size_t row = r0 + warp * 32 + lane;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const size_t row = r0 + rw + g + 8 * h;
-                if (row >= n) continue;
+        for (int c0 = 0; c0 < M; c0 += 16) {
+            uint32_t v[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                  "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                  "=r"(v[14]), "=r"(v[15])
+                : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < n) {
 #pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    const int m = t * 8 + 2 * t4 + j;
-                    const float z = acc[t][2 * h + j] + sb[m];
-                    const float a = act ? fmaxf(z, 0.f) : z;
-                    if (A) A[row * M + m] = a;
-                    Y[row * M + m] = R ? R[row * M + m] + a : a;
+                for (int q = 0; q < 4; ++q) {
+                    float a[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float z = __uint_as_float(v[4 * q + j]) + sbias[c0 + 4 * q + j];
+                        a[j] = act ? fmaxf(z, 0.f) : z;
+                    }
+                    const size_t off = row * M + c0 + 4 * q;
+                    const float4 av = make_float4(a[0], a[1], a[2], a[3]);
+                    if (A) *reinterpret_cast<float4*>(A + off) = av;
+                    float4 yv = av;
+                    if (R) {
+                        const float4 rv = *reinterpret_cast<const float4*>(R + off);
+                        yv = make_float4(rv.x + av.x, rv.y + av.y, rv.z + av.z, rv.w + av.w);
+                    }
+                    *reinterpret_cast<float4*>(Y + off) = yv;
                 }
             }
+        }
+        // accumulator read and shared operand consumed before the next tile
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+    }
+    if (issued && threadIdx.x == 0) pipe::mbar_wait(bar, phase, nullptr);  // let a late commit land
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
     }
 }
 
@@ -852,6 +965,37 @@ clsparseStatus build_graph(_clsparseB200Spai* net, const clsparseCsrMatrix* A, c
     return clsparseSuccess;
 }
 
+// Launches the tcgen05 dense layer: a persistent grid of up to four CTAs per
+// SM (shared memory and TMEM columns allow four), one 128-row tile at a time.
+template <int M, int K1, int K2>
+void launch_umma(const float* X1, const float* X2, const float* W, const float* b, const float* R, float* Y,
+                 float* A, size_t n, int act, int device, cudaStream_t s) {
+    constexpr size_t bytes = umma::smem_bytes<M, K1 + K2>();
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(linear_fwd_umma<M, K1, K2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(bytes));
+        configured = true;
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const size_t tiles = (n + 127) / 128;
+    const uint32_t grid = static_cast<uint32_t>(std::max<size_t>(1, std::min<size_t>(tiles, size_t(sms) * 4)));
+    linear_fwd_umma<M, K1, K2><<<grid, 128, bytes, s>>>(X1, X2, W, b, R, Y, A, n, act);
+}
+
+// Whether a tcgen05 layer's commit wait ran out since the last check (clears
+// the flag).
+bool umma_failed() {
+    int h = 0;
+    cudaMemcpyFromSymbol(&h, g_umma_error, sizeof(int));
+    if (h) {
+        const int zero = 0;
+        cudaMemcpyToSymbol(g_umma_error, &zero, sizeof(int));
+    }
+    return h != 0;
+}
+
 void forward(_clsparseB200Spai* net, int bf16, cudaStream_t s) {
     Graph& gr = net->gr;
     const Offsets& o = net->o;
@@ -860,30 +1004,27 @@ void forward(_clsparseB200Spai* net, int bf16, cudaStream_t s) {
     const uint32_t tiles = nblk(n, kRows);
     linear_fwd<H, NF, 0><<<tiles, 256, 0, s>>>(gr.F, nullptr, P + o.w_in, P + o.b_in, nullptr, gr.Hs[0],
                                                 nullptr, n, 1, bf16);
-    // BF16 forward: the dense layers on tensor cores; FP32 weights (gradient
-    // checks): CUDA-core FMAs.
-    const uint32_t tc_grid = static_cast<uint32_t>(std::min<size_t>((n + 63) / 64, 1184));
+    // BF16 forward: the dense layers on the tcgen05 tensor cores; FP32 weights
+    // (gradient checks): CUDA-core FMAs.
+    const int dev = net->device;
     for (int l = 0; l < NL; ++l) {
         if (bf16)
-            linear_fwd_tc<H, H, 0><<<tc_grid, 128, 0, s>>>(gr.Hs[l], nullptr, P + o.U[l], nullptr, nullptr,
-                                                           gr.Hu[l], nullptr, n, 0);
+            launch_umma<H, H, 0>(gr.Hs[l], nullptr, P + o.U[l], nullptr, nullptr, gr.Hu[l], nullptr, n, 0, dev, s);
         else
             linear_fwd<H, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[l], nullptr, P + o.U[l], nullptr, nullptr, gr.Hu[l],
                                                       nullptr, n, 0, bf16);
         message_fwd<<<warps_grid(n), 256, 0, s>>>(gr.rp, gr.cols, gr.ehat, gr.Hu[l], P + o.w[l], P + o.c[l],
                                                   gr.S[l], gr.n, bf16);
         if (bf16)
-            linear_fwd_tc<H, H, H><<<tc_grid, 128, 0, s>>>(gr.Hs[l], gr.S[l], P + o.V[l], P + o.d[l], gr.Hs[l],
-                                                           gr.Hs[l + 1], gr.Au[l], n, 1);
+            launch_umma<H, H, H>(gr.Hs[l], gr.S[l], P + o.V[l], P + o.d[l], gr.Hs[l], gr.Hs[l + 1], gr.Au[l], n, 1,
+                                 dev, s);
         else
             linear_fwd<H, H, H><<<tiles, 256, 0, s>>>(gr.Hs[l], gr.S[l], P + o.V[l], P + o.d[l], gr.Hs[l],
                                                       gr.Hs[l + 1], gr.Au[l], n, 1, bf16);
     }
     if (bf16) {
-        linear_fwd_tc<HO, H, 0><<<tc_grid, 128, 0, s>>>(gr.Hs[NL], nullptr, P + o.P, nullptr, nullptr, gr.Hp,
-                                                        nullptr, n, 0);
-        linear_fwd_tc<HO, H, 0><<<tc_grid, 128, 0, s>>>(gr.Hs[NL], nullptr, P + o.Q, nullptr, nullptr, gr.Hq,
-                                                        nullptr, n, 0);
+        launch_umma<HO, H, 0>(gr.Hs[NL], nullptr, P + o.P, nullptr, nullptr, gr.Hp, nullptr, n, 0, dev, s);
+        launch_umma<HO, H, 0>(gr.Hs[NL], nullptr, P + o.Q, nullptr, nullptr, gr.Hq, nullptr, n, 0, dev, s);
     } else {
         linear_fwd<HO, H, 0><<<tiles, 256, 0, s>>>(gr.Hs[NL], nullptr, P + o.P, nullptr, nullptr, gr.Hp,
                                                    nullptr, n, 0, bf16);
@@ -1081,8 +1222,9 @@ clsparseStatus clsparseB200SpaiLossGrad(clsparseB200Spai net, const cldenseVecto
         if (capacity < size_t(net->o.total)) return clsparseInsufficientMemory;
         cudaMemcpyAsync(grad, net->grad, size_t(net->o.total) * 4, cudaMemcpyDeviceToHost, control->stream);
     }
-    return cudaStreamSynchronize(control->stream) == cudaSuccess ? clsparseSuccess
-                                                                 : clsparseInvalidKernelExecution;
+    if (cudaStreamSynchronize(control->stream) != cudaSuccess || umma_failed())
+        return clsparseInvalidKernelExecution;
+    return clsparseSuccess;
 }
 
 clsparseStatus clsparseB200SpaiTrainStep(clsparseB200Spai net, const cldenseVector* probes, cl_int K,
@@ -1106,6 +1248,8 @@ clsparseStatus clsparseB200SpaiBuild(clsparseB200Spai net, clsparseControl contr
     DeviceGuard g(control->device);
     forward(net, 1, control->stream);
     export_g(net, control->stream);
+    if (cudaStreamSynchronize(control->stream) != cudaSuccess || umma_failed())
+        return clsparseInvalidKernelExecution;
     return finish_call(control);
 }
 

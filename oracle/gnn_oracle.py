@@ -69,7 +69,7 @@ class Graph:
     """Scaled operator, tril pattern, local loss blocks and node features of an
     SPD CSR matrix (sorted columns)."""
 
-    def __init__(self, rp, col, val):
+    def __init__(self, rp, col, val, with_blocks=True):
         rp = np.asarray(rp, dtype=np.int64)
         col = np.asarray(col, dtype=np.int64)
         val = np.asarray(val, dtype=np.float64)
@@ -92,9 +92,9 @@ class Graph:
         absum = np.bincount(rows[self.offdiag], weights=np.abs(self.ehat[self.offdiag]), minlength=n)
         deg = np.bincount(rows[self.offdiag], minlength=n)
         self.F = np.stack([np.ones(n), absum, deg / 8.0, np.zeros(n)], axis=1)
-        Ad = self.Ahat.toarray() if n <= 4000 else None
-        self.blocks = []
-        for i in range(n):
+        Ad = self.Ahat.toarray() if n <= 4000 and with_blocks else None
+        self.blocks = []  # loss blocks; not needed for the forward pass alone
+        for i in range(n if with_blocks else 0):
             P = self.Lcol[self.Lrp[i]:self.Lrp[i + 1]]
             if Ad is not None:
                 self.blocks.append(Ad[np.ix_(P, P)])
@@ -118,26 +118,41 @@ def sigmoid(z):
     return 1.0 / (1.0 + np.exp(-z))
 
 
-def forward(p, gr: Graph):
+def bf16_round(x):
+    """Round to the nearest BF16 value (ties to even) through FP32, as
+    __float2bfloat16_rn does; returned as float64."""
+    u = np.ascontiguousarray(np.asarray(x, dtype=np.float32)).view(np.uint32)
+    u = (u + (((u >> 16) & 1) + 0x7FFF)) & 0xFFFF0000
+    return u.view(np.float32).astype(np.float64)
+
+
+def forward(p, gr: Graph, bf16=False):
+    """The network's forward pass. bf16=True restates the library's BF16
+    inference: every weight is rounded to BF16, and the four dense layers that
+    run on tensor cores (U, V, P, Q) also round their inputs (FP32 activations)
+    to BF16; accumulation stays wide."""
     W = unpack(p)
+    if bf16:
+        W = {k: bf16_round(v) for k, v in W.items()}
+    rx = bf16_round if bf16 else (lambda v: v)
     c = {}
     h = relu(gr.F @ W["w_in"].T + W["b_in"])
     c["H0"] = h
     Hs = [h]
     for l in range(NL):
-        hu = h @ W[f"U{l}"].T
+        hu = rx(h) @ W[f"U{l}"].T
         pre = hu[gr.cols] + gr.ehat[:, None] * W[f"w{l}"] + W[f"c{l}"]
         msg = relu(pre) * gr.offdiag[:, None]
         s = np.zeros_like(h)
         np.add.at(s, gr.rows, msg)
-        z = np.concatenate([h, s], axis=1) @ W[f"V{l}"].T + W[f"d{l}"]
+        z = rx(np.concatenate([h, s], axis=1)) @ W[f"V{l}"].T + W[f"d{l}"]
         a = relu(z)
         c[f"Hu{l}"], c[f"pre{l}"], c[f"S{l}"], c[f"Z{l}"] = hu, pre, s, z
         h = h + a
         Hs.append(h)
     c["Hs"] = Hs
-    hp = h @ W["P"].T
-    hq = h @ W["Q"].T
+    hp = rx(h) @ W["P"].T
+    hq = rx(h) @ W["Q"].T
     pre_o = hp[gr.Lrow] + hq[gr.Lcol] + gr.Le[:, None] * W["r"] + W["t"]
     z_d = h @ W["w_d"] + W["b_d"][0]
     g = np.where(gr.isdiag, softplus(z_d[gr.Lrow]), relu(pre_o) @ W["w_o"] + W["b_o"][0])

@@ -52,3 +52,15 @@ def test_kaporin_loss_is_lowest_at_fsai(small_graph):
     for _ in range(5):
         L1, _ = go.loss_and_dg(g + 1e-3 * rng.normal(size=g.size), gr)
         assert L1 > L0
+
+
+def test_bf16_round_matches_torch():
+    """The oracle's BF16 rounding (ties to even through FP32) against torch's
+    float32 -> bfloat16 conversion."""
+    import torch
+    rng = np.random.default_rng(3)
+    x = np.concatenate([rng.normal(size=4000) * 10.0 ** rng.integers(-6, 6, 4000),
+                        [1.0, 1.0 + 2.0 ** -8, 1.0 + 3 * 2.0 ** -8, -1.0 - 2.0 ** -8, 0.0]]).astype(np.float32)
+    ref = torch.from_numpy(x).to(torch.bfloat16).to(torch.float64).numpy()
+    np.testing.assert_array_equal(go.bf16_round(x), ref)
+    assert go.bf16_round(np.float32(1.0 + 2.0 ** -8)) == 1.0  # tie to even

@@ -47,6 +47,32 @@ def test_bf16_weights_close_to_fp32(ctrl):
     spai.release()
 
 
+@pytest.mark.parametrize("m", [24, 300], ids=["576 rows", "90000 rows"])
+def test_bf16_forward_matches_oracle(ctrl, m):
+    """The BF16 inference pass (dense layers on tensor cores, BF16 weights and
+    layer inputs, FP32 accumulation) against the oracle's restatement of the
+    same roundings in FP64: the exported factor agrees to 2e-3 in norm (FP32
+    activations may round to a neighbouring BF16 value where the oracle's FP64
+    ones do not). 576 rows leave a partial 128-row tile; 90000 rows give
+    every CTA of the persistent grid several tiles."""
+    rp, c, v = matgen.diffusion2d_grf(m, corr_len=0.2, sigma=1.5, seed=8)
+    A = api.CsrMatrix.from_numpy(rp, c, v)
+    spai = api.Spai(11)
+    spai.set_matrix(A, ctrl)
+    spai.build(ctrl)
+    _, _, G = spai.factor()
+    gr = go.Graph(rp, c, v, with_blocks=False)
+    g = G / gr.dinv[gr.Lcol]  # the network's output on the scaled operator
+    p = spai.params().astype(np.float64)
+    g16, _ = go.forward(p, gr, bf16=True)
+    g64, _ = go.forward(p, gr, bf16=False)
+    rel = np.linalg.norm(g - g16) / np.linalg.norm(g16)
+    assert rel <= 2e-3, rel
+    # the BF16 roundings themselves are visible: the test can tell the modes apart
+    assert np.linalg.norm(g64 - g16) / np.linalg.norm(g16) > 5 * rel
+    spai.release()
+
+
 def test_factor_pattern_and_positive_diagonal(ctrl):
     (rp, c, v), A, spai = _setup(ctrl)
     spai.build(ctrl)
