@@ -965,31 +965,24 @@ clsparseStatus build_graph(_clsparseB200Spai* net, const clsparseCsrMatrix* A, c
     return clsparseSuccess;
 }
 
-// Launches the tcgen05 dense layer: a persistent grid of up to four CTAs per
-// SM (fewer where shared memory allows fewer), one 128-row tile at a time.
-// Measured on the 1024^2 factor build: 4.55 ms at four per SM, 5.9 ms with
-// the 8-10 that shared memory and TMEM would allow on the 64-column layers.
+// Launches the tcgen05 dense layer: a persistent grid of four CTAs per SM
+// (shared memory and TMEM columns allow four on every layer), one 128-row
+// tile at a time.
 template <int M, int K1, int K2>
 void launch_umma(const float* X1, const float* X2, const float* W, const float* b, const float* R, float* Y,
                  float* A, size_t n, int act, int device, cudaStream_t s) {
     constexpr size_t bytes = umma::smem_bytes<M, K1 + K2>();
-    constexpr int kTmemCtas = 512 / (M < 32 ? 32 : M);
-    static int per_sm = 0;
-    if (per_sm == 0) {
+    static_assert(4 * (M < 32 ? 32 : M) <= 512 && 4 * bytes <= 227 * 1024, "four CTAs per SM");
+    static bool configured = false;
+    if (!configured) {
         cudaFuncSetAttribute(linear_fwd_umma<M, K1, K2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(bytes));
-        int occ = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, linear_fwd_umma<M, K1, K2>, 128, bytes) !=
-                cudaSuccess ||
-            occ < 1)
-            occ = 1;
-        per_sm = std::min(std::min(occ, kTmemCtas), 4);
+        configured = true;
     }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const size_t tiles = (n + 127) / 128;
-    const uint32_t grid =
-        static_cast<uint32_t>(std::max<size_t>(1, std::min<size_t>(tiles, size_t(sms) * per_sm)));
+    const uint32_t grid = static_cast<uint32_t>(std::max<size_t>(1, std::min<size_t>(tiles, size_t(sms) * 4)));
     linear_fwd_umma<M, K1, K2><<<grid, 128, bytes, s>>>(X1, X2, W, b, R, Y, A, n, act);
 }
 
