@@ -91,6 +91,19 @@ __device__ __forceinline__ T ld_val(const V* p) {
     }
 }
 
+// The same through the read-only (L1-allocating) path, for access patterns in
+// which neighbouring threads read the same lines in different iterations
+// (one thread per row).
+template <typename T, typename V>
+__device__ __forceinline__ T ld_val_ro(const V* p) {
+    if constexpr (std::is_same_v<V, __nv_bfloat16>) {
+        const unsigned short u = __ldg(reinterpret_cast<const unsigned short*>(p));
+        return static_cast<T>(__uint_as_float(static_cast<unsigned>(u) << 16));
+    } else {
+        return static_cast<T>(__ldg(p));
+    }
+}
+
 // Converts a matrix value held in registers or shared memory to T.
 template <typename T, typename V>
 __device__ __forceinline__ T to_t(V v) {

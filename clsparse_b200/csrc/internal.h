@@ -102,6 +102,7 @@ struct matrix_meta {
     clsparseIdx_t num_nonzeros = 0;
     uint32_t nnz_lo = 0;                // row_pointer[0]
     uint32_t nnz_hi = 0;                // row_pointer[num_rows]
+    uint32_t max_row = 0;               // longest row (nonzeros)
     int device = 0;
     // Row-block shape the words were made with (the reference's constants by
     // default; clsparseB200CsrMetaCreateTuned sets others) and the CTA width

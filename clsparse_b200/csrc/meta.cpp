@@ -11,6 +11,7 @@
 //                 mutate the words)
 //   bits 23..0   chunk index inside a long row, or for a block of several short
 //                rows the number of threads the reference reduced each row with
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -266,6 +267,8 @@ clsparseStatus create_meta(clsparseCsrMatrix* csrMatx, clsparseControl control, 
     for (size_t k = 0; k < w; ++k) word_nnz[k] = rp[static_cast<size_t>(meta->h_rowBlocks[k] >> 32)];
     meta->nnz_lo = rp.front();
     meta->nnz_hi = rp.back();
+    for (size_t r = 0; r + 1 < rp.size(); ++r)
+        meta->max_row = std::max<uint32_t>(meta->max_row, static_cast<uint32_t>(rp[r + 1] - rp[r]));
     if (cudaMalloc(&meta->d_rowBlocks, w * sizeof(cl_ulong)) != cudaSuccess ||
         cudaMalloc(&meta->d_word_nnz, w * sizeof(uint32_t)) != cudaSuccess ||
         cudaMalloc(&meta->d_lr_partial, w * sizeof(double)) != cudaSuccess ||

@@ -88,6 +88,43 @@ def test_spmv_edge_matrices(ctrl, orc, dtype, meta, case):
         assert_parity(orc, rp, col, val, x, y0, alpha, beta, out, dtype)
 
 
+SHORT_ROW_CASES = {
+    "poisson": None,
+    "lengths_0_to_16": list(np.random.default_rng(7).integers(0, 17, 30_000)),
+    "sixteen_then_seventeen": [16] * 3000 + [17] + [4] * 3000,  # longest row 17: row-block kernel
+    "all_empty": [0] * 1000,
+}
+
+
+@pytest.mark.parametrize("ext", [False, True], ids=["plain", "extended"])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+@pytest.mark.parametrize("case", sorted(SHORT_ROW_CASES))
+def test_spmv_short_rows_both_kernels(ctrl, orc, monkeypatch, dtype, case, ext):
+    """Matrices whose rows are all at most 16 long run one thread per row; the
+    same products through the row-block kernel (CLSPARSE_B200_SHORT_ROWS=0) and
+    both against the oracle."""
+    if case == "poisson":
+        rp, col, val = matgen.poisson2d(96)
+        ncols = len(rp) - 1
+    else:
+        ncols = 20_000
+        rp, col, val = matgen.random_lengths(SHORT_ROW_CASES[case], ncols, seed=3)
+    n = len(rp) - 1
+    x, y0 = vecs(n, ncols, 8)
+    ctrl.enable_extended_precision(ext)
+    outs = []
+    for mode in ("1", "0"):
+        monkeypatch.setenv("CLSPARSE_B200_SHORT_ROWS", mode)
+        for alpha, beta in ((1.0, 0.0), (-0.75, 1.25)):
+            out, _ = gpu_spmv(ctrl, rp, col, val, x, y0, alpha, beta, dtype, meta=True, ncols=ncols)
+            assert_parity(orc, rp, col, val, x, y0, alpha, beta, out, dtype)
+            outs.append(out)
+    ctrl.enable_extended_precision(False)
+    if case == "sixteen_then_seventeen":  # both settings ran the row-block kernel
+        np.testing.assert_array_equal(outs[0], outs[2])
+        np.testing.assert_array_equal(outs[1], outs[3])
+
+
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
 def test_spmv_extended_precision(ctrl, orc, dtype):
     ctrl.enable_extended_precision(True)
