@@ -238,6 +238,17 @@ __device__ __forceinline__ Acc<T, EXT> block_reduce_acc(Acc<T, EXT> a, T* scratc
 // returns true with the totals in out[] (valid in every thread of that CTA).
 // It also resets the ticket to zero for the next launch. No CTA ever waits
 // for another, so there is nothing to deadlock.
+// Arrival on a reduction ticket: a release-acquire atomic add at GPU scope.
+// The release orders this thread's partial store before the arrival; the
+// acquire lets the last arriving CTA read every other CTA's partial (its other
+// threads see them after the CTA barrier that follows). Cheaper than a full
+// fence before a relaxed atomic.
+__device__ __forceinline__ uint32_t ticket_arrive(uint32_t* ticket) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(ticket) : "memory");
+    return old;
+}
+
 template <int K, typename U = double>
 __device__ __forceinline__ bool grid_reduce_last(const U (&v)[K], U* partials, uint32_t* ticket,
                                                  U (&out)[K]) {
@@ -250,13 +261,11 @@ __device__ __forceinline__ bool grid_reduce_last(const U (&v)[K], U* partials, u
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int k = 0; k < K; ++k) partials[(size_t)k * G + blockIdx.x] = tot[k];
-        __threadfence();
-        const uint32_t t = atomicAdd(ticket, 1u);
+        const uint32_t t = ticket_arrive(ticket);
         is_last = (t == G - 1);
     }
     __syncthreads();
     if (!is_last) return false;
-    __threadfence();
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         U a = U(0);
@@ -294,13 +303,11 @@ __device__ __forceinline__ bool grid_reduce_tree(const U (&v)[K], U* partials, u
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int k = 0; k < K; ++k) partials[(size_t)k * G + blockIdx.x] = tot[k];
-        __threadfence();
-        const uint32_t t = atomicAdd(tickets + 1 + g, 1u);
+        const uint32_t t = ticket_arrive(tickets + 1 + g);
         stage = (t == g1 - g0 - 1) ? 1 : 0;
     }
     __syncthreads();
     if (stage == 0) return false;
-    __threadfence();
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         U a = U(0);
@@ -311,13 +318,11 @@ __device__ __forceinline__ bool grid_reduce_tree(const U (&v)[K], U* partials, u
 #pragma unroll
         for (int k = 0; k < K; ++k) gpart[(size_t)k * kTreeGroups + g] = tot[k];
         tickets[1 + g] = 0u;
-        __threadfence();
-        const uint32_t t = atomicAdd(tickets, 1u);
+        const uint32_t t = ticket_arrive(tickets);
         stage = (t == ngroups - 1) ? 2 : 0;
     }
     __syncthreads();
     if (stage != 2) return false;
-    __threadfence();
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         U a = U(0);

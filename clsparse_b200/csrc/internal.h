@@ -104,6 +104,7 @@ struct matrix_meta {
     uint32_t nnz_hi = 0;                // row_pointer[num_rows]
     uint32_t max_row = 0;               // longest row (nonzeros)
     int device = 0;
+    int sm_count = 148;                 // SMs of the device the meta was made on
     // Row-block shape the words were made with (the reference's constants by
     // default; clsparseB200CsrMetaCreateTuned sets others) and the CTA width
     // of the adaptive kernel.

@@ -245,6 +245,7 @@ clsparseStatus create_meta(clsparseCsrMatrix* csrMatx, clsparseControl control, 
 
     auto meta = std::make_unique<matrix_meta>();
     meta->device = control->device;
+    meta->sm_count = control->sm_count > 0 ? control->sm_count : 148;
     meta->num_rows = csrMatx->num_rows;
     meta->num_nonzeros = csrMatx->num_nonzeros;
     meta->blk_size = blk;
