@@ -202,6 +202,33 @@ def gnn_profile(builds: int):
           flush=True)
 
 
+def learned_profile(iters: int):
+    """A short learned + mixed FP32 solve on the C5 matrix (network trained
+    briefly on 32^2 members of the family) with the solver loop in host chunks
+    (loop mode 1), so every kernel of a learned inner iteration is an ordinary
+    stream launch a profiler lists; ITERS bounds the inner iterations."""
+    import torch
+    from clsparse_b200 import _lib as L
+    from clsparse_b200 import api, learn, matgen
+    api.setup()
+    ctrl = api.Control()
+    spai, _ = learn.train(ctrl, sizes=(32,), seeds=range(2), steps=20, lr=3e-3)
+    ctrl.set_solver_loop_mode(1)
+    A = api.CsrMatrix.from_numpy(*matgen.diffusion2d_grf(1024, corr_len=0.05, sigma=2.0, seed=1005))
+    A.create_meta(ctrl)
+    spai.set_matrix(A, ctrl)
+    spai.build(ctrl)
+    n = A.num_rows
+    b = torch.tensor(np.random.default_rng(1).uniform(-1, 1, n), device="cuda")
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    sc = api.SolverControl(L.DIAGONAL, iters, 1e-10, 0.0)
+    info = api.cg_learned(x, A, b, sc, spai, ctrl, inner="fp32", inner_tol=0.3)
+    sc.release()
+    spai.release()
+    print(json.dumps({"learned_profile_inner_iterations": info["innerIterations"]}), flush=True)
+    ctrl.release()
+
+
 def cg_section(ctrl, with_cpu: bool):
     """Time-to-solution of the solver configurations the headline metric names.
 
@@ -626,6 +653,9 @@ def main():
     ap.add_argument("--no-cg", action="store_true", help="skip the CG time-to-solution section")
     ap.add_argument("--gnn-profile", type=int, default=0, metavar="BUILDS",
                     help="only run BUILDS learned-factor builds on the C5 matrix (profiling)")
+    ap.add_argument("--learned-profile", type=int, default=0, metavar="ITERS",
+                    help="only run a learned + mixed solve of at most ITERS inner iterations in loop mode 1 "
+                         "(profiling)")
     ap.add_argument("--cg-profile", type=int, default=0, metavar="ITERS",
                     help="only run ITERS iterations of FP64 Jacobi-CG on the C5 matrix with directly launched "
                          "kernels (for a profiler's launch list), then exit")
@@ -636,6 +666,9 @@ def main():
         return
     if args.cg_profile:
         cg_profile(args.cg_profile)
+        return
+    if args.learned_profile:
+        learned_profile(args.learned_profile)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
