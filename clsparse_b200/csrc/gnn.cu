@@ -790,8 +790,30 @@ struct Graph {
 using namespace clsp;
 using namespace clsp::gnn;
 
-// The learned preconditioner object: network parameters, optimiser state and
-// the graph of the matrix it was last set to.
+// Host copy of a matrix the network was set to, with the device addresses it
+// came from: the key of the graph cache (contents compared bit for bit, so a
+// matrix changed in place is never taken for the cached one).
+struct HostCsr {
+    const void* ptrs[3] = {};
+    uint32_t n = 0, nnz = 0;
+    std::vector<uint32_t> rp, cols;
+    std::vector<double> vals;
+    bool same(const HostCsr& o) const {
+        return ptrs[0] == o.ptrs[0] && ptrs[1] == o.ptrs[1] && ptrs[2] == o.ptrs[2] && n == o.n && nnz == o.nnz &&
+               rp == o.rp && cols == o.cols &&
+               std::memcmp(vals.data(), o.vals.data(), vals.size() * sizeof(double)) == 0;
+    }
+};
+
+struct CachedGraph {
+    HostCsr key;
+    Graph gr;
+};
+
+// The learned preconditioner object: network parameters, optimiser state, the
+// graph of the matrix it is set to, and the graphs of up to kGraphCache
+// matrices it was set to before (training cycles through a set of matrices;
+// each graph takes tens of allocations and host passes to build).
 struct _clsparseB200Spai {
     Offsets o;
     float* prm = nullptr;   // FP32 master weights
@@ -801,8 +823,11 @@ struct _clsparseB200Spai {
     int step = 0;
     int device = 0;
     Graph gr;
+    HostCsr cur;                       // the matrix gr was built from
+    std::vector<CachedGraph> cache;    // least recently used first
     ~_clsparseB200Spai() {
         gr.release();
+        for (CachedGraph& e : cache) e.gr.release();
         if (prm) cudaFree(prm);
         if (grad) cudaFree(grad);
         if (m) cudaFree(m);
@@ -812,22 +837,45 @@ struct _clsparseB200Spai {
 
 namespace {
 
+// Graphs of matrices up to kGraphCacheRows rows are kept for reuse, at most
+// kGraphCache of them (CLSPARSE_B200_SPAI_CACHE=0: none).
+constexpr size_t kGraphCache = 8;
+constexpr uint32_t kGraphCacheRows = 65536;
+
+bool graph_cache_enabled() {
+    const char* e = std::getenv("CLSPARSE_B200_SPAI_CACHE");
+    return !(e && e[0] == '0' && e[1] == '\0');
+}
+
+// Copies A's arrays to the host (the graph is built there).
+clsparseStatus read_host_csr(const clsparseCsrMatrix* A, clsparseControl c, HostCsr& h) {
+    h.n = A->num_rows;
+    h.nnz = A->num_nonzeros;
+    h.ptrs[0] = dev_ptr<const uint32_t>(A->row_pointer, A->off_row_pointer);
+    h.ptrs[1] = dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices);
+    h.ptrs[2] = dev_ptr<const double>(A->values, A->off_values);
+    h.rp.resize(size_t(h.n) + 1);
+    h.cols.resize(h.nnz);
+    h.vals.resize(h.nnz);
+    cudaStream_t s = c->stream;
+    cudaMemcpyAsync(h.rp.data(), h.ptrs[0], (size_t(h.n) + 1) * 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h.cols.data(), h.ptrs[1], size_t(h.nnz) * 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h.vals.data(), h.ptrs[2], size_t(h.nnz) * 8, cudaMemcpyDeviceToHost, s);
+    return cudaStreamSynchronize(s) == cudaSuccess ? clsparseSuccess : clsparseInvalidMemObject;
+}
+
 // Builds the graph structures of an SPD matrix A (FP64 values, sorted
-// columns, every diagonal present, at most kMaxP entries per row of tril(A)).
-clsparseStatus build_graph(_clsparseB200Spai* net, const clsparseCsrMatrix* A, clsparseControl c) {
+// columns, every diagonal present, at most kMaxP entries per row of tril(A))
+// from its host copy h.
+clsparseStatus build_graph(_clsparseB200Spai* net, const clsparseCsrMatrix* A, clsparseControl c,
+                           const HostCsr& h) {
     Graph& gr = net->gr;
     gr.release();
     const uint32_t n = A->num_rows, nnz = A->num_nonzeros;
-    std::vector<uint32_t> rp(n + 1), cols(nnz);
-    std::vector<double> vals(nnz);
+    const std::vector<uint32_t>& rp = h.rp;
+    const std::vector<uint32_t>& cols = h.cols;
+    const std::vector<double>& vals = h.vals;
     cudaStream_t s = c->stream;
-    cudaMemcpyAsync(rp.data(), dev_ptr<const uint32_t>(A->row_pointer, A->off_row_pointer), (n + 1) * 4,
-                    cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(cols.data(), dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices), size_t(nnz) * 4,
-                    cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(vals.data(), dev_ptr<const double>(A->values, A->off_values), size_t(nnz) * 8,
-                    cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) return clsparseInvalidMemObject;
     const uint32_t base = rp[0];
     std::vector<double> dinv(n, 0.0);
     for (uint32_t i = 0; i < n; ++i) {
@@ -1192,7 +1240,42 @@ clsparseStatus clsparseB200SpaiSetMatrix(clsparseB200Spai net, const clsparseCsr
     if (st != clsparseSuccess) return st;
     if (!A || A->num_rows != A->num_cols || A->num_rows == 0) return clsparseInvalidSystemSize;
     DeviceGuard g(control->device);
-    return build_graph(net, A, control);
+    HostCsr h;
+    st = read_host_csr(A, control, h);
+    if (st != clsparseSuccess) return st;
+    if (net->gr.built && net->cur.same(h)) return clsparseSuccess;
+    if (graph_cache_enabled()) {
+        // keep the current graph (most recent last), take a cached one if it matches
+        size_t hit = net->cache.size();
+        for (size_t i = 0; i < net->cache.size(); ++i)
+            if (net->cache[i].key.same(h)) {
+                hit = i;
+                break;
+            }
+        CachedGraph found;
+        if (hit < net->cache.size()) {
+            found = std::move(net->cache[hit]);
+            net->cache.erase(net->cache.begin() + static_cast<std::ptrdiff_t>(hit));
+        }
+        if (net->gr.built && net->gr.n <= kGraphCacheRows) {
+            net->cache.push_back(CachedGraph{std::move(net->cur), net->gr});
+            net->gr = Graph();  // now owned by the cache entry
+            while (net->cache.size() > kGraphCache) {
+                net->cache.front().gr.release();
+                net->cache.erase(net->cache.begin());
+            }
+        }
+        if (found.gr.built) {
+            net->gr.release();
+            net->gr = found.gr;
+            net->cur = std::move(found.key);
+            return clsparseSuccess;
+        }
+    }
+    net->cur = std::move(h);
+    st = build_graph(net, A, control, net->cur);
+    if (st != clsparseSuccess) net->cur = HostCsr();
+    return st;
 }
 
 clsparseStatus clsparseB200SpaiParams(clsparseB200Spai net, cl_float* host, size_t capacity, size_t* count,

@@ -138,3 +138,60 @@ def test_learned_solver_reaches_fp64_residual(ctrl, inner, loop_mode):
     res = np.linalg.norm(b - A @ x.cpu().numpy()) / np.linalg.norm(b)
     assert res <= 2e-10, (res, info)
     spai.release()
+
+
+def test_graph_cache_reuse_and_in_place_change(ctrl, monkeypatch):
+    """Setting the network to a matrix it was set to before reuses the cached
+    graph: the built factor is bitwise that of a network without the cache
+    (CLSPARSE_B200_SPAI_CACHE=0). A matrix changed in place at the same
+    addresses is rebuilt, not taken for the cached one."""
+    mats = [matgen.diffusion2d_grf(20, corr_len=0.2, sigma=1.5, seed=s) for s in (31, 32)]
+    As = [api.CsrMatrix.from_numpy(*m) for m in mats]
+
+    def factors(seq):
+        spai = api.Spai(5)
+        out = []
+        for k in seq:
+            spai.set_matrix(As[k], ctrl)
+            spai.build(ctrl)
+            out.append(spai.factor()[2].copy())
+        spai.release()
+        return out
+
+    seq = [0, 1, 0, 1, 0]
+    cached = factors(seq)
+    monkeypatch.setenv("CLSPARSE_B200_SPAI_CACHE", "0")
+    fresh = factors(seq)
+    monkeypatch.delenv("CLSPARSE_B200_SPAI_CACHE")
+    for a, b in zip(cached, fresh):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(cached[0], cached[2])
+    # change A0's values in place (same device buffers): the factor must follow
+    spai = api.Spai(5)
+    spai.set_matrix(As[0], ctrl)
+    spai.build(ctrl)
+    before = spai.factor()[2].copy()
+    spai.set_matrix(As[1], ctrl)
+    As[0].val.mul_(2.0)
+    spai.set_matrix(As[0], ctrl)
+    spai.build(ctrl)
+    after = spai.factor()[2]
+    ref = api.Spai(5)
+    monkeypatch.setenv("CLSPARSE_B200_SPAI_CACHE", "0")
+    ref.set_matrix(As[0], ctrl)
+    ref.build(ctrl)
+    np.testing.assert_array_equal(after, ref.factor()[2])
+    assert not np.array_equal(after, before)
+    spai.release()
+    ref.release()
+
+
+def test_training_same_with_and_without_graph_cache(ctrl, monkeypatch):
+    """Training cycles through its matrices; the cached graphs give the same
+    loss history, bit for bit, as rebuilding every step."""
+    s1, h1 = learn.train(ctrl, sizes=(24,), seeds=range(3), steps=12, lr=3e-3)
+    monkeypatch.setenv("CLSPARSE_B200_SPAI_CACHE", "0")
+    s0, h0 = learn.train(ctrl, sizes=(24,), seeds=range(3), steps=12, lr=3e-3)
+    s1.release()
+    s0.release()
+    assert h1 == h0
