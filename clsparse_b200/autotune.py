@@ -11,6 +11,13 @@ point: a candidate that disagrees raises), and it is timed with CUDA events
 (median of `reps` launches). The fastest shape is returned with the whole
 sweep.
 
+Matrices whose rows are all at most 16 long (stencils) take the library's
+thread-per-row path whatever the meta's shape, so for them every candidate
+times the same kernel and the sweep only confirms parity; the table's entries
+for such matrices (poisson512, diffusion3d_64) were measured with the
+row-block kernel (CLSPARSE_B200_SHORT_ROWS=0) and apply only under that
+setting.
+
 Batched CG. `tune_batched_lanes` times clsparseScsrcgBatched on batches of one
 size class at a time with every lanes-per-row width and keeps the fastest per
 class.
