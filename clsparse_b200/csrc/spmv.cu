@@ -247,8 +247,8 @@ uint32_t short_rows_grid(const matrix_meta* m, uint32_t nrows) {
 }
 
 template <typename V, typename T, bool EXT, int K>
-void launch_row_per_thread(const CsrView<V>& A, const T* alpha, const T* beta, const T* x, T* y, const EpiDev<T>& e,
-                     cudaStream_t s) {
+void launch_row_per_thread(const CsrView<V>& A, const T* alpha, const T* beta, const T* x, T* y,
+                           const EpiDev<T>& e, cudaStream_t s) {
     csr_vector_kernel<V, T, EXT, 1, K><<<short_rows_grid(A.meta, A.nrows), kThreads, 0, s>>>(
         A.vals, A.cols, A.rp, x, y, alpha, beta, A.nrows, e);
 }
