@@ -22,7 +22,12 @@
 // streams, or different host threads, running at the same time) race on it
 // and must be serialised by the caller. The first call on each device looks
 // up the array's device address (cudaGetSymbolAddress) with that device
-// current; make that first call before any stream capture is begun.
+// current; make that first call before any stream capture is begun. Only a
+// successful lookup is kept: a call whose lookup fails returns
+// clsparseInvalidDevice and the next call tries again. The address is kept
+// for the life of the process, so resetting a device (cudaDeviceReset) after
+// the first call on it is not supported: the array may be reloaded elsewhere.
+#include <atomic>
 #include <mutex>
 
 #include "device_common.cuh"
@@ -39,11 +44,27 @@ constexpr uint64_t kMaxElements = static_cast<uint64_t>(kSlots) * kChunk;
 // [0, kSlots): partial sums; word kSlots: arrival ticket (as uint32).
 static __device__ __align__(256) double g_dot_scratch[kSlots + 32];
 
-// Device addresses of g_dot_scratch, looked up once per device.
+// Device addresses of g_dot_scratch, one per device: null until a lookup
+// with that device current has succeeded.
 constexpr int kMaxDevices = 64;
-std::once_flag g_addr_once[kMaxDevices];
-double* g_addr[kMaxDevices];
-cudaError_t g_addr_err[kMaxDevices];
+std::mutex g_addr_mutex[kMaxDevices];
+std::atomic<double*> g_addr[kMaxDevices];
+
+double* scratch_address(int dev) {
+    double* p = g_addr[dev].load(std::memory_order_acquire);
+    if (p) return p;
+    std::lock_guard<std::mutex> lock(g_addr_mutex[dev]);
+    p = g_addr[dev].load(std::memory_order_relaxed);
+    if (p) return p;
+    void* q = nullptr;
+    if (cudaGetSymbolAddress(&q, g_dot_scratch) != cudaSuccess || q == nullptr) {
+        cudaGetLastError();  // not sticky: leave no error behind for the caller's next call
+        return nullptr;
+    }
+    p = static_cast<double*>(q);
+    g_addr[dev].store(p, std::memory_order_release);
+    return p;
+}
 
 __global__ void __launch_bounds__(kThreads)
     dot_noalloc_kernel(const double* __restrict__ x, const double* __restrict__ y, uint64_t n,
@@ -74,15 +95,10 @@ clsparseStatus cldenseDdotNoAlloc(clsparseScalar* r, const cldenseVector* x, con
     if (n > 0 && (!x->values || !y->values)) return clsparseInvalidMemObject;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return clsparseInvalidDevice;
-    // One-time set-up on this device: the host-side symbol is only a stand-in,
-    // the kernel needs the array's device address.
-    std::call_once(g_addr_once[dev], [dev] {
-        void* p = nullptr;
-        g_addr_err[dev] = cudaGetSymbolAddress(&p, g_dot_scratch);
-        g_addr[dev] = static_cast<double*>(p);
-    });
-    if (g_addr_err[dev] != cudaSuccess || g_addr[dev] == nullptr) return clsparseInvalidDevice;
-    double* scratch = g_addr[dev];
+    // Set-up on this device (first successful call): the host-side symbol is
+    // only a stand-in, the kernel needs the array's device address.
+    double* scratch = scratch_address(dev);
+    if (scratch == nullptr) return clsparseInvalidDevice;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(queue);
     // the ticket must start at zero; a call cut short earlier may have left it set
     if (cudaMemsetAsync(scratch + kSlots, 0, sizeof(double), s) != cudaSuccess)

@@ -213,8 +213,11 @@ clsparseDcsrcgLearned(cldenseVector* x, const clsparseCsrMatrix* A, const cldens
  * Limit: at most 33,554,432 elements (clsparseInvalidSize beyond). Returns
  * once the work is enqueued on queue. All calls share the array, so calls
  * that overlap on the GPU race and must be serialised by the caller. The
- * first call on a device looks the array up on that device; make it before
- * beginning any stream capture. No counterpart in the reference. */
+ * first successful call on a device looks the array up on that device; make
+ * it before beginning any stream capture. A failed lookup returns
+ * clsparseInvalidDevice and is retried by the next call. Resetting a device
+ * (cudaDeviceReset) after the first call on it is not supported. No
+ * counterpart in the reference. */
 CLSPARSE_EXPORT clsparseStatus
 cldenseDdotNoAlloc(clsparseScalar* r, const cldenseVector* x, const cldenseVector* y,
                    cl_command_queue queue);
