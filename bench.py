@@ -110,27 +110,52 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(rp, col, val, seconds=12.0):
-    """Oracle port of the reference SpMV on all host cores for ~`seconds`."""
+# CPU timing protocol of the reference's benchmark client
+# (src/benchmarks/clsparse-bench/functions/clfunc_xSpMdV.hpp:208-215 with
+# src/benchmarks/clsparse-bench/src/statisticalTimer.cpp:270-293): SAMPLES
+# host-timed samples, each the mean of CALLS back-to-back calls; samples
+# further than 3 standard deviations from the mean are pruned; the mean of
+# the rest is reported.
+CPU_SAMPLES = 20
+CPU_CALLS = 20
+
+
+def cpu_spmv_protocol(rp, col, val, samples=CPU_SAMPLES, calls=CPU_CALLS):
+    """The oracle port of the reference SpMV (FP64, alpha 1, beta 0) on all
+    host cores through a thread pool created once, timed by the protocol
+    above. One function serves both the repo arm's cpu_baseline and the
+    --impl reference arm, so the two report the same measurement."""
     import oracle
     n = len(rp) - 1
     threads = os.cpu_count() or 1
     x = np.random.default_rng(3).uniform(-1, 1, n)
     y = np.zeros(n)
     nbytes = 4 * (len(col) + n) + 8 * (len(col) + 2 * n)
-    oracle.dcsrmv_mt(rp, col, val, 1.0, x, 0.0, y, threads)  # warm
-    t0 = time.perf_counter()
-    reps = 0
-    while True:
+    for _ in range(3):  # warm: pool start-up, page faults, caches
         oracle.dcsrmv_mt(rp, col, val, 1.0, x, 0.0, y, threads)
-        reps += 1
-        el = time.perf_counter() - t0
-        if el >= seconds or reps >= 1000:
-            break
-    gbs = nbytes * reps / el / 1e9
+    per_call = []
+    for _ in range(samples):
+        t0 = time.perf_counter()
+        for _ in range(calls):
+            oracle.dcsrmv_mt(rp, col, val, 1.0, x, 0.0, y, threads)
+        per_call.append((time.perf_counter() - t0) / calls)
+    mean = statistics.fmean(per_call)
+    sd = statistics.pstdev(per_call)
+    kept = [t for t in per_call if abs(t - mean) <= 3.0 * sd] or per_call
+    t = statistics.fmean(kept)
+    gbs = nbytes / t / 1e9
     return {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
-            "sample": f"{reps} full FP64 SpMVs of the same 2M-row matrix ({el:.1f} s, "
-                      f"row ranges balanced by nnz over {threads} threads)"}
+            "seconds_per_call": t,
+            "sample": f"{samples} samples x {calls} full FP64 SpMVs of the same 2M-row matrix, 3-sigma pruning "
+                      f"({len(per_call) - len(kept)} pruned); row ranges balanced by nnz over a pool of "
+                      f"{threads} host threads created once"}
+
+
+def cpu_baseline(rp, col, val):
+    """Oracle port of the reference SpMV on all host cores (the protocol above)."""
+    r = cpu_spmv_protocol(rp, col, val)
+    r.pop("seconds_per_call")
+    return r
 
 
 def _timed(fn, reps=2):
@@ -475,34 +500,29 @@ def make_matrix():
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the oracle port of the reference SpMV on all host
+    cores, by the same protocol and function as the repo arm's cpu_baseline:
+    each step is one sample of CPU_CALLS SpMVs (fewer calls per sample above
+    20 steps, so that about 400 SpMVs are timed whatever --steps is)."""
     if rank != 0:
         return
     rp, col, val = make_matrix()
-    import oracle
     n = len(rp) - 1
-    threads = os.cpu_count() or 1
-    x = np.random.default_rng(3).uniform(-1, 1, n)
-    y = np.zeros(n)
     nbytes = 4 * (len(col) + n) + 8 * (len(col) + 2 * n)
-    for _ in range(max(args.warmup, 1)):
-        oracle.dcsrmv_mt(rp, col, val, 1.0, x, 0.0, y, threads)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        oracle.dcsrmv_mt(rp, col, val, 1.0, x, 0.0, y, threads)
-        times.append(time.perf_counter() - t0)
-    total = sum(times)
-    gbs = nbytes * args.steps / total / 1e9
+    samples = max(args.steps, 3)
+    calls = CPU_CALLS if samples <= CPU_SAMPLES else max(2, (CPU_SAMPLES * CPU_CALLS) // samples)
+    r = cpu_spmv_protocol(rp, col, val, samples=samples, calls=calls)
+    gbs = r["value"]
     line = {
-        "impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s",
+        "impl": "reference", "metric": METRIC, "value": gbs, "unit": "GB/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(1e3 * total / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": round(1e3 * r["seconds_per_call"], 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": {"workload": WORKLOAD, "nnz": int(len(col)), "rows": n, "bytes_per_step": nbytes},
-        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} full FP64 SpMVs (oracle restatement of the reference "
-                                   "algorithm; the reference's OpenCL path has no runtime here)"},
-        "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": r["cores"], "kind": "port",
+                         "sample": r["sample"] + " (oracle restatement of the reference algorithm; the "
+                                                 "reference's OpenCL path has no runtime here)"},
+        "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 

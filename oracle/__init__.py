@@ -49,6 +49,9 @@ def lib():
                                              C.c_double, _f64p, _f64p]
         L.oracle_dcsrmv_mt.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, C.c_double, _f64p, C.c_double,
                                        _f64p, C.c_int]
+        L.oracle_dcg_mt.restype = C.c_int
+        L.oracle_dcg_mt.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, _f64p, _f64p, C.c_int, C.c_double, C.c_int,
+                                    C.POINTER(C.c_double)]
         for sfx, fp in (("d", _f64p), ("s", _f32p)):
             for name in (f"oracle_{sfx}cg", f"oracle_{sfx}bicgstab"):
                 f = getattr(L, name)
@@ -138,6 +141,21 @@ def dcsrmv_absscale(rp, col, val, alpha, x, beta, y):
 def dcsrmv_mt(rp, col, val, alpha, x, beta, y, threads):
     lib().oracle_dcsrmv_mt(len(rp) - 1, rp, col, val, float(alpha), x, float(beta), y, int(threads))
     return y
+
+
+def reference_solution(rp, col, val, b, rel_tol=1e-12, max_iters=1_000_000, threads=None):
+    """FP64 Jacobi-PCG (oracle_dcg_mt: the reference CG's operation order on a
+    pool of host threads, L2 stop test) from x = 0 to ||b - A x||_2 / ||b||_2
+    <= rel_tol. Returns (x, iterations, final relative residual of the
+    recursion). Used as the FP64 oracle solution of the large configurations."""
+    import os
+    n = len(rp) - 1
+    x = np.zeros(n)
+    res = C.c_double(0.0)
+    it = lib().oracle_dcg_mt(n, np.ascontiguousarray(rp, np.uint32), np.ascontiguousarray(col, np.uint32),
+                             np.ascontiguousarray(val, np.float64), x, np.ascontiguousarray(b, np.float64),
+                             int(max_iters), float(rel_tol), int(threads or os.cpu_count() or 1), C.byref(res))
+    return x, it, res.value
 
 
 def solve(kind, dtype, rp, col, val, x0, b, precond, max_iters, rel_tol, abs_tol, n_iters_in=0):

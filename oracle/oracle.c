@@ -17,8 +17,11 @@
  *   oracle_{d,s}cg     src/library/solvers/conjugate-gradients.hpp:47-228 with the
  *                      stop test of solvers/solver-control.hpp:47-64
  *   oracle_{d,s}bicgstab  src/library/solvers/biconjugate-gradients-stabilized.hpp:41-268
- *   oracle_dcsrmv_mt   the same SpMV split over host threads by row blocks (the
- *                      CPU baseline bench.py times)
+ *   oracle_dcsrmv_mt   the same SpMV split over a reused pool of host threads by
+ *                      equal-nonzero row ranges (the CPU baseline bench.py times)
+ *   oracle_dcg_mt      FP64 Jacobi-PCG in the order of conjugate-gradients.hpp on
+ *                      the same thread pool, L2 stop test: reference solutions of
+ *                      the large configurations
  */
 #include <math.h>
 #include <float.h>
@@ -176,6 +179,11 @@ void oracle_dcsrmv_absscale(uint32_t n, const uint32_t *rp, const uint32_t *col,
 
 /* ------------------------------------------------------ threaded baseline */
 
+/* The CPU baseline's SpMV: rows split into equal-nonzero ranges over a pool of
+ * host threads that is created once and reused by every call, so a timed call
+ * holds only the SpMV itself (no thread start-up). The calling thread works on
+ * the first range. Not thread-safe: one caller at a time. */
+
 typedef struct {
     uint32_t r0, r1;
     const uint32_t *rp, *col;
@@ -184,37 +192,248 @@ typedef struct {
     double *y;
 } spmv_task;
 
-static void *spmv_worker(void *p)
+static void spmv_rows(const spmv_task *t)
 {
-    spmv_task *t = (spmv_task *)p;
     for (uint32_t r = t->r0; r < t->r1; r++) {
         double s = 0.0;
         for (uint32_t j = t->rp[r]; j < t->rp[r + 1]; j++) s += t->alpha * t->val[j] * t->x[t->col[j]];
         t->y[r] = (t->beta == 0.0) ? s : s + t->beta * t->y[r];
     }
+}
+
+#define POOL_MAX 256
+static int pool_size = 0; /* threads including the caller; 0 = no pool */
+static pthread_t pool_tid[POOL_MAX];
+static pthread_barrier_t pool_start, pool_done;
+static spmv_task pool_task[POOL_MAX];
+static volatile int pool_quit = 0;
+typedef void (*pool_fn)(int k, void *ctx);
+static pool_fn pool_job;
+static void *pool_ctx;
+
+static void *pool_worker(void *arg)
+{
+    const int k = (int)(intptr_t)arg;
+    for (;;) {
+        pthread_barrier_wait(&pool_start);
+        if (pool_quit) break;
+        pool_job(k, pool_ctx);
+        pthread_barrier_wait(&pool_done);
+    }
     return NULL;
 }
 
-/* FP64 SpMV over `threads` host threads, rows split into equal-nonzero ranges. */
+static void pool_stop(void)
+{
+    if (pool_size <= 1) {
+        pool_size = 0;
+        return;
+    }
+    pool_quit = 1;
+    pthread_barrier_wait(&pool_start);
+    for (int k = 1; k < pool_size; k++) pthread_join(pool_tid[k], NULL);
+    pthread_barrier_destroy(&pool_start);
+    pthread_barrier_destroy(&pool_done);
+    pool_quit = 0;
+    pool_size = 0;
+}
+
+static void pool_resize(int threads)
+{
+    if (threads == pool_size) return;
+    pool_stop();
+    pool_size = threads;
+    if (threads <= 1) return;
+    pthread_barrier_init(&pool_start, NULL, (unsigned)threads);
+    pthread_barrier_init(&pool_done, NULL, (unsigned)threads);
+    for (int k = 1; k < threads; k++) pthread_create(&pool_tid[k], NULL, pool_worker, (void *)(intptr_t)k);
+}
+
+/* Runs job(k, ctx) for k in [0, pool_size) and returns when all are done;
+ * the calling thread runs k = 0. */
+static void pool_run(pool_fn job, void *ctx)
+{
+    pool_job = job;
+    pool_ctx = ctx;
+    if (pool_size > 1) pthread_barrier_wait(&pool_start);
+    job(0, ctx);
+    if (pool_size > 1) pthread_barrier_wait(&pool_done);
+}
+
+static void spmv_job(int k, void *ctx)
+{
+    (void)ctx;
+    spmv_rows(&pool_task[k]);
+}
+
+/* First row r in [lo, n] with rp[r] >= target. */
+static uint32_t first_row_at(const uint32_t *rp, uint32_t lo, uint32_t n, uint64_t target)
+{
+    uint32_t hi = n;
+    while (lo < hi) {
+        uint32_t mid = lo + (hi - lo) / 2;
+        if ((uint64_t)rp[mid] < target) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+/* Row ranges of `parts` threads with equal nonzeros (bounds[0..parts]). */
+static void nnz_ranges(const uint32_t *rp, uint32_t n, int parts, uint32_t *bounds)
+{
+    const uint64_t nnz = rp[n] - rp[0];
+    bounds[0] = 0;
+    for (int k = 0; k < parts; k++)
+        bounds[k + 1] = (k == parts - 1) ? n
+                        : first_row_at(rp, bounds[k], n, rp[0] + (nnz * (uint64_t)(k + 1)) / (uint64_t)parts);
+}
+
+/* FP64 SpMV over `threads` host threads (the pool is resized when the count
+ * changes), rows split into equal-nonzero ranges by binary search. */
 void oracle_dcsrmv_mt(uint32_t n, const uint32_t *rp, const uint32_t *col, const double *val,
                       double alpha, const double *x, double beta, double *y, int threads)
 {
     if (threads < 1) threads = 1;
-    if (threads > 256) threads = 256;
-    pthread_t tid[256];
-    spmv_task task[256];
-    uint64_t nnz = rp[n] - rp[0];
-    uint32_t r = 0;
-    for (int k = 0; k < threads; k++) {
-        uint64_t target = rp[0] + (nnz * (uint64_t)(k + 1)) / (uint64_t)threads;
-        uint32_t r1 = r;
-        while (r1 < n && rp[r1] < target) r1++;
-        if (k == threads - 1) r1 = n;
-        task[k] = (spmv_task){r, r1, rp, col, val, x, alpha, beta, y};
-        r = r1;
+    if (threads > POOL_MAX) threads = POOL_MAX;
+    pool_resize(threads);
+    uint32_t bounds[POOL_MAX + 1];
+    nnz_ranges(rp, n, threads, bounds);
+    for (int k = 0; k < threads; k++)
+        pool_task[k] = (spmv_task){bounds[k], bounds[k + 1], rp, col, val, x, alpha, beta, y};
+    pool_run(spmv_job, NULL);
+}
+
+/* Ends the pool's threads (the next threaded call starts a new pool). */
+void oracle_pool_shutdown(void)
+{
+    pool_stop();
+}
+
+/* Threaded FP64 Jacobi-PCG used to make reference solutions of the large
+ * configurations (the serial oracle_dcg below is the parity oracle for
+ * iteration counts). Operation order of conjugate-gradients.hpp:100-226:
+ * r = b - A x, z = D^-1 r, p = z, then per iteration q = A p, alpha =
+ * <r,z>/<p,q>, x += alpha p, r -= alpha q, z = D^-1 r, beta = <r,z>_new /
+ * <r,z>, p = z + beta p; stopped on the L2 relative residual
+ * ||r||_2 / ||b||_2 <= rel_tol (the stop test the mixed-precision solvers of
+ * this library use). Rows without a diagonal entry keep z_i = r_i. Per-thread
+ * partial sums are added in thread order, so a run is reproducible for a
+ * given thread count. Returns the iterations. */
+typedef struct {
+    const uint32_t *rp, *col, *bounds;
+    const double *val, *b, *dinv;
+    double *x, *r, *z, *p, *q;
+    double alpha, beta;
+    int phase;
+    double part[POOL_MAX][4];
+} cg_mt_ctx;
+
+static void cg_mt_job(int k, void *vctx)
+{
+    cg_mt_ctx *c = (cg_mt_ctx *)vctx;
+    const uint32_t r0 = c->bounds[k], r1 = c->bounds[k + 1];
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (uint32_t i = r0; i < r1; i++) {
+        if (c->phase == 0) { /* r = b - A x; z = D^-1 r; p = z; <r,z>, <r,r>, <b,b> */
+            double t = 0.0;
+            for (uint32_t j = c->rp[i]; j < c->rp[i + 1]; j++) t += c->val[j] * c->x[c->col[j]];
+            const double ri = c->b[i] - t;
+            c->r[i] = ri;
+            c->z[i] = c->dinv[i] * ri;
+            c->p[i] = c->z[i];
+            s0 += ri * c->z[i];
+            s1 += ri * ri;
+            s2 += c->b[i] * c->b[i];
+        } else if (c->phase == 1) { /* q = A p; <p,q> */
+            double t = 0.0;
+            for (uint32_t j = c->rp[i]; j < c->rp[i + 1]; j++) t += c->val[j] * c->p[c->col[j]];
+            c->q[i] = t;
+            s0 += c->p[i] * t;
+        } else if (c->phase == 2) { /* x, r, z updates; <r,z>, <r,r> */
+            c->x[i] += c->alpha * c->p[i];
+            const double ri = c->r[i] - c->alpha * c->q[i];
+            c->r[i] = ri;
+            c->z[i] = c->dinv[i] * ri;
+            s0 += ri * c->z[i];
+            s1 += ri * ri;
+        } else { /* p = z + beta p */
+            c->p[i] = c->z[i] + c->beta * c->p[i];
+        }
     }
-    for (int k = 0; k < threads; k++) pthread_create(&tid[k], NULL, spmv_worker, &task[k]);
-    for (int k = 0; k < threads; k++) pthread_join(tid[k], NULL);
+    c->part[k][0] = s0;
+    c->part[k][1] = s1;
+    c->part[k][2] = s2;
+}
+
+static void cg_mt_sum(const cg_mt_ctx *c, int parts, double *out)
+{
+    out[0] = out[1] = out[2] = 0.0;
+    for (int k = 0; k < parts; k++) {
+        out[0] += c->part[k][0];
+        out[1] += c->part[k][1];
+        out[2] += c->part[k][2];
+    }
+}
+
+int oracle_dcg_mt(uint32_t n, const uint32_t *rp, const uint32_t *col, const double *val, double *x,
+                  const double *b, int max_iters, double rel_tol, int threads, double *final_rel_res)
+{
+    if (threads < 1) threads = 1;
+    if (threads > POOL_MAX) threads = POOL_MAX;
+    pool_resize(threads);
+    cg_mt_ctx *c = (cg_mt_ctx *)calloc(1, sizeof(cg_mt_ctx));
+    uint32_t *bounds = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(threads + 1));
+    double *work = (double *)malloc(sizeof(double) * (size_t)n * 5);
+    double *dinv = work + 4 * (size_t)n;
+    nnz_ranges(rp, n, threads, bounds);
+    for (uint32_t i = 0; i < n; i++) { /* first matching diagonal entry */
+        dinv[i] = 1.0;
+        for (uint32_t j = rp[i]; j < rp[i + 1]; j++)
+            if (col[j] == i) {
+                dinv[i] = 1.0 / val[j];
+                break;
+            }
+    }
+    c->rp = rp;
+    c->col = col;
+    c->val = val;
+    c->bounds = bounds;
+    c->b = b;
+    c->dinv = dinv;
+    c->x = x;
+    c->r = work;
+    c->z = work + n;
+    c->p = work + 2 * (size_t)n;
+    c->q = work + 3 * (size_t)n;
+    double s[3];
+    c->phase = 0;
+    pool_run(cg_mt_job, c);
+    cg_mt_sum(c, threads, s);
+    double rz = s[0];
+    const double bn = sqrt(s[2]);
+    double res = bn > 0.0 ? sqrt(s[1]) / bn : 0.0;
+    int it = 0;
+    while (bn > 0.0 && res > rel_tol && it < max_iters) {
+        c->phase = 1;
+        pool_run(cg_mt_job, c);
+        cg_mt_sum(c, threads, s);
+        c->alpha = rz / s[0];
+        c->phase = 2;
+        pool_run(cg_mt_job, c);
+        cg_mt_sum(c, threads, s);
+        res = sqrt(s[1]) / bn;
+        c->beta = s[0] / rz;
+        rz = s[0];
+        it++;
+        if (res <= rel_tol) break;
+        c->phase = 3;
+        pool_run(cg_mt_job, c);
+    }
+    if (final_rel_res) *final_rel_res = res;
+    free(work);
+    free(bounds);
+    free(c);
+    return it;
 }
 
 /* --------------------------------------------------------------- solvers */
