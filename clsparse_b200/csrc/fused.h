@@ -28,13 +28,20 @@ struct WordMat {
 };
 
 // Grid exchange area: arrival counter, release flag and error flag (zero at
-// launch) and two buffers of four partial sums per CTA.
+// launch) and two buffers of four partial sums per CTA; the limit of one
+// barrier wait, and a test switch under which the last CTA to arrive does not
+// release the first barrier, so that every wait runs out (the failure path's
+// test: the kernel must end with the barrier-timeout status, every CTA gone).
 struct FusedSync {
     unsigned long long* arrive;
     unsigned long long* release;
     int* err;
     double* partials;
+    unsigned long long wait_ns;
+    int never_release;
 };
+
+constexpr unsigned long long kFusedWaitNs = 4000000000ull;  // one barrier wait gives up after 4 s
 
 constexpr size_t kFusedSyncHead = 256;  // bytes zeroed before each launch
 inline size_t fused_sync_bytes(uint32_t G) { return kFusedSyncHead + 2 * 4 * static_cast<size_t>(G) * sizeof(double); }
@@ -46,6 +53,8 @@ inline FusedSync fused_sync_at(void* base) {
     s.release = reinterpret_cast<unsigned long long*>(b + 128);
     s.err = reinterpret_cast<int*>(b + 192);
     s.partials = reinterpret_cast<double*>(b + kFusedSyncHead);
+    s.wait_ns = kFusedWaitNs;
+    s.never_release = 0;
     return s;
 }
 

@@ -36,8 +36,6 @@
 namespace clsp {
 namespace {
 
-constexpr uint64_t kWaitNs = 4000000000ull;  // one barrier wait gives up after 4 s
-
 __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -94,7 +92,7 @@ __device__ bool grid_exchange(const FusedSync& g, unsigned long long& epoch, con
         __threadfence();
         bool ok = true;
         const unsigned long long t = atomicAdd(g.arrive, 1ull);
-        if (t + 1ull == epoch * G) {
+        if (t + 1ull == epoch * G && !g.never_release) {
             st_release(g.release, epoch);
         } else {
             uint64_t t0 = 0;
@@ -108,7 +106,7 @@ __device__ bool grid_exchange(const FusedSync& g, unsigned long long& epoch, con
                     const uint64_t now = global_ns();
                     if (t0 == 0) {
                         t0 = now;
-                    } else if (now - t0 > kWaitNs) {
+                    } else if (now - t0 > g.wait_ns) {
                         atomicExch(g.err, 1);
                         ok = false;
                         break;

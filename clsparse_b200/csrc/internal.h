@@ -134,6 +134,7 @@ struct _solverControl {
     PRINT_MODE printMode = QUIET;
     cl_uint deviceStatus = 0;
     cl_int normType = 0;  // 0: reference L1 stop test, 1: L2 (clsparseB200SolverSetNormType)
+    cl_int stopOnNonFinite = 0;  // internal: inner solves of the refinement end on a non-finite residual
     void printSummary(clsparseStatus status) const;
 };
 

@@ -128,6 +128,7 @@ clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const clden
     inner.preconditioner = sc->preconditioner;
     inner.normType = 1;
     inner.printMode = QUIET;
+    inner.stopOnNonFinite = 1;  // a broken factor costs one inner iteration, not the budget
 
     const double target = sc->relativeTolerance;
     const int max_inner_total = sc->maxIters;
@@ -209,7 +210,11 @@ clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const clden
         prev_factor = use_factor;
         predicted = res * inner.currentResidual;
         inner_total += inner.nIters + 1;
-        update_kernel<<<g, kThreads, 0, s>>>(x, static_cast<const float*>(w.d.ptr), bnorm, n);
+        // A correction from an inner solve that went non-finite is dropped: x
+        // keeps its last FP64 value and the next step (with Jacobi, if the
+        // learned factor caused it) starts from there.
+        if ((inner.deviceStatus & 0x10u) == 0)
+            update_kernel<<<g, kThreads, 0, s>>>(x, static_cast<const float*>(w.d.ptr), bnorm, n);
         ++outer;
     }
     info->outerIterations = outer;

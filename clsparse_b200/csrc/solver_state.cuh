@@ -28,6 +28,7 @@ struct SolverState {
     double absTol;
     int maxIters;
     int norm_type;  // 0: ||.||_1 as the reference, 1: ||.||_2
+    int stop_nonfinite;  // 1: a non-finite residual ends the solve (inner solves of the refinement)
     // scalars of the iteration, in T like the reference
     T norm_b, rz, rz_old, yp, alpha, beta, omega, norm_r, res;
     T rsr_old, rsr_new, rs_amp, amss, amsams;
@@ -45,9 +46,13 @@ struct SolverState {
 
 // The reference's stop test (solver-control.hpp:47-64): converged if
 // res <= relTol or res <= absTol * initial residual, or out of iterations.
+// The reference keeps iterating on a non-finite residual until maxIters; the
+// inner solves of the mixed-precision refinement stop at once instead
+// (stop_nonfinite), so that a broken preconditioner costs one iteration.
 template <typename T>
 __device__ __forceinline__ bool solver_finished(const SolverState<T>& s, double res) {
-    return (res <= s.relTol) || (res <= s.absTol * s.init_res) || (s.nIters >= s.maxIters);
+    return (res <= s.relTol) || (res <= s.absTol * s.init_res) || (s.nIters >= s.maxIters) ||
+           (s.stop_nonfinite && !isfinite(res));
 }
 
 __device__ __forceinline__ void set_condition(unsigned long long h, unsigned int v) {

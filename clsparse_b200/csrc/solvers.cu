@@ -649,6 +649,7 @@ void init_state(SolverState<T>& h, clSParseSolverControl sc) {
     h.absTol = sc->absoluteTolerance;
     h.maxIters = sc->maxIters;
     h.norm_type = sc->normType & 1;
+    h.stop_nonfinite = sc->stopOnNonFinite ? 1 : 0;
     h.nIters = sc->nIters;
     h.one = T(1);
     h.zero = T(0);
@@ -735,6 +736,13 @@ bool fused_ok(clsparseControl c, const matrix_meta* m) {
 
 size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
+// After a persistent solve ended on a barrier timeout, CTAs that had passed
+// a barrier may have counted long-row chunks whose other owners had already
+// left: the meta's arrival tickets are zeroed so that later SpMVs start clean.
+void reset_long_row_tickets(const matrix_meta* m, cudaStream_t s) {
+    if (m && m->d_lr_ticket) cudaMemsetAsync(m->d_lr_ticket, 0, m->num_words * sizeof(uint32_t), s);
+}
+
 // Launches the persistent solver: sizes the barrier area, makes the per-CTA
 // word ranges of A (and G, Gt) when the operands or the grid changed, zeroes
 // the barrier counters and launches one cooperative kernel.
@@ -774,6 +782,13 @@ clsparseStatus run_fused(clsparseControl c, SolverCache& cache, bool rebuild, Fu
     }
     if (cudaMemsetAsync(base, 0, kFusedSyncHead, c->stream) != cudaSuccess) return clsparseInvalidKernelExecution;
     fa.sync = fused_sync_at(base);
+    // Failure-path test switches: a shorter wait limit, and a first barrier
+    // that is never released (every wait then runs out).
+    if (const char* e = std::getenv("CLSPARSE_B200_BARRIER_WAIT_NS")) {
+        const unsigned long long v = std::strtoull(e, nullptr, 10);
+        if (v > 0) fa.sync.wait_ns = v;
+    }
+    if (const char* e = std::getenv("CLSPARSE_B200_TEST_BARRIER_NEVER_RELEASE")) fa.sync.never_release = std::atoi(e) != 0;
     fa.A = word_mat(Av, wA);
     if (G) fa.G = word_mat(*G, wG);
     if (Gt) fa.Gt = word_mat(*Gt, wGt);
@@ -892,6 +907,10 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
         return stt;
     }
     stt = read_back<T>(c, cache, sc);
+    if (sc->deviceStatus & kStatusBarrierTimeout) {
+        reset_long_row_tickets(Av.meta, c->stream);
+        cache.valid = false;
+    }
     if (ws && stt == clsparseSuccess)
         ws->rz = static_cast<double>(reinterpret_cast<SolverState<T>*>(static_cast<char*>(c->pinned) + 2048)->rz_old);
     sc->printSummary(stt);
@@ -1125,6 +1144,12 @@ clsparseStatus pcg_factor_solve(cldenseVector* xv, const clsparseCsrMatrix* A, c
         return stt;
     }
     stt = read_back<T>(c, cache, sc);
+    if (sc->deviceStatus & kStatusBarrierTimeout) {
+        reset_long_row_tickets(Av.meta, c->stream);
+        reset_long_row_tickets(G.meta, c->stream);
+        reset_long_row_tickets(Gt.meta, c->stream);
+        cache.valid = false;
+    }
     if (ws && stt == clsparseSuccess)
         ws->rz = static_cast<double>(reinterpret_cast<SolverState<T>*>(static_cast<char*>(c->pinned) + 2048)->rz);
     return stt;
