@@ -1002,10 +1002,12 @@ clsparseStatus build_graph(_clsparseB200Spai* net, const clsparseCsrMatrix* A, c
         pat.num_cols = n;
         pat.num_nonzeros = nnzL;
         pat.row_pointer = gr.Lrp;
+        pat.col_indices = gr.Lcol;
         if (clsparseCsrMetaCreate(&pat, c) != clsparseSuccess) return clsparseOutOfResources;
         gr.metaL = static_cast<matrix_meta*>(pat.meta);
         pat.meta = nullptr;
         pat.row_pointer = gr.LTrp;
+        pat.col_indices = gr.LTrow;
         if (clsparseCsrMetaCreate(&pat, c) != clsparseSuccess) return clsparseOutOfResources;
         gr.metaLT = static_cast<matrix_meta*>(pat.meta);
     }

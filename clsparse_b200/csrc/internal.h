@@ -196,6 +196,11 @@ struct CsrView {
     const matrix_meta* meta;
 };
 
+// Sets *bad (device int, not cleared here) when any of the n column indices
+// at cols is >= ncols (spmv.cu); clsparseCsrMetaCreate's structure check.
+cudaError_t launch_validate_columns(const uint32_t* cols, size_t n, uint32_t ncols, int* bad, int sm_count,
+                                    cudaStream_t s);
+
 // Number of CTAs an SpMV of this matrix launches (sizes epilogue partials).
 uint32_t spmv_num_ctas(const matrix_meta* meta, uint32_t nrows, uint32_t nnz);
 

@@ -237,6 +237,12 @@ clsparseStatus create_meta(clsparseCsrMatrix* csrMatx, clsparseControl control, 
     std::vector<clsparseIdx_t> rp;
     st = read_row_pointer(csrMatx, control, rp);
     if (st != clsparseSuccess) return st;
+    // Structure check before any kernel trusts the matrix: row pointers
+    // monotone (read_row_pointer), spanning exactly num_nonzeros entries, and
+    // every column index below num_cols (device pass below).
+    if (static_cast<size_t>(rp.back() - rp.front()) != static_cast<size_t>(csrMatx->num_nonzeros))
+        return clsparseInvalidValue;
+    if (csrMatx->num_nonzeros > 0 && csrMatx->col_indices == nullptr) return clsparseInvalidMemObject;
 
     if (csrMatx->meta) {
         delete static_cast<matrix_meta*>(csrMatx->meta);
@@ -286,8 +292,20 @@ clsparseStatus create_meta(clsparseCsrMatrix* csrMatx, clsparseControl control, 
     if (e == cudaSuccess)
         e = cudaMemsetAsync(meta->d_lr_ticket, 0, w * sizeof(uint32_t), control->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(meta->d_error, 0, sizeof(int), control->stream);
+    // column indices of the matrix's entries rp[0] .. rp[n] - 1; the flag
+    // borrows the meta's error word, cleared again below
+    if (e == cudaSuccess)
+        e = launch_validate_columns(dev_ptr<const uint32_t>(csrMatx->col_indices, csrMatx->off_col_indices) + rp.front(),
+                                    csrMatx->num_nonzeros, static_cast<uint32_t>(csrMatx->num_cols), meta->d_error,
+                                    meta->sm_count, control->stream);
+    int bad = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, meta->d_error, sizeof(int), cudaMemcpyDeviceToHost, control->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(control->stream);
     if (e != cudaSuccess) return clsparseInvalidKernelExecution;
+    if (bad) return clsparseInvalidValue;
+    if (cudaMemsetAsync(meta->d_error, 0, sizeof(int), control->stream) != cudaSuccess ||
+        cudaStreamSynchronize(control->stream) != cudaSuccess)
+        return clsparseInvalidKernelExecution;
     meta->h_word_nnz = std::move(word_nnz);
     csrMatx->meta = meta.release();
     return clsparseSuccess;

@@ -358,6 +358,38 @@ clsparseStatus csrmv_entry(const clsparseScalar* alpha, const clsparseCsrMatrix*
 
 }  // namespace
 
+// Column-range check of a CSR matrix: sets *bad when any of the n column
+// indices is >= ncols. One pass over the indices (16-byte loads where the
+// buffer is aligned), one flag write per CTA at most.
+__global__ void __launch_bounds__(256) validate_columns_kernel(const uint32_t* __restrict__ cols, size_t n,
+                                                               uint32_t ncols, int* bad) {
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    const size_t tid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    bool out = false;
+    const size_t head = ((16 - (reinterpret_cast<uintptr_t>(cols) & 15u)) & 15u) / 4;
+    const size_t h = head < n ? head : n;
+    for (size_t i = tid; i < h; i += stride) out |= cols[i] >= ncols;
+    const uint4* q = reinterpret_cast<const uint4*>(cols + h);
+    const size_t nq = (n - h) / 4;
+    for (size_t i = tid; i < nq; i += stride) {
+        const uint4 c = __ldcs(q + i);
+        out |= (c.x >= ncols) | (c.y >= ncols) | (c.z >= ncols) | (c.w >= ncols);
+    }
+    for (size_t i = h + 4 * nq + tid; i < n; i += stride) out |= cols[i] >= ncols;
+    if (__syncthreads_or(out) && threadIdx.x == 0) atomicOr(bad, 1);
+}
+
+cudaError_t launch_validate_columns(const uint32_t* cols, size_t n, uint32_t ncols, int* bad, int sm_count,
+                                    cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    size_t grid = (n / 4 + 255) / 256;
+    const size_t cap = static_cast<size_t>(sm_count > 0 ? sm_count : 148) * 8;
+    if (grid > cap) grid = cap;
+    if (grid == 0) grid = 1;
+    validate_columns_kernel<<<static_cast<uint32_t>(grid), 256, 0, s>>>(cols, n, ncols, bad);
+    return cudaGetLastError();
+}
+
 }  // namespace clsp
 
 extern "C" {

@@ -277,3 +277,47 @@ def test_spmv_irregular_full_size(ctrl, orc, dtype):
     s1 = orc.dcsrmv_absscale(rp, col, valc, 1.0, np.asarray(x, t).astype(np.float64), 0.0, y0)
     s2 = orc.dcsrmv_absscale(rp, col, valc, 1.0, np.asarray(x2, t).astype(np.float64), 0.0, y0)
     assert np.all(lin <= 4 * TOL[dtype] * (s1 + s2) + np.finfo(t).tiny)
+
+
+@pytest.mark.parametrize("where", ["first", "middle", "last"])
+def test_meta_create_rejects_out_of_range_column(ctrl, where):
+    """clsparseCsrMetaCreate checks the structure before any kernel trusts
+    it (the reference only checks buffer sizes, in debug builds:
+    src/library/internal/clsparse-validate.cpp:69-133): a column index >=
+    num_cols anywhere -- in the unaligned head, the vectorised body or the
+    tail of the index array -- is clsparseInvalidValue, and nothing is
+    attached to the matrix."""
+    from clsparse_b200 import _lib as L
+    rp, col, val = matgen.random_lengths(np.full(500, 7), 1000, seed=3)
+    col = col.copy()
+    pos = {"first": 0, "middle": len(col) // 2 + 1, "last": len(col) - 1}[where]
+    col[pos] = 1000
+    A = api.CsrMatrix.from_numpy(rp, col, val, num_cols=1000)
+    with pytest.raises(api.ClsparseError) as e:
+        A.create_meta(ctrl)
+    assert e.value.status == L.clsparseInvalidValue
+    assert not A.s.meta
+    col[pos] = 999
+    B = api.CsrMatrix.from_numpy(rp, col, val, num_cols=1000)
+    B.create_meta(ctrl)
+    assert B.s.meta
+
+
+def test_meta_create_rejects_bad_row_pointers(ctrl):
+    from clsparse_b200 import _lib as L
+    rp, col, val = matgen.random_lengths([3, 4, 5], 10, seed=1)
+    bad = rp.copy()
+    bad[1], bad[2] = bad[2], bad[1]  # not monotone
+    A = api.CsrMatrix.from_numpy(bad, col, val, num_cols=10)
+    with pytest.raises(api.ClsparseError) as e:
+        A.create_meta(ctrl)
+    assert e.value.status == L.clsparseInvalidValue
+    # row pointers spanning fewer entries than num_nonzeros
+    A = api.CsrMatrix.from_numpy(rp, col, val, num_cols=10)
+    A.s.num_nonzeros = len(col) - 1
+    with pytest.raises(api.ClsparseError) as e:
+        A.create_meta(ctrl)
+    assert e.value.status == L.clsparseInvalidValue
+    # the same arrays with consistent sizes pass
+    A = api.CsrMatrix.from_numpy(rp, col, val, num_cols=10)
+    A.create_meta(ctrl)
