@@ -268,12 +268,18 @@ def cg_section(ctrl, with_cpu: bool):
         (clsparseDcsrcgLearned); the network is trained on the GPU by the
         library's kernels on 128^2 matrices of the family (different seeds)
         before the timed solves; training time is reported separately.
-    Each solve is timed on its second call (the first captures the graph)."""
+    Each solve is timed on its second call (the first captures the graph).
+    Every solution's error against the FP64 oracle solution is stated
+    (error_vs_fp64_oracle, relative 2-norm): C1 against the serial oracle
+    restatement of the reference CG at the same stop test, C3 / C5 against the
+    oracle's threaded FP64 Jacobi-PCG run to a relative residual of 1e-12,
+    computed on the host after all GPU timings."""
     import torch
     from clsparse_b200 import _lib as L
     from clsparse_b200 import api, learn, matgen
 
     out = {}
+    solutions = {}  # config -> {entry: x on the host}, compared with the oracle at the end
 
     def fp64_cg(A, b, x, l2=True, max_iters=200000):
         def run():
@@ -308,11 +314,13 @@ def cg_section(ctrl, with_cpu: bool):
         import oracle
         rp, col, val = c1
         t0 = time.perf_counter()
-        _, oi = oracle.solve("cg", np.float64, rp, col, val, np.zeros(n), b.cpu().numpy(), 1, 200000, 1e-10, 0.0)
+        xo, oi = oracle.solve("cg", np.float64, rp, col, val, np.zeros(n), b.cpu().numpy(), 1, 200000, 1e-10, 0.0)
         tc = time.perf_counter() - t0
         c1_out["cpu_baseline"] = {"s": round(tc, 3), "iterations": oi.nIters, "cores": 1, "kind": "port",
                                   "sample": "the whole solve, oracle restatement of the reference CG"}
         c1_out["speedup_vs_cpu"] = round(tc / t, 1)
+        xg = x.cpu().numpy()
+        c1_out["error_vs_fp64_oracle"] = float(np.linalg.norm(xg - xo) / np.linalg.norm(xo))
     out["C1"] = c1_out
     del A
 
@@ -325,6 +333,7 @@ def cg_section(ctrl, with_cpu: bool):
     x = torch.zeros(n, dtype=torch.float64, device="cuda")
     t64, i64 = fp64_cg(A, b, x)
     r64 = true_res(c3, x, b)
+    solutions["C3"] = {"fp64_jacobi": x.cpu().numpy()}
 
     def mixed():
         x.zero_()
@@ -333,6 +342,7 @@ def cg_section(ctrl, with_cpu: bool):
         sc.release()
         return r
     tm, im = _timed(mixed)
+    solutions["C3"]["mixed_fp32"] = x.cpu().numpy()
     out["C3"] = {"workload": "3D 7-point log-normal diffusion 128^3 (n=2,097,152, sigma 1.5), rel. L2 residual 1e-10",
                  "fp64_jacobi": {"s": round(t64, 5), "iterations": i64["nIters"] + 1, "true_residual": r64},
                  "mixed_fp32": {"s": round(tm, 5), "inner_iterations": im["innerIterations"],
@@ -376,6 +386,7 @@ def cg_section(ctrl, with_cpu: bool):
     x = torch.zeros(n, dtype=torch.float64, device="cuda")
     t64, i64 = fp64_cg(A, b, x)
     r64 = true_res(c5, x, b)
+    solutions["C5"] = {"fp64_jacobi": x.cpu().numpy()}
 
     def mixed5():
         x.zero_()
@@ -385,6 +396,7 @@ def cg_section(ctrl, with_cpu: bool):
         return r
     tm, im = _timed(mixed5)
     rm = true_res(c5, x, b)
+    solutions["C5"]["mixed_fp32"] = x.cpu().numpy()
     tb0 = time.perf_counter()
     spai.set_matrix(A, ctrl)
     spai.build(ctrl)
@@ -399,6 +411,7 @@ def cg_section(ctrl, with_cpu: bool):
         return r
     tl, il = _timed(learned)
     rl = true_res(c5, x, b)
+    solutions["C5"]["learned_mixed_fp32"] = x.cpu().numpy()
     spai.release()
     out["C5"] = {"workload": "2D GRF diffusion 1024^2 (n=1,048,576, corr 0.05, sigma 2), rel. L2 residual 1e-10",
                  "fp64_jacobi": {"s": round(t64, 5), "iterations": i64["nIters"] + 1, "true_residual": r64},
@@ -410,6 +423,14 @@ def cg_section(ctrl, with_cpu: bool):
                                         "fell_back_to_jacobi": il["fell_back"], "factor_build_s": round(build_s, 3),
                                         "speedup": round(t64 / tl, 3)},
                  "train_s": round(train_s, 2), "train_loss_first_last": [hist[0], hist[-1]]}
+    # errors against the FP64 oracle solutions (host, after every GPU timing)
+    import oracle
+    for name, mat in (("C3", c3), ("C5", c5)):
+        rp, col, val = mat
+        bh = np.random.default_rng(1).uniform(-1, 1, len(rp) - 1)
+        xo, _, _ = oracle.reference_solution(rp, col, val, bh, rel_tol=1e-12)
+        for entry, xs in solutions[name].items():
+            out[name][entry]["error_vs_fp64_oracle"] = float(np.linalg.norm(xs - xo) / np.linalg.norm(xo))
     return out
 
 
