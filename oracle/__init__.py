@@ -1,8 +1,10 @@
 """CPU oracle of the clSPARSE hot path -- test infrastructure only.
 
 Python side of oracle/oracle.c (the project's C restatement of the reference
-algorithms) and of oracle/_ref/librefbins.so (the reference's own
-ComputeRowBlocks compiled from its sources). Only tests, __graft_entry__.smoke()
+algorithms), of oracle/_ref/librefbins.so (the reference's own
+ComputeRowBlocks compiled from its sources) and of oracle/_ref/librefspmv.so
+(the reference's own SpMV kernels, csrmv_adaptive.cl and csrmv_general.cl,
+compiled from its sources and run on host threads through oracle/clc_shim.h). Only tests, __graft_entry__.smoke()
 and bench.py's CPU baseline use this package, as the checker or the timed CPU
 baseline; the product library never imports it.
 """
@@ -17,6 +19,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 _lib = None
 _ref = None
+_refspmv = None
 
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
@@ -156,6 +159,101 @@ def reference_solution(rp, col, val, b, rel_tol=1e-12, max_iters=1_000_000, thre
                              np.ascontiguousarray(val, np.float64), x, np.ascontiguousarray(b, np.float64),
                              int(max_iters), float(rel_tol), int(threads or os.cpu_count() or 1), C.byref(res))
     return x, it, res.value
+
+
+def ref_spmv_lib():
+    """The reference's own SpMV kernels run on the host (oracle/_ref/librefspmv.so,
+    built by oracle/Makefile from src/library/kernels/csrmv_{adaptive,general}.cl),
+    or None where oracle/_ref was not built."""
+    global _refspmv
+    if _refspmv is None:
+        path = HERE / "_ref" / "librefspmv.so"
+        if not path.exists():
+            return None
+        _refspmv = C.CDLL(str(path))
+    return _refspmv
+
+
+def _tag(dtype, extended):
+    return ("d" if np.dtype(dtype) == np.float64 else "s") + ("_ext" if extended else "_plain")
+
+
+def ref_csrmv_adaptive(rp, col, val, x, y, alpha, beta, dtype=np.float64, extended=False):
+    """y = alpha*A*x + beta*y by the reference's csrmv_adaptive kernel
+    (csrmv_adaptive.cl:312-687) with the row blocks of the reference's own
+    ComputeRowBlocks; returns the new y (a copy). Work-groups run one after
+    another on host threads, so large matrices take seconds."""
+    L, R = ref_spmv_lib(), ref_lib()
+    if L is None or R is None:
+        raise RuntimeError("oracle/_ref not built")
+    t = np.dtype(dtype)
+    rp = np.ascontiguousarray(rp, np.uint32)
+    n = len(rp) - 1
+    dry = R.ref_row_blocks_size(rp, n)
+    words = np.zeros(dry // 2 + 1, np.uint64)
+    used = R.ref_row_blocks(rp, n, words, len(words))
+    meta = np.zeros(max(dry, used) + 2, np.uint64)  # the reference's meta buffer: words, then error slots
+    meta[: used // 2] = words[: used // 2]
+    pad = 1024  # BLOCKSIZE: the stream loads read up to a block past the last nonzero
+    cols = np.concatenate([np.asarray(col, np.uint32), np.zeros(pad, np.uint32)])
+    vals = np.concatenate([np.asarray(val, t), np.zeros(pad, t)])
+    xv = np.ascontiguousarray(x, t)
+    yv = np.array(y, dtype=t, copy=True)
+    a = np.array([alpha], t)
+    b = np.array([beta], t)
+    fn = getattr(L, "ref_csrmv_adaptive_" + _tag(t, extended))
+    fn.restype = C.c_int
+    rc = fn(vals.ctypes.data_as(C.c_void_p), cols.ctypes.data_as(C.c_void_p), rp.ctypes.data_as(C.c_void_p),
+            xv.ctypes.data_as(C.c_void_p), yv.ctypes.data_as(C.c_void_p), meta.ctypes.data_as(C.c_void_p),
+            C.c_uint(used), a.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p))
+    if rc != 0:
+        raise RuntimeError(f"reference kernel launch failed ({rc})")
+    return yv
+
+
+def ref_subwave(nnz, nrows, wave_size=64):
+    """The sub-wave width the reference's csrmv_vector picks from the average
+    row length (csrmv-vector.hpp:34-49)."""
+    per_row = nnz // nrows if nrows else 0
+    sw = wave_size
+    if wave_size > 32 and per_row < 64:
+        sw = 32
+    if per_row < 32:
+        sw = 16
+    if per_row < 16:
+        sw = 8
+    if per_row < 8:
+        sw = 4
+    if per_row < 4:
+        sw = 2
+    return sw
+
+
+def ref_csrmv_general(rp, col, val, x, y, alpha, beta, dtype=np.float64, extended=False, subwave=None):
+    """y = alpha*A*x + beta*y by the reference's csrmv_general kernel
+    (csrmv_general.cl:178-259), the path it takes without a meta; returns the
+    new y (a copy)."""
+    L = ref_spmv_lib()
+    if L is None:
+        raise RuntimeError("oracle/_ref not built")
+    t = np.dtype(dtype)
+    rp = np.ascontiguousarray(rp, np.uint32)
+    n = len(rp) - 1
+    sw = subwave or ref_subwave(int(rp[-1] - rp[0]), n)
+    cols = np.ascontiguousarray(col, np.uint32)
+    vals = np.ascontiguousarray(val, t)
+    xv = np.ascontiguousarray(x, t)
+    yv = np.array(y, dtype=t, copy=True)
+    a = np.array([alpha], t)
+    b = np.array([beta], t)
+    fn = getattr(L, f"ref_csrmv_general_{_tag(t, extended)}_sw{sw}")
+    fn.restype = C.c_int
+    rc = fn(C.c_uint(n), rp.ctypes.data_as(C.c_void_p), cols.ctypes.data_as(C.c_void_p),
+            vals.ctypes.data_as(C.c_void_p), xv.ctypes.data_as(C.c_void_p), yv.ctypes.data_as(C.c_void_p),
+            a.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p))
+    if rc != 0:
+        raise RuntimeError(f"reference kernel launch failed ({rc})")
+    return yv
 
 
 def solve(kind, dtype, rp, col, val, x0, b, precond, max_iters, rel_tol, abs_tol, n_iters_in=0):

@@ -6,7 +6,13 @@
  * baseline may load it, and only as the checker or the timed CPU baseline;
  * the product library never calls it. Parity is pinned by
  * tests/golden/rowblocks_*.npz, produced by the reference's own
- * ComputeRowBlocks compiled from its sources (oracle/Makefile -> oracle/_ref/).
+ * ComputeRowBlocks compiled from its sources (oracle/Makefile -> oracle/_ref/),
+ * and, for the SpMV restatements, by tests/golden/spmv_ref.npz: the outputs
+ * of the reference's own csrmv_adaptive / csrmv_general OpenCL kernels,
+ * compiled from its sources and run on the host through oracle/clc_shim.h.
+ * The CG / BiCGStab restatements are not pinned to reference outputs (the
+ * reference's solvers need its OpenCL runtime); they are built from the
+ * pinned SpMV and follow the reference's operation order line by line.
  *
  *   oracle_row_blocks  csr-meta.hpp:93-261 (ComputeRowBlocks, incl. the
  *                      trailing-block quirk) and :263-269 (size-only run)
