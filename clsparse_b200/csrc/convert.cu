@@ -19,6 +19,7 @@
 // Dense matrices: row-major as the reference reads them, column-major
 // honoured, lead_dim as given (0 means packed).
 #include "device_common.cuh"
+#include "scan.cuh"
 #include "internal.h"
 
 namespace clsp {
@@ -132,50 +133,6 @@ __global__ void compact_rows_kernel(const T* __restrict__ D, Dense dv, uint32_t 
             pos += __popc(ball);
         }
     }
-}
-
-// In-place inclusive scan of v[0..n) in three phases: per-block scans (each
-// thread rewrites only its own element) with block totals, an exclusive scan
-// of the block totals by one CTA, and the carries added back. part holds
-// ceil(n / 1024) words.
-__global__ void scan_blocks_kernel(uint32_t* __restrict__ v, uint32_t n, uint32_t* __restrict__ part) {
-    __shared__ uint32_t s[1024];
-    const uint32_t i = blockIdx.x * 1024u + threadIdx.x;
-    s[threadIdx.x] = i < n ? v[i] : 0u;
-    __syncthreads();
-    for (uint32_t off = 1; off < 1024; off <<= 1) {
-        const uint32_t t = threadIdx.x >= off ? s[threadIdx.x - off] : 0u;
-        __syncthreads();
-        s[threadIdx.x] += t;
-        __syncthreads();
-    }
-    if (i < n) v[i] = s[threadIdx.x];
-    if (threadIdx.x == 1023) part[blockIdx.x] = s[1023];
-}
-
-__global__ void scan_parts_kernel(uint32_t* __restrict__ part, uint32_t nparts) {
-    __shared__ uint32_t s[1024];
-    uint32_t carry = 0;
-    for (uint32_t b = 0; b < nparts; b += 1024) {
-        const uint32_t i = b + threadIdx.x;
-        const uint32_t x = i < nparts ? part[i] : 0u;
-        s[threadIdx.x] = x;
-        __syncthreads();
-        for (uint32_t off = 1; off < 1024; off <<= 1) {
-            const uint32_t t = threadIdx.x >= off ? s[threadIdx.x - off] : 0u;
-            __syncthreads();
-            s[threadIdx.x] += t;
-            __syncthreads();
-        }
-        if (i < nparts) part[i] = carry + s[threadIdx.x] - x;
-        carry += s[1023];
-        __syncthreads();
-    }
-}
-
-__global__ void scan_add_kernel(uint32_t* __restrict__ v, uint32_t n, const uint32_t* __restrict__ part) {
-    const uint32_t i = blockIdx.x * 1024u + threadIdx.x;
-    if (i < n) v[i] += part[blockIdx.x];
 }
 
 // y = alpha * A * x + beta * y for a COO matrix sorted by row: G lanes per
@@ -352,9 +309,7 @@ clsparseStatus dense2csr(const cldenseMatrix* A, clsparseCsrMatrix* csr, clspars
     count_rows_kernel<T><<<grid_for(static_cast<uint64_t>(rows) * 32, control->sm_count), kThreads, 0, s>>>(
         D, dv, rows, cols, rp + 1);
     if (rows) {
-        scan_blocks_kernel<<<nparts, 1024, 0, s>>>(rp + 1, rows, part);
-        scan_parts_kernel<<<1, 1024, 0, s>>>(part, nparts);
-        scan_add_kernel<<<nparts, 1024, 0, s>>>(rp + 1, rows, part);
+        scan::inclusive_u32(rp + 1, rows, part, s);
     }
     uint32_t* hv = static_cast<uint32_t*>(control->pinned) + 512;
     cudaMemcpyAsync(hv, rp + rows, 4, cudaMemcpyDeviceToHost, s);

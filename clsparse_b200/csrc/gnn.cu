@@ -40,6 +40,7 @@
 #include "device_common.cuh"
 #include "internal.h"
 #include "pipeline.cuh"
+#include "scan.cuh"
 
 namespace clsp {
 namespace gnn {
@@ -48,7 +49,7 @@ constexpr int H = 64;      // hidden width
 constexpr int HO = 32;     // width of the edge output MLP
 constexpr int NF = 4;      // node input features
 constexpr int NL = 4;      // message-passing layers
-constexpr int kMaxP = 8;   // max entries per row of tril(A) handled by the loss
+constexpr int kMaxTrainP = 32;  // max entries per row of tril(A) for training (local blocks B_i are m x m)
 
 // ---- flat parameter layout ----
 struct Offsets {
@@ -709,6 +710,153 @@ __global__ void node_features(const uint32_t* __restrict__ rp, const uint32_t* _
     }
 }
 
+// ---- graph of a matrix, built on the device
+
+// Status bits of the graph build.
+enum : uint32_t {
+    kGraphNotSpd = 1,     // a row without a positive diagonal entry
+    kGraphBadRows = 2,    // columns unsorted, repeated or out of range, or row_pointer[0] != 0
+    kGraphAsymmetric = 4  // the pattern is not symmetric (an entry (i, j) without (j, i))
+};
+
+// Per row i of A: 1 / sqrt(a_ii), the number of entries with column <= i (a
+// row of L = tril(A)) into Lc[i] and with column >= i (a row of L^T, on the
+// symmetric pattern) into Uc[i]; checks sortedness and the diagonal.
+__global__ void graph_rows(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols,
+                           const double* __restrict__ vals, uint32_t n, double* __restrict__ dinvs,
+                           uint32_t* __restrict__ Lc, uint32_t* __restrict__ Uc, uint32_t* __restrict__ info) {
+    uint32_t bad = 0, maxl = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t b = rp[i], e = rp[i + 1];
+        if (i == 0 && b != 0) bad |= kGraphBadRows;
+        if (e < b) {
+            bad |= kGraphBadRows;
+            Lc[i] = Uc[i] = 0;
+            dinvs[i] = 0.0;
+            continue;
+        }
+        double diag = 0.0;
+        uint32_t lc = 0, uc = 0, prev = 0;
+        for (uint32_t k = b; k < e; ++k) {
+            const uint32_t j = cols[k];
+            if (j >= n || (k > b && j <= prev)) bad |= kGraphBadRows;
+            prev = j;
+            if (j < i) {
+                ++lc;
+            } else if (j == i) {
+                ++lc;
+                ++uc;
+                diag = vals[k];
+            } else {
+                ++uc;
+            }
+        }
+        if (!(diag > 0.0)) bad |= kGraphNotSpd;
+        dinvs[i] = diag > 0.0 ? 1.0 / sqrt(diag) : 0.0;
+        Lc[i] = lc;
+        Uc[i] = uc;
+        maxl = lc > maxl ? lc : maxl;
+    }
+    if (bad) atomicOr(info, bad);
+    if (maxl) atomicMax(info + 1, maxl);
+}
+
+// Scaled values a_hat_ij = a_ij / sqrt(a_ii a_jj) on A's pattern; the rows of
+// L (the first Lrp[i+1] - Lrp[i] entries of A's sorted row i) with their
+// scaled values; the rows of L^T (the entries of A's row i with column >= i:
+// by symmetry, the rows of L holding column i, in increasing order) with the
+// position in L of each (the rank of column i in A's row j, a binary search).
+__global__ void graph_fill(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols,
+                           const double* __restrict__ vals, uint32_t n, const double* __restrict__ dinvs,
+                           const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ LTrp,
+                           float* __restrict__ ehat, uint32_t* __restrict__ Lcol, float* __restrict__ Le,
+                           uint32_t* __restrict__ LTrow, uint32_t* __restrict__ LTidx, uint32_t* __restrict__ info) {
+    uint32_t bad = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t b = rp[i], e = rp[i + 1];
+        const double di = dinvs[i];
+        uint32_t l = Lrp[i], u = LTrp[i];
+        const uint32_t lend = Lrp[i + 1], uend = LTrp[i + 1];
+        for (uint32_t k = b; k < e; ++k) {
+            const uint32_t j = cols[k];
+            const float eh = static_cast<float>(vals[k] * di * dinvs[j]);
+            ehat[k] = eh;
+            if (j <= i && l < lend) {
+                Lcol[l] = j;
+                Le[l] = eh;
+                ++l;
+            }
+            if (j >= i && u < uend) {
+                // entry (j, i) of L: column i in A's row j, lower entries first
+                const uint32_t jb = rp[j], je = rp[j + 1];
+                uint32_t lo = jb, hi = je;
+                while (lo < hi) {
+                    const uint32_t mid = lo + (hi - lo) / 2;
+                    if (cols[mid] < i)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                if (lo == je || cols[lo] != i) {
+                    bad |= kGraphAsymmetric;
+                    LTidx[u] = Lrp[j];
+                } else {
+                    LTidx[u] = Lrp[j] + (lo - jb);
+                }
+                LTrow[u] = j;
+                ++u;
+            }
+        }
+    }
+    if (bad) atomicOr(info, bad);
+}
+
+// Squared norm of one probe vector (a grid sum into out).
+__global__ void probe_norm(const float* __restrict__ v, uint32_t n, double* parts, uint32_t* ticket,
+                           double* out) {
+    double acc[1] = {0.0};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        acc[0] += static_cast<double>(v[i]) * v[i];
+    double tot[1];
+    if (dev::grid_reduce_last<1>(acc, parts, ticket, tot) && threadIdx.x == 0) out[0] = tot[0];
+}
+
+// m_i^2 per row (the size of the local block B_i), for the block offsets.
+__global__ void block_sizes(const uint32_t* __restrict__ Lrp, uint32_t n, uint32_t* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t m = Lrp[i + 1] - Lrp[i];
+        out[i] = m * m;
+    }
+}
+
+// Local blocks of the Kaporin loss: B_i = A_hat[P_i, P_i] with P_i the
+// columns of row i of L (a binary search in A's row P_a for column P_b).
+__global__ void block_fill(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols,
+                           const float* __restrict__ ehat, const uint32_t* __restrict__ Lrp,
+                           const uint32_t* __restrict__ Lcol, const uint32_t* __restrict__ Boff, uint32_t n,
+                           float* __restrict__ B) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t k0 = Lrp[i], m = Lrp[i + 1] - k0;
+        float* Bi = B + Boff[i];
+        for (uint32_t a = 0; a < m; ++a) {
+            const uint32_t r = Lcol[k0 + a];
+            const uint32_t rb = rp[r], re = rp[r + 1];
+            for (uint32_t c = 0; c < m; ++c) {
+                const uint32_t col = Lcol[k0 + c];
+                uint32_t lo = rb, hi = re;
+                while (lo < hi) {
+                    const uint32_t mid = lo + (hi - lo) / 2;
+                    if (cols[mid] < col)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                Bi[a * m + c] = (lo < re && cols[lo] == col) ? ehat[lo] : 0.f;
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------- host side
 
 constexpr int kRows = 16;  // rows per CTA of linear_fwd / linear_bwd
@@ -734,7 +882,12 @@ uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934665603u
 // the local blocks of the loss, and the exported factor.
 struct Graph {
     uint32_t n = 0, nnz = 0, nnzL = 0;
-    size_t nB = 0;
+    uint32_t cap_n = 0, cap_nnz = 0;  // sizes the buffers were allocated for (rows, entries of A)
+    uint32_t maxL = 0;                // longest row of L
+    size_t nB = 0, cap_B = 0;         // local blocks (training only, built on first use)
+    bool blocks_built = false;
+    uint32_t* scan_part = nullptr;    // block totals of the device scans
+    uint32_t* info = nullptr;         // [0] status bits, [1] longest row of L, [2..3] sizes read back
     const uint32_t* rp = nullptr;   // A's arrays (user memory)
     const uint32_t* cols = nullptr;
     float* ehat = nullptr;          // a_hat on A's pattern
@@ -770,7 +923,8 @@ struct Graph {
         delete metaL;
         delete metaLT;
         void* ptrs[] = {ehat, dinvs, Lrp, Lcol, Le, LTrp, LTrow, LTidx, Boff, B, F, Hp, Hq, g, dg, dH, dHn, dS,
-                        dHu, dHp, dHq, part, pw, pu, pv, pdv, pdu, red, ticket, G32, GT32, G16, GT16, G64, GT64};
+                        dHu, dHp, dHq, part, pw, pu, pv, pdv, pdu, red, ticket, G32, GT32, G16, GT16, G64, GT64,
+                        scan_part, info};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (int l = 0; l <= NL; ++l)
@@ -864,100 +1018,20 @@ clsparseStatus read_host_csr(const clsparseCsrMatrix* A, clsparseControl c, Host
     return cudaStreamSynchronize(s) == cudaSuccess ? clsparseSuccess : clsparseInvalidMemObject;
 }
 
-// Builds the graph structures of an SPD matrix A (FP64 values, sorted
-// columns, every diagonal present, at most kMaxP entries per row of tril(A))
-// from its host copy h.
-clsparseStatus build_graph(_clsparseB200Spai* net, const clsparseCsrMatrix* A, clsparseControl c,
-                           const HostCsr& h) {
-    Graph& gr = net->gr;
+// Allocates the graph's buffers for n rows and nnz entries of A (L and L^T
+// hold at most nnz entries), or keeps the present ones when they are large
+// enough: a network set to one matrix after another of the same size
+// allocates once. The local blocks of the loss are allocated on first use.
+bool ensure_graph_buffers(Graph& gr, uint32_t n, uint32_t nnz) {
+    if (gr.ehat != nullptr && gr.cap_n >= n && gr.cap_nnz >= nnz) return true;
     gr.release();
-    const uint32_t n = A->num_rows, nnz = A->num_nonzeros;
-    const std::vector<uint32_t>& rp = h.rp;
-    const std::vector<uint32_t>& cols = h.cols;
-    const std::vector<double>& vals = h.vals;
-    cudaStream_t s = c->stream;
-    const uint32_t base = rp[0];
-    std::vector<double> dinv(n, 0.0);
-    for (uint32_t i = 0; i < n; ++i) {
-        for (uint32_t k = rp[i]; k < rp[i + 1]; ++k)
-            if (cols[k - base] == i) dinv[i] = vals[k - base];
-        if (!(dinv[i] > 0.0)) return clsparseInvalidValue;  // not SPD (missing or non-positive diagonal)
-        dinv[i] = 1.0 / std::sqrt(dinv[i]);
-    }
-    std::vector<float> ehat(nnz);
-    std::vector<uint32_t> Lrp(n + 1, 0), Lcol, Lsrc;
-    for (uint32_t i = 0; i < n; ++i) {
-        uint32_t prev = 0;
-        bool first = true;
-        for (uint32_t k = rp[i]; k < rp[i + 1]; ++k) {
-            const uint32_t j = cols[k - base];
-            if (j >= n) return clsparseInvalidValue;
-            if (!first && j <= prev) return clsparseInvalidValue;  // columns must be sorted, unique
-            first = false;
-            prev = j;
-            ehat[k - base] = static_cast<float>(vals[k - base] * dinv[i] * dinv[j]);
-            if (j <= i) {
-                Lcol.push_back(j);
-                Lsrc.push_back(k - base);
-            }
-        }
-        Lrp[i + 1] = static_cast<uint32_t>(Lcol.size());
-        if (Lrp[i + 1] - Lrp[i] > static_cast<uint32_t>(kMaxP)) return clsparseInvalidValue;
-        if (Lrp[i + 1] == Lrp[i] || Lcol.back() != i) return clsparseInvalidValue;
-    }
-    const uint32_t nnzL = Lrp[n];
-    std::vector<float> Le(nnzL);
-    for (uint32_t k = 0; k < nnzL; ++k) Le[k] = ehat[Lsrc[k]];
-    // transpose of L
-    std::vector<uint32_t> LTrp(n + 1, 0), LTrow(nnzL), LTidx(nnzL);
-    for (uint32_t k = 0; k < nnzL; ++k) ++LTrp[Lcol[k] + 1];
-    for (uint32_t j = 0; j < n; ++j) LTrp[j + 1] += LTrp[j];
-    {
-        std::vector<uint32_t> fill(LTrp.begin(), LTrp.end() - 1);
-        for (uint32_t i = 0; i < n; ++i)
-            for (uint32_t k = Lrp[i]; k < Lrp[i + 1]; ++k) {
-                const uint32_t pos = fill[Lcol[k]]++;
-                LTrow[pos] = i;
-                LTidx[pos] = k;
-            }
-    }
-    // local blocks B_i = A_hat[P_i, P_i]
-    std::vector<uint32_t> Boff(n + 1, 0);
-    for (uint32_t i = 0; i < n; ++i) {
-        const uint32_t m = Lrp[i + 1] - Lrp[i];
-        Boff[i + 1] = Boff[i] + m * m;
-    }
-    std::vector<float> B(Boff[n]);
-    auto ahat_at = [&](uint32_t r, uint32_t col) -> float {
-        uint32_t lo = rp[r] - base, hi = rp[r + 1] - base;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) / 2;
-            if (cols[mid] < col)
-                lo = mid + 1;
-            else
-                hi = mid;
-        }
-        return (lo < rp[r + 1] - base && cols[lo] == col) ? ehat[lo] : 0.f;
-    };
-    for (uint32_t i = 0; i < n; ++i) {
-        const uint32_t k0 = Lrp[i], m = Lrp[i + 1] - k0;
-        for (uint32_t a = 0; a < m; ++a)
-            for (uint32_t b2 = 0; b2 < m; ++b2) B[Boff[i] + a * m + b2] = ahat_at(Lcol[k0 + a], Lcol[k0 + b2]);
-    }
-
-    gr.n = n;
-    gr.nnz = nnz;
-    gr.nnzL = nnzL;
-    gr.nB = Boff[n];
-    gr.rp = dev_ptr<const uint32_t>(A->row_pointer, A->off_row_pointer);
-    gr.cols = dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices);
-    gr.device = c->device;
+    const uint32_t nl = nnz;
     bool ok = dalloc(gr.ehat, nnz) == cudaSuccess && dalloc(gr.dinvs, n) == cudaSuccess &&
-              dalloc(gr.Lrp, n + 1) == cudaSuccess && dalloc(gr.Lcol, nnzL) == cudaSuccess &&
-              dalloc(gr.Le, nnzL) == cudaSuccess && dalloc(gr.LTrp, n + 1) == cudaSuccess &&
-              dalloc(gr.LTrow, nnzL) == cudaSuccess && dalloc(gr.LTidx, nnzL) == cudaSuccess &&
-              dalloc(gr.Boff, n + 1) == cudaSuccess && dalloc(gr.B, gr.nB) == cudaSuccess &&
-              dalloc(gr.F, size_t(n) * NF) == cudaSuccess;
+              dalloc(gr.Lrp, n + 1) == cudaSuccess && dalloc(gr.Lcol, nl) == cudaSuccess &&
+              dalloc(gr.Le, nl) == cudaSuccess && dalloc(gr.LTrp, n + 1) == cudaSuccess &&
+              dalloc(gr.LTrow, nl) == cudaSuccess && dalloc(gr.LTidx, nl) == cudaSuccess &&
+              dalloc(gr.Boff, n + 1) == cudaSuccess && dalloc(gr.F, size_t(n) * NF) == cudaSuccess &&
+              dalloc(gr.scan_part, scan::parts_for(n) + 1) == cudaSuccess && dalloc(gr.info, 4) == cudaSuccess;
     const size_t nh = size_t(n) * H, nho = size_t(n) * HO;
     for (int l = 0; l <= NL && ok; ++l) ok = dalloc(gr.Hs[l], nh) == cudaSuccess;
     for (int l = 0; l < NL && ok; ++l)
@@ -966,7 +1040,7 @@ clsparseStatus build_graph(_clsparseB200Spai* net, const clsparseCsrMatrix* A, c
     const size_t tiles = nblk(n, kRows);
     gr.part_floats = std::max({tiles * size_t(H * 2 * H + H), size_t(n) * 2 * H, size_t(n) * kOutPart});
     ok = ok && dalloc(gr.Hp, nho) == cudaSuccess && dalloc(gr.Hq, nho) == cudaSuccess &&
-         dalloc(gr.g, nnzL) == cudaSuccess && dalloc(gr.dg, nnzL) == cudaSuccess &&
+         dalloc(gr.g, nl) == cudaSuccess && dalloc(gr.dg, nl) == cudaSuccess &&
          dalloc(gr.dH, nh) == cudaSuccess && dalloc(gr.dHn, nh) == cudaSuccess &&
          dalloc(gr.dS, nh) == cudaSuccess && dalloc(gr.dHu, nh) == cudaSuccess &&
          dalloc(gr.dHp, nho) == cudaSuccess && dalloc(gr.dHq, nho) == cudaSuccess &&
@@ -974,33 +1048,75 @@ clsparseStatus build_graph(_clsparseB200Spai* net, const clsparseCsrMatrix* A, c
          dalloc(gr.pu, n) == cudaSuccess && dalloc(gr.pv, n) == cudaSuccess &&
          dalloc(gr.pdv, n) == cudaSuccess && dalloc(gr.pdu, n) == cudaSuccess &&
          dalloc(gr.red, 8 + 2 * kMaxReduceCtas) == cudaSuccess && dalloc(gr.ticket, 4) == cudaSuccess &&
-         dalloc(gr.G32, nnzL) == cudaSuccess && dalloc(gr.GT32, nnzL) == cudaSuccess &&
-         dalloc(gr.G16, nnzL) == cudaSuccess && dalloc(gr.GT16, nnzL) == cudaSuccess &&
-         dalloc(gr.G64, nnzL) == cudaSuccess && dalloc(gr.GT64, nnzL) == cudaSuccess;
+         dalloc(gr.G32, nl) == cudaSuccess && dalloc(gr.GT32, nl) == cudaSuccess &&
+         dalloc(gr.G16, nl) == cudaSuccess && dalloc(gr.GT16, nl) == cudaSuccess &&
+         dalloc(gr.G64, nl) == cudaSuccess && dalloc(gr.GT64, nl) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         gr.release();
-        return clsparseOutOfResources;
+        return false;
     }
-    cudaMemcpyAsync(gr.ehat, ehat.data(), size_t(nnz) * 4, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(gr.dinvs, dinv.data(), size_t(n) * 8, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(gr.Lrp, Lrp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(gr.Lcol, Lcol.data(), size_t(nnzL) * 4, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(gr.Le, Le.data(), size_t(nnzL) * 4, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(gr.LTrp, LTrp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(gr.LTrow, LTrow.data(), size_t(nnzL) * 4, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(gr.LTidx, LTidx.data(), size_t(nnzL) * 4, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(gr.Boff, Boff.data(), (n + 1) * 4, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(gr.B, B.data(), gr.nB * 4, cudaMemcpyHostToDevice, s);
+    gr.cap_n = n;
+    gr.cap_nnz = nnz;
+    return true;
+}
+
+// Reads the graph build's status words (and the two sizes copied next to
+// them) back to the host.
+bool read_info(Graph& gr, cudaStream_t s, uint32_t (&h)[4]) {
+    return cudaMemcpyAsync(h, gr.info, sizeof(h), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+           cudaStreamSynchronize(s) == cudaSuccess;
+}
+
+// Builds the graph structures of an SPD matrix A (FP64 values, sorted
+// columns, every diagonal present, symmetric pattern, row_pointer[0] == 0) on
+// the device: the scaled values, L = tril(A) and L^T with the positions of
+// L^T's entries in L, the node features, and the CSR-Adaptive metas of L and
+// L^T. The work is a row pass, two scans, a second row pass (no host copy of
+// A); the host reads back a few words to size and check the result.
+clsparseStatus build_graph(_clsparseB200Spai* net, const clsparseCsrMatrix* A, clsparseControl c) {
+    Graph& gr = net->gr;
+    const uint32_t n = A->num_rows, nnz = A->num_nonzeros;
+    cudaStream_t s = c->stream;
+    delete gr.metaL;
+    delete gr.metaLT;
+    gr.metaL = gr.metaLT = nullptr;
+    gr.built = false;
+    gr.blocks_built = false;
+    if (!ensure_graph_buffers(gr, n, nnz)) return clsparseOutOfResources;
+    gr.n = n;
+    gr.nnz = nnz;
+    gr.rp = dev_ptr<const uint32_t>(A->row_pointer, A->off_row_pointer);
+    gr.cols = dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices);
+    const double* vals = dev_ptr<const double>(A->values, A->off_values);
+    gr.device = c->device;
+    const uint32_t grid = std::min<uint32_t>(nblk(n, 256), static_cast<uint32_t>(std::max(c->sm_count, 1)) * 8);
+    cudaMemsetAsync(gr.info, 0, 16, s);
+    cudaMemsetAsync(gr.Lrp, 0, 4, s);
+    cudaMemsetAsync(gr.LTrp, 0, 4, s);
+    graph_rows<<<grid, 256, 0, s>>>(gr.rp, gr.cols, vals, n, gr.dinvs, gr.Lrp + 1, gr.LTrp + 1, gr.info);
+    scan::inclusive_u32(gr.Lrp + 1, n, gr.scan_part, s);
+    scan::inclusive_u32(gr.LTrp + 1, n, gr.scan_part, s);
+    cudaMemcpyAsync(gr.info + 2, gr.Lrp + n, 4, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(gr.info + 3, gr.LTrp + n, 4, cudaMemcpyDeviceToDevice, s);
+    uint32_t h[4];
+    if (cudaGetLastError() != cudaSuccess || !read_info(gr, s, h)) return clsparseInvalidKernelExecution;
+    // not SPD, unsorted or out-of-range columns, or an asymmetric pattern
+    if (h[0] != 0 || h[2] != h[3] || h[2] > nnz) return clsparseInvalidValue;
+    gr.nnzL = h[2];
+    gr.maxL = h[1];
+    graph_fill<<<grid, 256, 0, s>>>(gr.rp, gr.cols, vals, n, gr.dinvs, gr.Lrp, gr.LTrp, gr.ehat, gr.Lcol, gr.Le,
+                                    gr.LTrow, gr.LTidx, gr.info);
     cudaMemsetAsync(gr.ticket, 0, 16, s);
     node_features<<<nblk(n, 256), 256, 0, s>>>(gr.rp, gr.cols, gr.ehat, gr.F, n);
-    if (cudaStreamSynchronize(s) != cudaSuccess) return clsparseInvalidKernelExecution;
+    if (cudaGetLastError() != cudaSuccess || !read_info(gr, s, h)) return clsparseInvalidKernelExecution;
+    if (h[0] != 0) return clsparseInvalidValue;
     {
         clsparseCsrMatrix pat;
         std::memset(&pat, 0, sizeof(pat));
         pat.num_rows = n;
         pat.num_cols = n;
-        pat.num_nonzeros = nnzL;
+        pat.num_nonzeros = gr.nnzL;
         pat.row_pointer = gr.Lrp;
         pat.col_indices = gr.Lcol;
         if (clsparseCsrMetaCreate(&pat, c) != clsparseSuccess) return clsparseOutOfResources;
@@ -1012,6 +1128,38 @@ clsparseStatus build_graph(_clsparseB200Spai* net, const clsparseCsrMatrix* A, c
         gr.metaLT = static_cast<matrix_meta*>(pat.meta);
     }
     gr.built = true;
+    return clsparseSuccess;
+}
+
+// The local blocks B_i of the Kaporin loss, built on the first training use
+// of a graph (the factor build does not need them). Rows of L longer than
+// kMaxTrainP entries are refused (the blocks grow as the square).
+clsparseStatus ensure_blocks(Graph& gr, cudaStream_t s) {
+    if (gr.blocks_built) return clsparseSuccess;
+    if (gr.maxL > static_cast<uint32_t>(kMaxTrainP)) return clsparseInvalidValue;
+    if (static_cast<uint64_t>(gr.n) * gr.maxL * gr.maxL >= (1ull << 32)) return clsparseInvalidSize;
+    const uint32_t n = gr.n;
+    cudaMemsetAsync(gr.Boff, 0, 4, s);
+    block_sizes<<<nblk(n, 256), 256, 0, s>>>(gr.Lrp, n, gr.Boff + 1);
+    scan::inclusive_u32(gr.Boff + 1, n, gr.scan_part, s);
+    cudaMemcpyAsync(gr.info + 2, gr.Boff + n, 4, cudaMemcpyDeviceToDevice, s);
+    uint32_t h[4];
+    if (cudaGetLastError() != cudaSuccess || !read_info(gr, s, h)) return clsparseInvalidKernelExecution;
+    const size_t nB = h[2];
+    if (nB > gr.cap_B) {
+        if (gr.B) cudaFree(gr.B);
+        gr.B = nullptr;
+        gr.cap_B = 0;
+        if (dalloc(gr.B, nB) != cudaSuccess) {
+            cudaGetLastError();
+            return clsparseOutOfResources;
+        }
+        gr.cap_B = nB;
+    }
+    gr.nB = nB;
+    block_fill<<<nblk(n, 128), 128, 0, s>>>(gr.rp, gr.cols, gr.ehat, gr.Lrp, gr.Lcol, gr.Boff, n, gr.B);
+    if (cudaGetLastError() != cudaSuccess) return clsparseInvalidKernelExecution;
+    gr.blocks_built = true;
     return clsparseSuccess;
 }
 
@@ -1098,14 +1246,14 @@ double loss_and_dg(_clsparseB200Spai* net, const float* probes, int K, double la
     cudaMemsetAsync(gr.red + 2, 0, sizeof(double), s);
     std::vector<double> rnorm(K, 0.0);
     if (K > 0 && lambda > 0.0) {
-        // host norms of the probes (small K)
-        std::vector<float> hp(size_t(n) * K);
-        cudaMemcpyAsync(hp.data(), probes, hp.size() * 4, cudaMemcpyDeviceToHost, s);
-        cudaStreamSynchronize(s);
-        for (int k = 0; k < K; ++k) {
-            double a = 0.0;
-            for (uint32_t i = 0; i < n; ++i) a += double(hp[size_t(k) * n + i]) * hp[size_t(k) * n + i];
-            rnorm[k] = a;
+        // squared norms of the probes on the device, K words read back
+        double* dnorm = gr.red + 4;  // [4..7]; red[0..3] hold the loss sums
+        for (int k0 = 0; k0 < K; k0 += 4) {
+            const int kk = std::min(4, K - k0);
+            for (int k = 0; k < kk; ++k)
+                probe_norm<<<rg, 256, 0, s>>>(probes + size_t(k0 + k) * n, n, parts, gr.ticket, dnorm + k);
+            cudaMemcpyAsync(rnorm.data() + k0, dnorm, size_t(kk) * sizeof(double), cudaMemcpyDeviceToHost, s);
+            cudaStreamSynchronize(s);
         }
         for (int k = 0; k < K; ++k) {
             if (!(rnorm[k] > 0.0)) continue;
@@ -1242,6 +1390,12 @@ clsparseStatus clsparseB200SpaiSetMatrix(clsparseB200Spai net, const clsparseCsr
     if (st != clsparseSuccess) return st;
     if (!A || A->num_rows != A->num_cols || A->num_rows == 0) return clsparseInvalidSystemSize;
     DeviceGuard g(control->device);
+    if (A->num_rows > kGraphCacheRows || !graph_cache_enabled()) {
+        // Large matrices are built straight from the device arrays, every
+        // time (a rebuild reuses the buffers), with no host copy of A.
+        net->cur = HostCsr();
+        return build_graph(net, A, control);
+    }
     HostCsr h;
     st = read_host_csr(A, control, h);
     if (st != clsparseSuccess) return st;
@@ -1275,7 +1429,7 @@ clsparseStatus clsparseB200SpaiSetMatrix(clsparseB200Spai net, const clsparseCsr
         }
     }
     net->cur = std::move(h);
-    st = build_graph(net, A, control, net->cur);
+    st = build_graph(net, A, control);
     if (st != clsparseSuccess) net->cur = HostCsr();
     return st;
 }
@@ -1299,6 +1453,8 @@ clsparseStatus clsparseB200SpaiLossGrad(clsparseB200Spai net, const cldenseVecto
     if (st != clsparseSuccess) return st;
     if (K > 0 && (!probes || probes->num_values < size_t(K) * net->gr.n)) return clsparseInvalidSize;
     DeviceGuard g(control->device);
+    st = ensure_blocks(net->gr, control->stream);
+    if (st != clsparseSuccess) return st;
     const int bf16 = fp32Weights ? 0 : 1;
     forward(net, bf16, control->stream);
     const double L = loss_and_dg(net, K > 0 ? dev_ptr<const float>(probes->values, probes->off_values) : nullptr,

@@ -156,12 +156,17 @@ typedef struct _clsparseB200Spai* clsparseB200Spai;
 CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiCreate(clsparseB200Spai* spai, cl_ulong seed);
 CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiRelease(clsparseB200Spai spai);
 /* Prepares the graph of A (FP64 values, sorted columns, positive diagonal,
- * at most 8 entries per row of tril(A)) for training or building G. A's
+ * symmetric pattern, row_pointer[0] == 0) for training or building G; the
+ * graph is built on the device (no host copy of A beyond the cache key
+ * below). clsparseInvalidValue if A does not qualify. Building G takes rows
+ * of tril(A) of any length; training (LossGrad / TrainStep) takes at most 32
+ * entries per row of tril(A) and returns clsparseInvalidValue beyond. A's
  * arrays must stay valid while the network uses them. The graphs of up to 8
  * earlier matrices of at most 65,536 rows are kept (device memory, freed by
  * clsparseB200SpaiRelease) and reused when a matrix with the same device
- * addresses and bit-identical arrays is set again; call
- * clsparseB200SpaiBuild after setting a matrix before using G. */
+ * addresses and bit-identical arrays is set again; larger matrices are
+ * rebuilt on every call, into the same buffers when they are large enough.
+ * Call clsparseB200SpaiBuild after setting a matrix before using G. */
 CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiSetMatrix(clsparseB200Spai spai, const clsparseCsrMatrix* A,
                                                          clsparseControl control);
 /* Reads (toDevice = 0) or writes (1) the flat FP32 parameter vector; *count

@@ -195,3 +195,87 @@ def test_training_same_with_and_without_graph_cache(ctrl, monkeypatch):
     s1.release()
     s0.release()
     assert h1 == h0
+
+
+def laplacian27(m, seed=0):
+    """3D 27-point operator on an m^3 grid: every neighbour at Chebyshev
+    distance 1 couples with a positive random weight, the diagonal is the sum
+    of the row's weights plus a margin (SPD, 14 entries per row of tril(A))."""
+    n = m ** 3
+    idx = np.arange(n).reshape(m, m, m)
+    rng = np.random.default_rng(seed)
+    rows, cols = [], []
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                if (dz, dy, dx) == (0, 0, 0):
+                    continue
+                src = idx[max(0, -dz):m - max(0, dz), max(0, -dy):m - max(0, dy), max(0, -dx):m - max(0, dx)]
+                dst = idx[max(0, dz):m - max(0, -dz), max(0, dy):m - max(0, -dy), max(0, dx):m - max(0, -dx)]
+                rows.append(src.ravel())
+                cols.append(dst.ravel())
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    lo = np.minimum(r, c)
+    hi = np.maximum(r, c)
+    w = rng.uniform(0.5, 1.5, len(r))
+    key = lo.astype(np.int64) * n + hi
+    _, first = np.unique(key, return_index=True)
+    wsym = dict(zip(key[first].tolist(), w[first].tolist()))
+    vals = -np.array([wsym[k] for k in key.tolist()])
+    off = sp.csr_matrix((vals, (r, c)), shape=(n, n))
+    d = -np.asarray(off.sum(axis=1)).ravel() + 0.05
+    M = (off + sp.diags(d)).tocsr()
+    M.sort_indices()
+    return M.indptr.astype(np.uint32), M.indices.astype(np.uint32), M.data
+
+
+def test_27_point_stencil_trains_builds_and_solves(ctrl):
+    """Rows of tril(A) with 14 entries: the device graph build takes them, the
+    network trains on them (local blocks of 14 x 14), and the learned solve
+    reaches the FP64 residual."""
+    rp, col, val = laplacian27(12, seed=3)
+    n = len(rp) - 1
+    assert max(np.diff(sp.tril(sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64)))).tocsr().indptr)) == 14
+    A = api.CsrMatrix.from_numpy(rp, col, val)
+    A.create_meta(ctrl)
+    spai = api.Spai(17)
+    spai.set_matrix(A, ctrl)
+    losses = [spai.train_step(ctrl, lr=2e-3) for _ in range(40)]
+    assert np.mean(losses[-5:]) < losses[0]
+    spai.build(ctrl)
+    frp, fcol, G = spai.factor()
+    T = sp.tril(sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64)))).tocsr()
+    assert np.array_equal(frp.astype(np.int64), T.indptr) and np.array_equal(fcol.astype(np.int64), T.indices)
+    b = np.random.default_rng(2).uniform(-1, 1, n)
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    sc = api.SolverControl(L.DIAGONAL, 50000, 1e-10, 0.0)
+    info = api.cg_learned(x, A, torch.tensor(b, device="cuda"), sc, spai, ctrl, inner="fp32", inner_tol=0.3)
+    sc.release()
+    spai.release()
+    Ao = sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64)))
+    assert info["converged"] == 1
+    assert np.linalg.norm(b - Ao @ x.cpu().numpy()) / np.linalg.norm(b) <= 1.5e-10
+
+
+def test_device_graph_build_rejects_unsuitable_matrices(ctrl):
+    """The graph is built on the device; matrices it cannot take are refused
+    with clsparseInvalidValue: an asymmetric pattern, a non-positive
+    diagonal."""
+    rp, col, val = matgen.poisson2d(8)
+    M = sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64))).tolil()
+    M[0, 20] = -0.01  # (0, 20) without (20, 0)
+    M = M.tocsr()
+    M.sort_indices()
+    for bad in (M, None):
+        if bad is None:
+            v = val.copy()
+            v[0] = -1.0  # a_00 < 0
+            A = api.CsrMatrix.from_numpy(rp, col, v)
+        else:
+            A = api.CsrMatrix.from_numpy(bad.indptr.astype(np.uint32), bad.indices.astype(np.uint32), bad.data)
+        spai = api.Spai(1)
+        with pytest.raises(api.ClsparseError) as e:
+            spai.set_matrix(A, ctrl)
+        assert e.value.status == L.clsparseInvalidValue
+        spai.release()
