@@ -1,0 +1,612 @@
+// Banded inner solves of the mixed-precision refinement (project extension,
+// no reference counterpart; the reference's CG loop it replaces for these
+// matrices is src/library/solvers/conjugate-gradients.hpp:162-226).
+//
+// Storage. Stencil and banded matrices -- the 5- and 7-point operators of
+// the configured workloads and the learned factor G on tril(A) of them --
+// have a handful of distinct column offsets j - i. The refinement already
+// solves its inner systems on a private low-precision copy of A's values;
+// when A has at most kMaxDiags distinct offsets (and fills at least half of
+// those diagonals), that copy is laid out by diagonal instead of in CSR:
+// values [d][i] for the d-th offset in increasing order, zero where the
+// diagonal leaves the matrix, and no column indices or row pointers (DIA
+// storage; N. Bell and M. Garland, SC'09). On the 1024^2 five-point matrix
+// this is 21 MB of FP32 values against 46 MB for FP32 CSR; G and G^T (three
+// diagonals, BF16) are 6.3 MB each. The whole inner iteration's working set
+// then fits in the 126 MB L2.
+//
+// Engine. One cooperative launch per inner solve; every CTA owns a
+// contiguous slice of rows and every thread a strided set of them. Grid
+// exchanges (grid_sync.cuh) carry the dot products, so every CTA computes
+// bitwise the same alpha, beta and stop decision. Vectors written inside the
+// launch and read at neighbouring rows by other CTAs are double-buffered
+// (p, and r for the learned factor) so that a phase can form a neighbour's
+// new value itself instead of waiting for it:
+//
+//   Jacobi / none (2 exchanges per iteration)
+//     A: p_new = z + beta p_old, q = A p_new (neighbours' p_new formed on the
+//        fly), <p_new, q>                                  -> exchange: alpha
+//     B: x += alpha p_new, r -= alpha q, z = D^-1 r, <r,r>, <r,z>
+//                                                   -> exchange: stop, beta
+//   learned M^-1 = G^T G (2 exchanges per iteration)
+//     A: as above                                          -> exchange: alpha
+//     B: x += alpha p_new, r_new = r - alpha q into the other r buffer,
+//        z = G^T (G r_new) with the neighbours' (G r_new)_j and their r_new
+//        formed on the fly, <r_new, r_new>, ||G r_new||^2 = <r_new, z>
+//                                                   -> exchange: stop, beta
+//
+// Arithmetic: values and vectors FP32 (BF16 values widened), FMA
+// accumulation in FP32 in increasing column order, dot products accumulated
+// in FP64 -- the precision contract of the CSR inner solves. The stop test
+// is the inner solve's: ||r|| <= tol ||r_0|| (L2, recursive residual), or
+// maxIters. A continued solve (residual replacement) starts from x = 0 and
+// r = b and keeps the previous solve's last direction:
+// p = z + (<r,z> / rz_prev) p_prev.
+//
+// Safety: every barrier wait is bounded (grid_sync.cuh); a timeout leaves
+// the kernel through every CTA and is reported as the barrier-timeout status.
+#include <algorithm>
+#include <climits>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "device_common.cuh"
+#include "dia.h"
+#include "fused.h"
+#include "grid_sync.cuh"
+#include "internal.h"
+#include "solver_state.cuh"
+
+namespace clsp {
+namespace {
+
+constexpr int kSlots = 64;  // hash set of offsets (power of two, > kMaxDiags)
+// empty slot: every byte 0x80 (what cudaMemsetAsync writes), below any
+// offset j - i a matrix of fewer than 2^31 rows has
+constexpr int32_t kEmpty = static_cast<int32_t>(0x80808080u);
+// Threads per CTA of the persistent kernel (two CTAs per SM at 512).
+#ifndef CLSP_DIA_THREADS
+#define CLSP_DIA_THREADS 512
+#endif
+constexpr int kDiaThreads = CLSP_DIA_THREADS;
+constexpr int kDiaCtasPerSm = 1024 / kDiaThreads;
+
+__device__ __forceinline__ uint32_t slot_of(int32_t o) { return (static_cast<uint32_t>(o) * 2654435761u) >> 26; }
+
+// Inserts o into an open-addressed set of kSlots entries; false when full.
+// A plain read finds offsets already present without an atomic.
+__device__ bool set_insert(int32_t* table, int32_t o) {
+    uint32_t h = slot_of(o);
+    for (int probe = 0; probe < kSlots; ++probe) {
+        const int32_t cur = *reinterpret_cast<volatile int32_t*>(table + h);
+        if (cur == o) return true;
+        if (cur == kEmpty) {
+            const int32_t old = atomicCAS(table + h, kEmpty, o);
+            if (old == kEmpty || old == o) return true;
+        }
+        h = (h + 1) & (kSlots - 1);
+    }
+    return false;
+}
+
+// The distinct offsets cols[k] - i of a CSR matrix into `table` (kSlots
+// entries preset to kEmpty); flags[0] |= 1 when there are more than the set
+// holds, |= 2 when a row's columns are not strictly increasing.
+__global__ void dia_offsets_kernel(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols, uint32_t n,
+                                   int32_t* table, int* flags) {
+    __shared__ int32_t st[kSlots];
+    for (int s = threadIdx.x; s < kSlots; s += blockDim.x) st[s] = kEmpty;
+    __syncthreads();
+    int bad = 0;
+    int32_t last[4] = {kEmpty, kEmpty, kEmpty, kEmpty};  // offsets this thread inserted lately
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t b = rp[i], e = rp[i + 1];
+        for (uint32_t k = b; k < e; ++k) {
+            const uint32_t c = cols[k];
+            if (k > b && c <= cols[k - 1]) bad |= 2;
+            const int32_t o = static_cast<int32_t>(static_cast<int64_t>(c) - static_cast<int64_t>(i));
+            if (o == last[0] || o == last[1] || o == last[2] || o == last[3]) continue;
+            if (!set_insert(st, o)) bad |= 1;
+            last[3] = last[2];
+            last[2] = last[1];
+            last[1] = last[0];
+            last[0] = o;
+        }
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < kSlots; s += blockDim.x)
+        if (st[s] != kEmpty && !set_insert(table, st[s])) bad |= 1;
+    if (bad) atomicOr(flags, bad);
+}
+
+__device__ __forceinline__ float widen(float v) { return v; }
+__device__ __forceinline__ float widen(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float widen(double v) { return static_cast<float>(v); }
+
+template <typename VO>
+__device__ __forceinline__ VO narrow(double v) {
+    if constexpr (std::is_same_v<VO, __nv_bfloat16>)
+        return __double2bfloat16(v);
+    else
+        return static_cast<VO>(v);
+}
+template <typename VO>
+__device__ __forceinline__ VO narrow(__nv_bfloat16 v) {
+    if constexpr (std::is_same_v<VO, __nv_bfloat16>)
+        return v;
+    else
+        return static_cast<VO>(__bfloat162float(v));
+}
+template <typename VO>
+__device__ __forceinline__ VO narrow(float v) {
+    if constexpr (std::is_same_v<VO, __nv_bfloat16>)
+        return __float2bfloat16(v);
+    else
+        return static_cast<VO>(v);
+}
+
+// out[d * n + i] = vals of entry (i, i + off[d]), rounded to VO (out zeroed
+// before); the offsets are sorted, so the diagonal is found by a short scan.
+template <typename VI, typename VO>
+__global__ void dia_fill_kernel(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols,
+                                const VI* __restrict__ vals, uint32_t n, DiaOffsets offs, VO* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t b = rp[i], e = rp[i + 1];
+        int d = 0;
+        for (uint32_t k = b; k < e; ++k) {
+            const int32_t o = static_cast<int32_t>(static_cast<int64_t>(cols[k]) - static_cast<int64_t>(i));
+            while (d < offs.nd && offs.off[d] < o) ++d;  // columns increase, so d only moves forward
+            if (d < offs.nd && offs.off[d] == o) out[static_cast<size_t>(d) * n + i] = narrow<VO>(vals[k]);
+        }
+    }
+}
+
+// invD[i] = 1 / a_ii from the main diagonal of a DIA matrix; status |=
+// kStatusZeroDiag where it is zero.
+template <typename V>
+__global__ void dia_inv_diag_kernel(const V* __restrict__ diag, uint32_t n, float* __restrict__ invD, int* status) {
+    bool zero = false;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float v = widen(diag[i]);
+        invD[i] = 1.f / v;
+        zero |= (v == 0.f);
+    }
+    if (zero) atomicOr(status, kStatusZeroDiag);
+}
+
+// ---- the fused inner PCG
+
+// The rows a CTA owns in every phase: a static contiguous slice, each thread
+// a strided set of it. (Handing rows out in chunks from a per-phase counter,
+// so that faster CTAs take more, measured slower on B200: C5 learned inner
+// iteration 31.9 vs 27.6 us -- the per-chunk barrier and the dependent chunk
+// fetch cost more than the wait for the slowest slice at the exchange.)
+template <typename F>
+__device__ __forceinline__ void for_rows(uint32_t n, F body) {
+    const uint64_t c = blockIdx.x, G = gridDim.x;
+    const uint32_t r0 = static_cast<uint32_t>(c * n / G), r1 = static_cast<uint32_t>((c + 1) * n / G);
+    for (uint32_t i = r0 + threadIdx.x; i < r1; i += kDiaThreads) body(i);
+}
+
+// sum_d M[d][i] * xf(i + off[d]) over the ND diagonals (ND the matrix's
+// padded diagonal count), in increasing column order, FP32 FMAs. Every load
+// is unconditional -- indices outside the matrix are clamped and their
+// product replaced by zero with a select -- so all of a row's loads issue
+// before its first FMA waits on one.
+template <int ND, typename V, typename XF>
+__device__ __forceinline__ float dia_row(const DiaMat<V>& M, uint32_t n, uint32_t i, XF xf) {
+    float av[ND], xv[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        const int64_t j = static_cast<int64_t>(i) + M.off[d];
+        const bool in = j >= 0 && j < static_cast<int64_t>(n);
+        const uint32_t jc = in ? static_cast<uint32_t>(j) : i;
+        av[d] = widen(__ldg(M.vals + static_cast<size_t>(d) * n + i));
+        const float v = xf(jc);
+        xv[d] = in ? v : 0.f;
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) s = fmaf(av[d], xv[d], s);
+    return s;
+}
+
+// z_i = sum_e GT[e][i] t_{i + off_T[e]} for the learned factor, with the
+// t_j = (G r)_j of the neighbouring rows formed on the fly from rf (so no
+// grid barrier separates t = G r from z = G^T t); ti gets t_i itself (the
+// term of G^T's main diagonal, index gt_diag), whose square sums to
+// <r, G^T G r> = ||G r||^2.
+template <int NDG, typename VG, typename RF>
+__device__ __forceinline__ float zt_row(const DiaMat<VG>& G, const DiaMat<VG>& GT, int gt_diag, uint32_t n,
+                                        uint32_t i, RF rf, float& ti) {
+    float z = 0.f;
+    ti = 0.f;
+#pragma unroll
+    for (int e = 0; e < NDG; ++e) {
+        const int64_t j = static_cast<int64_t>(i) + GT.off[e];
+        const bool in = j >= 0 && j < static_cast<int64_t>(n);
+        const uint32_t jc = in ? static_cast<uint32_t>(j) : i;
+        const float gv = widen(__ldg(GT.vals + static_cast<size_t>(e) * n + i));
+        const float tj = in ? dia_row<NDG>(G, n, jc, rf) : 0.f;
+        z = fmaf(gv, tj, z);
+        ti = (e == gt_diag) ? tj : ti;
+    }
+    return z;
+}
+
+// Loads of vectors other CTAs wrote earlier in the same launch. The grid
+// exchange between two phases orders them (release by the writers, acquire
+// by thread 0 of the reader's CTA, then the CTA barrier), so plain weak
+// loads observe the new values (CLSP_DIA_LDCG 2, which also leaves the
+// compiler free to batch them); 1: L2-only loads, 0: weak loads through
+// inline PTX.
+#ifndef CLSP_DIA_LDCG
+#define CLSP_DIA_LDCG 2
+#endif
+__device__ __forceinline__ float vld(const float* p) {
+#if CLSP_DIA_LDCG == 2
+    return *p;
+#elif CLSP_DIA_LDCG == 1
+    return __ldcg(p);
+#else
+    return dev::ld_coherent(p);
+#endif
+}
+
+template <typename VA, typename VG, int PK, int NDA, int NDG>
+__global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_pcg_kernel(DiaPcgArgs<VA, VG> a) {
+    __shared__ GridSmem gs;
+    const FusedSync g = a.sync;
+    unsigned long long epoch = 0;
+    const uint32_t n = a.n;
+    const uint32_t tid = threadIdx.x;
+    // No __restrict__: these vectors are read at neighbouring rows by other CTAs.
+    float* x = a.x;
+    float* q = a.q;
+    float* t = a.t;
+    float* z = a.z;
+    const float* b = a.b;
+    const float* invD = a.invD;
+    const DiaPcgState in = *a.st;
+    const double tol2 = in.tol * in.tol;
+    int pold = in.pbuf & 1;
+    int cur = 0;
+    bool use_p = in.warm != 0;
+    double rz = 0.0, rr0 = 0.0, rr = 0.0;
+    float beta = 0.f;
+    int iters = 0, status = 0;
+
+    // ---- r = b, x = 0, z = M r, <r,z>, <r,r>
+    {
+        double acc[2] = {0.0, 0.0};
+        if constexpr (PK == 1) {
+            for_rows(n, [&](uint32_t i) {
+                float ti;
+                const float zi =
+                    zt_row<NDG>(a.G, a.GT, a.gt_diag, n, i, [&](uint32_t k) { return __ldg(b + k); }, ti);
+                const float ri = __ldg(b + i);
+                a.r[0][i] = ri;
+                x[i] = 0.f;
+                z[i] = zi;
+                acc[0] += static_cast<double>(ti) * ti;  // <r, G^T G r> = ||G r||^2
+                acc[1] += static_cast<double>(ri) * ri;
+            });
+        } else {
+            for_rows(n, [&](uint32_t i) {
+                const float ri = __ldg(b + i);
+                a.r[0][i] = ri;
+                x[i] = 0.f;
+                const float zi = invD ? ri * __ldg(invD + i) : ri;
+                z[i] = zi;
+                acc[0] += static_cast<double>(ri) * zi;
+                acc[1] += static_cast<double>(ri) * ri;
+            });
+        }
+        double tot[2];
+        if (!grid_exchange<2>(g, epoch, acc, tot, gs)) goto fail;
+        rz = tot[0];
+        rr0 = rr = tot[1];
+    }
+    if (!(rr0 > 0.0) || in.max_iters <= 0) goto finish;  // b == 0: x = 0
+    if (use_p) beta = static_cast<float>(rz / in.rz_prev);
+
+    for (;;) {
+        const int pn = pold ^ 1;
+        float* P = a.p[pn];
+        const float* Po = a.p[pold];
+        // ---- A: p_new = z + beta p_old, q = A p_new, <p_new, q>
+        {
+            double acc[1] = {0.0};
+            auto pv = [&](uint32_t j) {
+                const float zj = vld(z + j);
+                return use_p ? fmaf(beta, vld(Po + j), zj) : zj;
+            };
+            for_rows(n, [&](uint32_t i) {
+                const float qi = dia_row<NDA>(a.A, n, i, pv);
+                const float pi = pv(i);
+                P[i] = pi;
+                q[i] = qi;
+                acc[0] += static_cast<double>(pi) * qi;
+            });
+            double pq[1];
+            if (!grid_exchange<1>(g, epoch, acc, pq, gs)) goto fail;
+            if (!(pq[0] > 0.0)) {  // lost positive curvature (or not finite): stop, the caller restarts
+                status |= isfinite(pq[0]) ? kStatusCurvature : kStatusNonFinite;
+                break;
+            }
+            const float alpha = static_cast<float>(rz / pq[0]);
+            // ---- B
+            if constexpr (PK == 1) {
+                const float* Rc = a.r[cur];
+                float* Rn = a.r[cur ^ 1];
+                double acc2[2] = {0.0, 0.0};
+                auto rnew = [&](uint32_t k) { return fmaf(-alpha, vld(q + k), vld(Rc + k)); };
+                for_rows(n, [&](uint32_t i) {
+                    float ti;
+                    const float zi = zt_row<NDG>(a.G, a.GT, a.gt_diag, n, i, rnew, ti);
+                    x[i] = fmaf(alpha, P[i], x[i]);
+                    const float rn = fmaf(-alpha, q[i], Rc[i]);
+                    Rn[i] = rn;
+                    z[i] = zi;
+                    acc2[0] += static_cast<double>(rn) * rn;
+                    acc2[1] += static_cast<double>(ti) * ti;
+                });
+                double tot[2];
+                if (!grid_exchange<2>(g, epoch, acc2, tot, gs)) goto fail;
+                rr = tot[0];
+                cur ^= 1;
+                ++iters;
+                pold = pn;
+                use_p = true;
+                if (!isfinite(rr)) {
+                    status |= kStatusNonFinite;
+                    break;
+                }
+                if (rr <= tol2 * rr0 || iters >= in.max_iters) break;
+                beta = static_cast<float>(tot[1] / rz);
+                rz = tot[1];
+                continue;
+            } else {
+                float* R = a.r[0];
+                double acc2[2] = {0.0, 0.0};
+                for_rows(n, [&](uint32_t i) {
+                    x[i] = fmaf(alpha, P[i], x[i]);
+                    const float ri = fmaf(-alpha, q[i], R[i]);
+                    R[i] = ri;
+                    const float zi = invD ? ri * __ldg(invD + i) : ri;
+                    z[i] = zi;
+                    acc2[0] += static_cast<double>(ri) * ri;
+                    acc2[1] += static_cast<double>(ri) * zi;
+                });
+                double tot[2];
+                if (!grid_exchange<2>(g, epoch, acc2, tot, gs)) goto fail;
+                rr = tot[0];
+                ++iters;
+                pold = pn;
+                use_p = true;
+                if (!isfinite(rr)) {
+                    status |= kStatusNonFinite;
+                    break;
+                }
+                if (rr <= tol2 * rr0 || iters >= in.max_iters) break;
+                beta = static_cast<float>(tot[1] / rz);
+                rz = tot[1];
+                continue;
+            }
+        }
+    }
+finish:
+    if (blockIdx.x == 0 && tid == 0) {
+        a.st->iters = iters;
+        a.st->rr0 = rr0;
+        a.st->rr = rr;
+        a.st->rz_prev = rz;  // the denominator that formed the last direction
+        a.st->pbuf = pold;   // the buffer holding it
+        a.st->xbuf = cur;    // the buffer holding the last residual
+        atomicOr(&a.st->status, status);
+    }
+    return;
+fail:
+    if (tid == 0) atomicOr(&a.st->status, kStatusBarrierTimeout);
+}
+
+template <typename VA, typename VG, int PK, int NDA, int NDG>
+int dia_grid(int sm_count) {
+    static int per_sm = [] {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dia_pcg_kernel<VA, VG, PK, NDA, NDG>, kDiaThreads,
+                                                          0) != cudaSuccess) {
+            cudaGetLastError();
+            b = 1;
+        }
+        return std::max(1, std::min(b, kDiaCtasPerSm));
+    }();
+    return std::max(1, sm_count) * per_sm;
+}
+
+template <typename VA, typename VG, int PK, int NDA, int NDG>
+cudaError_t dia_launch(DiaPcgArgs<VA, VG>& a, int sm_count, cudaStream_t s, uint32_t& grid) {
+    grid = static_cast<uint32_t>(dia_grid<VA, VG, PK, NDA, NDG>(sm_count));
+    void* args[] = {&a};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(dia_pcg_kernel<VA, VG, PK, NDA, NDG>),
+                                       dim3(grid), dim3(kDiaThreads), args, 0, s);
+}
+
+// Padded diagonal counts the kernel is built for: A alone (Jacobi / none),
+// and (A, G) pairs for the learned factor (G and G^T padded alike).
+constexpr int kClassA[] = {3, 5, 7, 9, kMaxDiags};
+constexpr int kPairs[][2] = {{5, 3}, {7, 4}, {9, 5}, {kMaxDiags, kMaxDiags}};
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+}  // namespace
+
+bool dia_enabled() {
+    const char* e = std::getenv("CLSPARSE_B200_DIA");
+    return !(e && e[0] == '0' && e[1] == '\0');
+}
+
+clsparseStatus dia_detect(const uint32_t* rp, const uint32_t* cols, uint32_t n, uint32_t nnz, DiaWork& w,
+                          cudaStream_t s, DiaOffsets& offs) {
+    offs.nd = 0;
+    if (n == 0 || nnz == 0) return clsparseInvalidValue;
+    if (w.table.ensure(kSlots * sizeof(int32_t) + 64) != cudaSuccess) {
+        cudaGetLastError();
+        return clsparseOutOfResources;
+    }
+    int32_t* table = static_cast<int32_t*>(w.table.ptr);
+    int* flags = reinterpret_cast<int*>(table + kSlots);
+    cudaMemsetAsync(table, 0x80, kSlots * sizeof(int32_t), s);  // kEmpty in every slot
+    cudaMemsetAsync(flags, 0, sizeof(int), s);
+    const uint32_t grid = std::min<uint32_t>((n + 255) / 256, 1184);
+    dia_offsets_kernel<<<grid, 256, 0, s>>>(rp, cols, n, table, flags);
+    int32_t h[kSlots + 1];
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(h, table, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return clsparseInvalidKernelExecution;
+    if (h[kSlots] != 0) return clsparseInvalidValue;
+    std::vector<int32_t> o;
+    for (int k = 0; k < kSlots; ++k)
+        if (h[k] != kEmpty) o.push_back(h[k]);
+    if (o.empty() || o.size() > static_cast<size_t>(kMaxDiags)) return clsparseInvalidValue;
+    // at least half of the stored diagonal entries hold matrix entries
+    if (static_cast<uint64_t>(nnz) * 2 < static_cast<uint64_t>(o.size()) * n) return clsparseInvalidValue;
+    std::sort(o.begin(), o.end());
+    offs.nd = static_cast<int>(o.size());
+    for (int d = 0; d < offs.nd; ++d) offs.off[d] = o[d];
+    return clsparseSuccess;
+}
+
+template <typename VI, typename VO>
+clsparseStatus dia_build(const uint32_t* rp, const uint32_t* cols, const VI* vals, uint32_t n,
+                         const DiaOffsets& offs, int nd_pad, DeviceBuffer& buf, cudaStream_t s, DiaMat<VO>& out) {
+    if (nd_pad < offs.nd || nd_pad > kMaxDiags) return clsparseInvalidValue;
+    const size_t bytes = static_cast<size_t>(nd_pad) * n * sizeof(VO);
+    if (buf.ensure(bytes + 256) != cudaSuccess) {
+        cudaGetLastError();
+        return clsparseOutOfResources;
+    }
+    VO* v = static_cast<VO*>(buf.ptr);
+    cudaMemsetAsync(v, 0, bytes, s);
+    const uint32_t grid = std::min<uint32_t>((n + 255) / 256, 1184);
+    dia_fill_kernel<VI, VO><<<grid, 256, 0, s>>>(rp, cols, vals, n, offs, v);
+    if (cudaGetLastError() != cudaSuccess) return clsparseInvalidKernelExecution;
+    out.vals = v;
+    out.nd = nd_pad;  // padded diagonals: offset 0, values 0
+    for (int d = 0; d < kMaxDiags; ++d) out.off[d] = d < offs.nd ? offs.off[d] : 0;
+    return clsparseSuccess;
+}
+
+template <typename VA>
+clsparseStatus dia_jacobi(const DiaMat<VA>& A, uint32_t n, float* invD, int* status, cudaStream_t s) {
+    int d0 = -1;
+    for (int d = 0; d < A.nd; ++d)
+        if (A.off[d] == 0) d0 = d;
+    if (d0 < 0) return clsparseInvalidValue;  // no main diagonal: the CSR path reports it
+    const uint32_t grid = std::min<uint32_t>((n + 255) / 256, 1184);
+    dia_inv_diag_kernel<VA><<<grid, 256, 0, s>>>(A.vals + static_cast<size_t>(d0) * n, n, invD, status);
+    return cudaGetLastError() == cudaSuccess ? clsparseSuccess : clsparseInvalidKernelExecution;
+}
+
+void dia_classes(int nda, int ndg, bool learned, int& ca, int& cg) {
+    ca = cg = 0;
+    if (!learned) {
+        for (int c : kClassA)
+            if (nda <= c) {
+                ca = c;
+                return;
+            }
+        return;
+    }
+    for (const auto& p : kPairs)
+        if (nda <= p[0] && ndg <= p[1]) {
+            ca = p[0];
+            cg = p[1];
+            return;
+        }
+}
+
+namespace {
+
+// One inner solve as one cooperative launch.
+template <typename VA, typename VG>
+clsparseStatus dia_persistent_solve(DiaPcgArgs<VA, VG> a, bool learned, DiaWork& w, clsparseControl c,
+                                    DiaPcgState& st) {
+    cudaStream_t s = c->stream;
+    const uint32_t max_grid = static_cast<uint32_t>(std::max(1, c->sm_count) * 2);
+    const size_t sync_b = align256(fused_sync_bytes(max_grid));
+    if (w.sync.ensure(sync_b + align256(sizeof(DiaPcgState))) != cudaSuccess) {
+        cudaGetLastError();
+        return clsparseOutOfResources;
+    }
+    char* base = static_cast<char*>(w.sync.ptr);
+    DiaPcgState* dst = reinterpret_cast<DiaPcgState*>(base + sync_b);
+    st.status = 0;
+    cudaMemsetAsync(base, 0, kFusedSyncHead, s);
+    cudaMemcpyAsync(dst, &st, sizeof(st), cudaMemcpyHostToDevice, s);
+    a.sync = fused_sync_at(base);
+    // failure-path test switches, as for the CSR persistent engine
+    if (const char* e = std::getenv("CLSPARSE_B200_BARRIER_WAIT_NS")) {
+        const unsigned long long v = std::strtoull(e, nullptr, 10);
+        if (v > 0) a.sync.wait_ns = v;
+    }
+    if (const char* e = std::getenv("CLSPARSE_B200_TEST_BARRIER_NEVER_RELEASE")) a.sync.never_release = std::atoi(e) != 0;
+    a.st = dst;
+    const int sms = c->sm_count;
+    uint32_t grid = 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    const int na = a.A.nd, ng = a.G.nd;
+    if (!learned) {
+        if (na == 3) e = dia_launch<VA, VG, 0, 3, 3>(a, sms, s, grid);
+        else if (na == 5) e = dia_launch<VA, VG, 0, 5, 3>(a, sms, s, grid);
+        else if (na == 7) e = dia_launch<VA, VG, 0, 7, 3>(a, sms, s, grid);
+        else if (na == 9) e = dia_launch<VA, VG, 0, 9, 3>(a, sms, s, grid);
+        else if (na == kMaxDiags) e = dia_launch<VA, VG, 0, kMaxDiags, 3>(a, sms, s, grid);
+    } else {
+        if (na == 5 && ng == 3) e = dia_launch<VA, VG, 1, 5, 3>(a, sms, s, grid);
+        else if (na == 7 && ng == 4) e = dia_launch<VA, VG, 1, 7, 4>(a, sms, s, grid);
+        else if (na == 9 && ng == 5) e = dia_launch<VA, VG, 1, 9, 5>(a, sms, s, grid);
+        else if (na == kMaxDiags && ng == kMaxDiags) e = dia_launch<VA, VG, 1, kMaxDiags, kMaxDiags>(a, sms, s, grid);
+    }
+    if (e != cudaSuccess || grid > max_grid) {
+        cudaGetLastError();
+        return clsparseInvalidKernelExecution;
+    }
+    if (cudaMemcpyAsync(&st, dst, sizeof(st), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return clsparseInvalidKernelExecution;
+    if (st.status & kStatusBarrierTimeout) return clsparseInvalidKernelExecution;
+    return clsparseSuccess;
+}
+
+}  // namespace
+
+template <typename VA, typename VG>
+clsparseStatus dia_pcg_solve(DiaPcgArgs<VA, VG> a, bool learned, DiaWork& w, clsparseControl c,
+                             DiaPcgState& st) {
+    return dia_persistent_solve<VA, VG>(a, learned, w, c, st);
+}
+
+#define CLSP_DIA_INST(VA, VG)                                                                                 \
+    template clsparseStatus dia_pcg_solve<VA, VG>(DiaPcgArgs<VA, VG>, bool, DiaWork&, clsparseControl,       \
+                                                  DiaPcgState&);
+CLSP_DIA_INST(float, __nv_bfloat16)
+CLSP_DIA_INST(__nv_bfloat16, __nv_bfloat16)
+#undef CLSP_DIA_INST
+
+template clsparseStatus dia_build<double, float>(const uint32_t*, const uint32_t*, const double*, uint32_t,
+                                                 const DiaOffsets&, int, DeviceBuffer&, cudaStream_t, DiaMat<float>&);
+template clsparseStatus dia_build<double, __nv_bfloat16>(const uint32_t*, const uint32_t*, const double*, uint32_t,
+                                                         const DiaOffsets&, int, DeviceBuffer&, cudaStream_t,
+                                                         DiaMat<__nv_bfloat16>&);
+template clsparseStatus dia_build<__nv_bfloat16, __nv_bfloat16>(const uint32_t*, const uint32_t*,
+                                                                const __nv_bfloat16*, uint32_t, const DiaOffsets&,
+                                                                int, DeviceBuffer&, cudaStream_t,
+                                                                DiaMat<__nv_bfloat16>&);
+template clsparseStatus dia_jacobi<float>(const DiaMat<float>&, uint32_t, float*, int*, cudaStream_t);
+template clsparseStatus dia_jacobi<__nv_bfloat16>(const DiaMat<__nv_bfloat16>&, uint32_t, float*, int*,
+                                                  cudaStream_t);
+
+}  // namespace clsp

@@ -31,111 +31,11 @@
 #include <vector>
 
 #include "fused.h"
+#include "grid_sync.cuh"
 #include "spmv_word.cuh"
 
 namespace clsp {
 namespace {
-
-__device__ __forceinline__ uint64_t global_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
-
-struct GridSmem {
-    double red[32];
-    int ok;
-};
-
-// Grid exchange. Every CTA stores its K partial sums for `epoch` in its slot
-// (two buffers, by epoch parity), makes its writes visible and takes an
-// arrival ticket; the CTA drawing the last ticket of the epoch releases the
-// epoch flag, thread 0 of every other CTA waits for it (relaxed polling, one
-// acquire fence after). Then every thread reads the partials of CTAs tid,
-// tid + NT, ... and a block reduction finishes the sums, so every CTA obtains
-// bitwise the same totals, whatever the arrival order. K = 0 is a plain
-// barrier. A slot is rewritten two exchanges later at the earliest, when
-// every CTA has finished reading it.
-// Returns false (in every thread) when the grid has to stop: the wait ran out
-// (the error flag is then set) or another CTA reported that it did.
-template <int K>
-__device__ bool grid_exchange(const FusedSync& g, unsigned long long& epoch, const double (&v)[K > 0 ? K : 1],
-                              double (&out)[K > 0 ? K : 1], GridSmem& gs) {
-    double tot[K > 0 ? K : 1];
-    if constexpr (K > 0) {
-#pragma unroll
-        for (int k = 0; k < K; ++k) tot[k] = dev::block_sum(v[k], gs.red);
-    } else {
-        __syncthreads();
-    }
-    ++epoch;
-    const uint32_t G = gridDim.x;
-    const double* part = g.partials + (epoch & 1ull) * static_cast<size_t>(G) * 4;
-    if (threadIdx.x == 0) {
-        if constexpr (K > 0) {
-            double* mine = g.partials + (epoch & 1ull) * static_cast<size_t>(G) * 4 + static_cast<size_t>(blockIdx.x) * 4;
-#pragma unroll
-            for (int k = 0; k < K; ++k) mine[k] = tot[k];
-        }
-        __threadfence();
-        bool ok = true;
-        const unsigned long long t = atomicAdd(g.arrive, 1ull);
-        if (t + 1ull == epoch * G && !g.never_release) {
-            st_release(g.release, epoch);
-        } else {
-            uint64_t t0 = 0;
-            uint32_t spins = 0;
-            while (ld_relaxed(g.release) < epoch) {
-                if ((++spins & 255u) == 0u) {
-                    if (*reinterpret_cast<volatile int*>(g.err)) {
-                        ok = false;
-                        break;
-                    }
-                    const uint64_t now = global_ns();
-                    if (t0 == 0) {
-                        t0 = now;
-                    } else if (now - t0 > g.wait_ns) {
-                        atomicExch(g.err, 1);
-                        ok = false;
-                        break;
-                    }
-                }
-            }
-        }
-        fence_acq_rel();
-        gs.ok = ok ? 1 : 0;
-    }
-    __syncthreads();
-    if (!gs.ok) return false;
-    if constexpr (K > 0) {
-        double acc[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) acc[k] = 0.0;
-        for (uint32_t i = threadIdx.x; i < G; i += blockDim.x)
-#pragma unroll
-            for (int k = 0; k < K; ++k) acc[k] += __ldcg(part + static_cast<size_t>(i) * 4 + k);
-#pragma unroll
-        for (int k = 0; k < K; ++k) out[k] = dev::block_sum(acc[k], gs.red);
-    }
-    return true;
-}
-
-__device__ __forceinline__ bool grid_sync(const FusedSync& g, unsigned long long& epoch, GridSmem& gs) {
-    double none[1] = {0.0}, out[1];
-    return grid_exchange<0>(g, epoch, none, out, gs);
-}
 
 // The rows [r0, r1) whose vector entries this CTA updates.
 struct RowSlice {

@@ -42,9 +42,16 @@ struct DeviceBuffer {
 
 struct SolverCache;  // cached CUDA graph + work vectors of the last solve
 
+// Device buffers of the banded inner solves (dia.h): offset table, the
+// diagonal-storage copies of A, G and G^T, work vectors, exchange area.
+struct DiaWork {
+    DeviceBuffer table, A, G, GT, vecs, sync;
+};
+
 // Work area of the mixed-precision refinement (mixed.cu), owned by the control.
 struct MixedWork {
     DeviceBuffer lowvals, y, r32, d, parts;
+    std::unique_ptr<DiaWork> dia;
     void* pinned = nullptr;
     ~MixedWork() {
         if (pinned) cudaFreeHost(pinned);

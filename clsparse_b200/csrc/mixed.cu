@@ -20,6 +20,7 @@
 #include <cstring>
 
 #include "device_common.cuh"
+#include "dia.h"
 #include "internal.h"
 
 namespace clsp {
@@ -85,6 +86,119 @@ struct Factor {
     CsrView<__nv_bfloat16> G, GT;
 };
 
+// The inner CG solves on diagonal storage (dia.cu) when A -- and the learned
+// factor's G and G^T -- have few distinct column offsets: the low-precision
+// copy of A is laid out by diagonal instead of in CSR, and each inner solve
+// is one fused cooperative launch.
+template <typename V>
+struct BandedInner {
+    bool on = false;
+    DiaMat<V> A;
+    DiaMat<__nv_bfloat16> G, GT;
+    float* invD = nullptr;
+    float* vec[7] = {};  // r0, r1, p0, p1, q, t, z
+    int* status = nullptr;
+    bool have_p = false;  // a previous solve left a direction to continue
+    int pbuf = 0;
+    double rz_prev = 0.0;
+};
+
+template <typename V>
+bool setup_banded(BandedInner<V>& bi, const clsparseCsrMatrix* A, const Factor* factor, MixedWork& w,
+                  bool jacobi, clsparseControl c) {
+    if (!dia_enabled()) return false;
+    if (!w.dia) w.dia = std::make_unique<DiaWork>();
+    DiaWork& dw = *w.dia;
+    cudaStream_t s = c->stream;
+    const uint32_t n = A->num_rows, nnz = A->num_nonzeros;
+    const uint32_t* rp = dev_ptr<const uint32_t>(A->row_pointer, A->off_row_pointer);
+    const uint32_t* cols = dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices);
+    DiaOffsets oa, og, ot;
+    if (dia_detect(rp, cols, n, nnz, dw, s, oa) != clsparseSuccess) return false;
+    if (factor) {
+        if (dia_detect(factor->G.rp, factor->G.cols, n, factor->G.nnz, dw, s, og) != clsparseSuccess ||
+            dia_detect(factor->GT.rp, factor->GT.cols, n, factor->GT.nnz, dw, s, ot) != clsparseSuccess)
+            return false;
+    }
+    // padded diagonal counts of the engine's builds; the fallback from the
+    // learned factor to Jacobi runs the same A, so A takes the learned class
+    int ca = 0, cg = 0;
+    dia_classes(oa.nd, factor ? std::max(og.nd, ot.nd) : 0, factor != nullptr, ca, cg);
+    if (ca == 0) return false;
+    if (dia_build<double, V>(rp, cols, dev_ptr<const double>(A->values, A->off_values), n, oa, ca, dw.A, s, bi.A) !=
+        clsparseSuccess)
+        return false;
+    if (factor && (dia_build<__nv_bfloat16, __nv_bfloat16>(factor->G.rp, factor->G.cols, factor->G.vals, n, og, cg,
+                                                           dw.G, s, bi.G) != clsparseSuccess ||
+                   dia_build<__nv_bfloat16, __nv_bfloat16>(factor->GT.rp, factor->GT.cols, factor->GT.vals, n, ot,
+                                                           cg, dw.GT, s, bi.GT) != clsparseSuccess))
+        return false;
+    const size_t stride = (static_cast<size_t>(n) + 63) & ~size_t(63);
+    if (dw.vecs.ensure(8 * stride * sizeof(float) + 256) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    float* base = static_cast<float*>(dw.vecs.ptr);
+    bi.invD = base;
+    for (int k = 0; k < 7; ++k) bi.vec[k] = base + (k + 1) * stride;
+    bi.status = reinterpret_cast<int*>(base + 8 * stride);
+    cudaMemsetAsync(bi.status, 0, sizeof(int), s);
+    if (jacobi) {
+        // a zero diagonal entry: the CSR path runs and reports it
+        int zero = 0;
+        if (dia_jacobi<V>(bi.A, n, bi.invD, bi.status, s) != clsparseSuccess ||
+            cudaMemcpyAsync(&zero, bi.status, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess || zero != 0)
+            return false;
+    }
+    bi.on = true;
+    return true;
+}
+
+// One inner solve on the banded engine, with the bookkeeping of the CSR
+// engine's: inner.nIters (iterations - 1), the reached relative residual,
+// the device status bits.
+template <typename V>
+clsparseStatus banded_solve(BandedInner<V>& bi, bool learned, bool jacobi, float* x, const float* b, uint32_t n,
+                            double tol, bool warm, _solverControl& inner, MixedWork& w, clsparseControl c) {
+    DiaPcgArgs<V, __nv_bfloat16> a;
+    a.A = bi.A;
+    a.G = bi.G;
+    a.GT = bi.GT;
+    a.invD = jacobi ? bi.invD : nullptr;
+    a.b = b;
+    a.x = x;
+    a.r[0] = bi.vec[0];
+    a.r[1] = bi.vec[1];
+    a.p[0] = bi.vec[2];
+    a.p[1] = bi.vec[3];
+    a.q = bi.vec[4];
+    a.t = bi.vec[5];
+    a.z = bi.vec[6];
+    a.n = n;
+    a.gt_diag = 0;
+    for (int d = bi.GT.nd - 1; d >= 0; --d)  // the first zero offset: the real diagonal, padding comes after
+        if (bi.GT.off[d] == 0) a.gt_diag = d;
+    DiaPcgState st;
+    st.tol = tol;
+    st.max_iters = inner.maxIters;
+    st.warm = (warm && bi.have_p && bi.rz_prev > 0.0) ? 1 : 0;
+    st.pbuf = bi.pbuf;
+    st.rz_prev = bi.rz_prev;
+    const clsparseStatus stt = dia_pcg_solve<V, __nv_bfloat16>(a, learned, *w.dia, c, st);
+    if (stt != clsparseSuccess) {
+        inner.deviceStatus = static_cast<cl_uint>(st.status);
+        return stt;
+    }
+    inner.nIters = st.iters - 1;
+    inner.currentResidual = st.rr0 > 0.0 ? std::sqrt(st.rr / st.rr0) : 0.0;
+    inner.deviceStatus = static_cast<cl_uint>(st.status);
+    bi.have_p = st.iters > 0 && st.status == 0;
+    bi.pbuf = st.pbuf;
+    bi.rz_prev = st.rz_prev;
+    return clsparseSuccess;
+}
+
 enum class Inner { Cg, BiCgStab };
 
 template <typename V>
@@ -105,7 +219,10 @@ clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const clden
     double* x = dev_ptr<double>(xv->values, xv->off_values);
     const double* b = dev_ptr<const double>(bv->values, bv->off_values);
     V* lv = static_cast<V*>(w.lowvals.ptr);
-    round_values_kernel<V><<<grid_for(nnz, c->sm_count), kThreads, 0, s>>>(Avals, lv, nnz);
+    BandedInner<V> bi;
+    if (method == Inner::Cg)
+        setup_banded<V>(bi, A, factor, w, sc->preconditioner == DIAGONAL, c);
+    if (!bi.on) round_values_kernel<V><<<grid_for(nnz, c->sm_count), kThreads, 0, s>>>(Avals, lv, nnz);
 
     // FP64 operator and the low-precision copy sharing its structure and meta
     CsrView<double> A64{Avals, dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices),
@@ -198,7 +315,11 @@ clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const clden
         ws.warm = have_prev && prev_factor == use_factor && !breakdown && res <= 2.0 * predicted;
         inner.nIters = 0;
         inner.deviceStatus = 0;
-        if (method == Inner::BiCgStab)  // restarted every refinement step
+        if (bi.on)
+            st = banded_solve<V>(bi, use_factor, sc->preconditioner == DIAGONAL, static_cast<float*>(w.d.ptr),
+                                 static_cast<const float*>(w.r32.ptr), static_cast<uint32_t>(n), inner_tol, ws.warm,
+                                 inner, w, c);
+        else if (method == Inner::BiCgStab)  // restarted every refinement step
             st = bicg_solve_typed<V, float>(&dvec, &Alow, &rvec, &inner, c);
         else if (use_factor)
             st = pcg_factor_typed<V, float, __nv_bfloat16>(&dvec, &Alow, &rvec, &inner, factor->G, factor->GT,
