@@ -235,6 +235,13 @@ __device__ __forceinline__ float zt_row(const DiaMat<VG>& G, const DiaMat<VG>& G
     return z;
 }
 
+// Learned iteration: 1 = three phases (B forms t = G r_new and stores it, C
+// forms z = G^T t and ends with a plain barrier), 0 = two phases (B forms z
+// with the neighbours' t_j recomputed).
+#ifndef CLSP_DIA_SPLIT
+#define CLSP_DIA_SPLIT 1
+#endif
+
 // Loads of vectors other CTAs wrote earlier in the same launch. The grid
 // exchange between two phases orders them (release by the writers, acquire
 // by thread 0 of the reader's CTA, then the CTA barrier), so plain weak
@@ -344,11 +351,16 @@ __global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_pcg_kernel(Dia
                 auto rnew = [&](uint32_t k) { return fmaf(-alpha, vld(q + k), vld(Rc + k)); };
                 for_rows(n, [&](uint32_t i) {
                     float ti;
+#if CLSP_DIA_SPLIT
+                    ti = dia_row<NDG>(a.G, n, i, rnew);
+                    t[i] = ti;
+#else
                     const float zi = zt_row<NDG>(a.G, a.GT, a.gt_diag, n, i, rnew, ti);
+                    z[i] = zi;
+#endif
                     x[i] = fmaf(alpha, P[i], x[i]);
                     const float rn = fmaf(-alpha, q[i], Rc[i]);
                     Rn[i] = rn;
-                    z[i] = zi;
                     acc2[0] += static_cast<double>(rn) * rn;
                     acc2[1] += static_cast<double>(ti) * ti;
                 });
@@ -366,6 +378,11 @@ __global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_pcg_kernel(Dia
                 if (rr <= tol2 * rr0 || iters >= in.max_iters) break;
                 beta = static_cast<float>(tot[1] / rz);
                 rz = tot[1];
+#if CLSP_DIA_SPLIT
+                // C: z = G^T t; a plain barrier, <r, z> = ||t||^2 came with B's exchange
+                for_rows(n, [&](uint32_t i) { z[i] = dia_row<NDG>(a.GT, n, i, [&](uint32_t k) { return vld(t + k); }); });
+                if (!grid_sync(g, epoch, gs)) goto fail;
+#endif
                 continue;
             } else {
                 float* R = a.r[0];
