@@ -7,11 +7,15 @@
  * C++ raw-string delimiters the reference wraps them in. This header supplies
  * what OpenCL C takes from its runtime:
  *
- *   - work-items: one POSIX thread per work-item of a work-group; the
- *     work-groups of a launch run one after another, in group order, so the
- *     kernel's cross-group waits (the first long-row work-group releasing the
- *     others, csrmv_adaptive.cl:596-600, and the last one waiting for all,
- *     :651) are already satisfied when they are reached;
+ *   - work-items: on x86-64 one fiber per work-item on the calling thread
+ *     (a minimal stack switch below: callee-saved registers and the stack
+ *     pointer); barrier() yields, and the group's live work-items run round
+ *     by round from one barrier to the next, in work-item order, so a launch
+ *     is deterministic, atomics included. Elsewhere one POSIX thread per
+ *     work-item. The work-groups of a launch run one after another, in group
+ *     order, so the kernel's cross-group waits (the first long-row work-group
+ *     releasing the others, csrmv_adaptive.cl:596-600, and the last one
+ *     waiting for all, :651) are already satisfied when they are reached;
  *   - barrier(): waits for every work-item of the group that has not yet
  *     returned from the kernel (a returned work-item counts as arrived), which
  *     is how csrmv_general.cl's row loop behaves when the last group's
@@ -31,6 +35,7 @@
 #include <math.h>
 #include <pthread.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 /* ---- OpenCL C scalar type names */
@@ -41,12 +46,61 @@ typedef unsigned long ulong;
 static __thread unsigned clc_lid, clc_gid;
 static unsigned clc_ngroups, clc_wg_size;
 
+#if defined(__x86_64__)
+static unsigned clc_lid_f, clc_gid_f;
+static inline size_t get_local_id(unsigned d) { return d == 0 ? clc_lid_f : 0; }
+static inline size_t get_group_id(unsigned d) { return d == 0 ? clc_gid_f : 0; }
+#else
 static inline size_t get_local_id(unsigned d) { return d == 0 ? clc_lid : 0; }
 static inline size_t get_group_id(unsigned d) { return d == 0 ? clc_gid : 0; }
+#endif
 static inline size_t get_local_size(unsigned d) { return d == 0 ? clc_wg_size : 1; }
 static inline size_t get_num_groups(unsigned d) { return d == 0 ? clc_ngroups : 1; }
-static inline size_t get_global_id(unsigned d) { return d == 0 ? (size_t)clc_gid * clc_wg_size + clc_lid : 0; }
+static inline size_t get_global_id(unsigned d) { return d == 0 ? get_group_id(0) * clc_wg_size + get_local_id(0) : 0; }
 static inline size_t get_global_size(unsigned d) { return d == 0 ? (size_t)clc_ngroups * clc_wg_size : 1; }
+
+/* ---- fibers (x86-64): work-items as coroutines on the calling thread */
+typedef void (*clc_body_fn)(void *args);
+#if defined(__x86_64__)
+#define CLC_FIBERS 1
+void clc_swap(void **save_sp, void *const *load_sp);
+__asm__(".text\n"
+        ".p2align 4\n"
+        "clc_swap:\n"
+        "  pushq %rbp\n  pushq %rbx\n  pushq %r12\n  pushq %r13\n  pushq %r14\n  pushq %r15\n"
+        "  movq %rsp, (%rdi)\n"
+        "  movq (%rsi), %rsp\n"
+        "  popq %r15\n  popq %r14\n  popq %r13\n  popq %r12\n  popq %rbx\n  popq %rbp\n"
+        "  ret\n");
+
+#define CLC_MAX_WG 1024
+#define CLC_STACK (64 * 1024)
+static void *clc_sched_sp;
+static void *clc_fib_sp[CLC_MAX_WG];
+static int clc_fib_done[CLC_MAX_WG];
+static char *clc_stacks;
+static unsigned clc_cur;
+static clc_body_fn clc_fbody;
+static void *clc_fargs;
+static void clc_fiber_main(void)
+{
+    clc_fbody(clc_fargs);
+    clc_fib_done[clc_cur] = 1;
+    clc_swap(&clc_fib_sp[clc_cur], &clc_sched_sp); /* never resumed */
+    __builtin_unreachable();
+}
+
+static void clc_fiber_init(unsigned l)
+{
+    uintptr_t top = ((uintptr_t)(clc_stacks + (size_t)(l + 1) * CLC_STACK)) & ~(uintptr_t)15;
+    void **sp = (void **)top;
+    *--sp = 0;                          /* fake return address: entry sees rsp % 16 == 8 */
+    *--sp = (void *)clc_fiber_main;     /* popped by clc_swap's ret */
+    for (int k = 0; k < 6; k++) *--sp = 0; /* rbp rbx r12 r13 r14 r15 */
+    clc_fib_sp[l] = sp;
+    clc_fib_done[l] = 0;
+}
+#endif
 
 /* ---- barrier over the work-items of the group that are still running */
 static pthread_mutex_t clc_m = PTHREAD_MUTEX_INITIALIZER;
@@ -64,6 +118,10 @@ static void clc_release_locked(void)
 static void barrier(int flags)
 {
     (void)flags;
+#if defined(__x86_64__)
+    clc_swap(&clc_fib_sp[clc_cur], &clc_sched_sp); /* back to the group's scheduler */
+    return;
+#endif
     pthread_mutex_lock(&clc_m);
     clc_arrived++;
     if (clc_arrived == clc_active) {
@@ -124,7 +182,6 @@ static inline unsigned atomic_max(volatile unsigned *p, unsigned v)
 }
 
 /* ---- launch: ngroups work-groups of wg_size work-items, groups in order */
-typedef void (*clc_body_fn)(void *args);
 static clc_body_fn clc_body;
 static void *clc_args;
 static pthread_barrier_t clc_group_bar;
@@ -152,9 +209,45 @@ static void *clc_thread(void *arg)
     return NULL;
 }
 
+#if defined(__x86_64__)
+/* Runs every group's work-items as fibers: round by round, each live
+ * work-item runs to its next barrier or its end, in work-item order. */
+static int clc_launch_fibers(unsigned ngroups, unsigned wg_size, clc_body_fn body, void *args)
+{
+    if (wg_size == 0 || wg_size > CLC_MAX_WG) return -1;
+    if (!clc_stacks) {
+        clc_stacks = (char *)malloc((size_t)CLC_MAX_WG * CLC_STACK);
+        if (!clc_stacks) return -1;
+    }
+    clc_ngroups = ngroups;
+    clc_wg_size = wg_size;
+    clc_fbody = body;
+    clc_fargs = args;
+    for (unsigned g = 0; g < ngroups; g++) {
+        clc_gid_f = g;
+        for (unsigned l = 0; l < wg_size; l++) clc_fiber_init(l);
+        unsigned live = wg_size;
+        while (live > 0) {
+            live = 0;
+            for (unsigned l = 0; l < wg_size; l++) {
+                if (clc_fib_done[l]) continue;
+                clc_cur = l;
+                clc_lid_f = l;
+                clc_swap(&clc_sched_sp, &clc_fib_sp[l]);
+                if (!clc_fib_done[l]) live++;
+            }
+        }
+    }
+    return 0;
+}
+#endif
+
 /* Returns 0 on success. Not reentrant: one launch at a time per library. */
 static int clc_launch(unsigned ngroups, unsigned wg_size, clc_body_fn body, void *args)
 {
+#if defined(__x86_64__)
+    return clc_launch_fibers(ngroups, wg_size, body, args);
+#endif
     static pthread_mutex_t once = PTHREAD_MUTEX_INITIALIZER;
     pthread_mutex_lock(&once);
     clc_ngroups = ngroups;
@@ -186,6 +279,26 @@ static int clc_launch(unsigned ngroups, unsigned wg_size, clc_body_fn body, void
     pthread_barrier_destroy(&clc_group_bar);
     pthread_mutex_unlock(&once);
     return rc;
+}
+
+/* Launch of a kernel without barriers: the work-items run one after another
+ * on the calling thread (same results, far cheaper than a thread per
+ * work-item). */
+static int clc_launch_seq(unsigned ngroups, unsigned wg_size, clc_body_fn body, void *args)
+{
+    clc_ngroups = ngroups;
+    clc_wg_size = wg_size;
+    for (unsigned g = 0; g < ngroups; g++)
+        for (unsigned l = 0; l < wg_size; l++) {
+            clc_gid = g;
+            clc_lid = l;
+#if defined(__x86_64__)
+            clc_gid_f = g;
+            clc_lid_f = l;
+#endif
+            body(args);
+        }
+    return 0;
 }
 
 /* ---- OpenCL C keywords and build constants (after the shim's own code) */

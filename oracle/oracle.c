@@ -10,9 +10,12 @@
  * and, for the SpMV restatements, by tests/golden/spmv_ref.npz: the outputs
  * of the reference's own csrmv_adaptive / csrmv_general OpenCL kernels,
  * compiled from its sources and run on the host through oracle/clc_shim.h.
- * The CG / BiCGStab restatements are not pinned to reference outputs (the
- * reference's solvers need its OpenCL runtime); they are built from the
- * pinned SpMV and follow the reference's operation order line by line.
+ * The CG / BiCGStab restatements are pinned by tests/golden/solvers_ref.npz:
+ * runs of the reference's host solver code (its OpenCL runtime is not
+ * buildable here, so oracle/ref_solvers.py issues the same kernel sequence)
+ * over the reference's own SpMV, dot, reduce, blas1, transform and
+ * diagonal-extraction kernels, compiled from its sources and run on the
+ * host (oracle/_ref/librefblas1.so, librefspmv.so).
  *
  *   oracle_row_blocks  csr-meta.hpp:93-261 (ComputeRowBlocks, incl. the
  *                      trailing-block quirk) and :263-269 (size-only run)

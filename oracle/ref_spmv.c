@@ -14,6 +14,7 @@
 #include <math.h>
 #include <pthread.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #pragma GCC visibility push(hidden)
