@@ -248,3 +248,17 @@ SIGNATURES.update({
                                                C.c_void_p, cl_int, C.c_double, P(clsparseB200MixedInfo), P(cl_int),
                                                C.c_void_p]),
 })
+
+SIGNATURES.update({
+    "clsparseB200DistCgCreate": (clsparseStatus, [P(C.c_void_p), P(clsparseCsrMatrix), cl_uint, cl_uint, cl_int,
+                                                  C.c_void_p]),
+    "clsparseB200DistCgRelease": (clsparseStatus, [C.c_void_p]),
+    "clsparseB200DistCgBuffers": (clsparseStatus, [C.c_void_p, P(P(C.c_double)), P(P(C.c_double)),
+                                                   P(P(C.c_double))]),
+    "clsparseB200DistCgStart": (clsparseStatus, [C.c_void_p, P(cldenseVector), P(cldenseVector), C.c_void_p]),
+    "clsparseB200DistCgResidual": (clsparseStatus, [C.c_void_p, C.c_void_p]),
+    "clsparseB200DistCgProduct": (clsparseStatus, [C.c_void_p, C.c_void_p]),
+    "clsparseB200DistCgUpdate": (clsparseStatus, [C.c_void_p, cl_int, C.c_void_p, C.c_void_p]),
+    "clsparseB200DistCgState": (clsparseStatus, [C.c_void_p, P(cl_int), C.c_void_p, C.c_void_p]),
+    "clsparseB200DistCgGather": (clsparseStatus, [C.c_void_p, C.c_void_p, C.c_void_p, cl_uint, C.c_void_p]),
+})

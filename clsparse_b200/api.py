@@ -196,10 +196,12 @@ class SolverControl:
         r = lib().clsparseCreateSolverControl(precond, max_iters, rel_tol, abs_tol)
         check(r.status, "clsparseCreateSolverControl")
         self.handle = r.control
+        self.max_iters = int(max_iters)
 
     def set_params(self, precond, max_iters, rel_tol, abs_tol):
         check(lib().clsparseSetSolverParams(self.handle, precond, max_iters, rel_tol, abs_tol),
               "clsparseSetSolverParams")
+        self.max_iters = int(max_iters)
 
     def print_mode(self, mode):
         check(lib().clsparseSolverPrintMode(self.handle, mode), "clsparseSolverPrintMode")

@@ -237,6 +237,56 @@ cldenseDdotNoAlloc(clsparseScalar* r, const cldenseVector* x, const cldenseVecto
 CLSPARSE_EXPORT clsparseStatus
 clsparseB200SetSolverLoopMode(clsparseControl control, cl_int mode);
 
+/* ---- Row-partitioned FP64 CG, one rank's device work (multi-GPU) ----
+ * No counterpart in the reference (one queue per control,
+ * src/library/internal/clsparse-control.hpp:30-47); it replaces
+ * clsparseDcsrcg (include/clSPARSE.h:374-378) for a matrix split by rows
+ * over several GPUs. A rank holds its rows (columns renumbered into an
+ * "extended" vector of extLength entries whose entries ownOffset ..
+ * ownOffset + rows - 1 are the rank's own) and local x, b. Between the
+ * stages the caller moves data with its own collectives on the control's
+ * stream: the other ranks' entries of the extended vectors (xExt before
+ * Residual, zExt before every Product) and a sum over ranks of the four
+ * FP64 `sums` before every Update. One solve:
+ *   Start; exchange xExt; Residual; exchange zExt; Product; all-reduce sums;
+ *   for step = 0, 1, ...: Update(step); exchange zExt; Product; all-reduce
+ *   sums; and every few steps State, until it reports done.
+ * The iteration is CG in the Chronopoulos-Gear form (one all-reduce per
+ * step), with the reference's L1 stop test, residuals and nIters
+ * (conjugate-gradients.hpp:65-226, solver-control.hpp:47-64); the decisions
+ * are taken on the device and steps after the finish do nothing, so State
+ * is the only host synchronisation. */
+typedef struct _clsparseB200DistCg* clsparseB200DistCg;
+
+/* Local rows (FP64, num_cols ignored); precond DIAGONAL or NOPRECOND.
+ * clsparseInvalidValue if a column is >= extLength or, with DIAGONAL, a
+ * row's diagonal (column ownOffset + row) is missing or zero. */
+CLSPARSE_EXPORT clsparseStatus
+clsparseB200DistCgCreate(clsparseB200DistCg* handle, const clsparseCsrMatrix* localRows, cl_uint extLength,
+                         cl_uint ownOffset, cl_int precond, clsparseControl control);
+CLSPARSE_EXPORT clsparseStatus clsparseB200DistCgRelease(clsparseB200DistCg handle);
+/* Device addresses of the extended vectors and of the four sums. */
+CLSPARSE_EXPORT clsparseStatus
+clsparseB200DistCgBuffers(clsparseB200DistCg handle, cl_double** xExt, cl_double** zExt, cl_double** sums);
+/* Binds x (updated in place) and b; copies x into xExt's own entries. */
+CLSPARSE_EXPORT clsparseStatus
+clsparseB200DistCgStart(clsparseB200DistCg handle, cldenseVector* x, const cldenseVector* b, clsparseControl control);
+CLSPARSE_EXPORT clsparseStatus clsparseB200DistCgResidual(clsparseB200DistCg handle, clsparseControl control);
+CLSPARSE_EXPORT clsparseStatus clsparseB200DistCgProduct(clsparseB200DistCg handle, clsparseControl control);
+/* Tolerances and iteration limit from solverControl. */
+CLSPARSE_EXPORT clsparseStatus
+clsparseB200DistCgUpdate(clsparseB200DistCg handle, cl_int step, clSParseSolverControl solverControl,
+                         clsparseControl control);
+/* Waits for the stream; *done = 1 once finished; fills solverControl's
+ * nIters and residuals (clsparseB200SolverGetInfo). */
+CLSPARSE_EXPORT clsparseStatus
+clsparseB200DistCgState(clsparseB200DistCg handle, cl_int* done, clSParseSolverControl solverControl,
+                        clsparseControl control);
+/* dst[i] = src[idx[i]] for i < count (packs entries to send). */
+CLSPARSE_EXPORT clsparseStatus
+clsparseB200DistCgGather(cl_double* dst, const cl_double* src, const cl_uint* idx, cl_uint count,
+                         clsparseControl control);
+
 #ifdef __cplusplus
 }
 #endif

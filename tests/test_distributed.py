@@ -1,8 +1,9 @@
 """The multi-GPU host logic (clsparse_b200.distributed) on CPU: partitions,
-and the row-partitioned CG and the batched sharding run as a world-size-2
-gloo process group (spawned processes, 127.0.0.1) with the local SpMV done by
-scipy. A rank that leaves is noticed by the others through a failing
-collective (the process group's timeout), not by a hang."""
+exchange plans, and the row-partitioned CG driver and the batched sharding
+run as a world-size-2 gloo process group (spawned processes, 127.0.0.1) with
+the rank's kernels replaced by a CPU stand-in (tests/dist_host_rank.py). A
+rank that leaves is noticed by the others through a failing collective (the
+process group's timeout), not by a hang."""
 from __future__ import annotations
 
 import os
@@ -10,8 +11,6 @@ import socket
 
 import numpy as np
 import pytest
-import scipy.sparse as sp
-import scipy.sparse.linalg as spla
 import torch.multiprocessing as mp
 
 from clsparse_b200 import distributed as D
@@ -46,31 +45,57 @@ def _problem():
     return rp, col, val, b
 
 
-def _rank_main(rank, world, port, q):
-    """Row-partitioned CG, then the batched sharding, on one gloo group."""
+def _cg_problems():
+    """(name, rp, col, val, b, precond, max_iters, rel): a stencil (halo
+    exchange), an irregular matrix (all-gather), the iteration limit, no
+    preconditioner and a zero right-hand side."""
+    rp, col, val, b = _problem()
+    rs = matgen.random_spd(3000, per_row=8, seed=4)
+    bs = np.random.default_rng(5).uniform(-1, 1, 3000)
+    return [("stencil", rp, col, val, b, 1, 5000, 1e-10),
+            ("irregular", *rs, bs, 1, 5000, 1e-10),
+            ("limit", rp, col, val, b, 1, 5, 1e-10),
+            ("none", rp, col, val, b, 0, 5000, 1e-8),
+            ("zero_b", rp, col, val, np.zeros_like(b), 1, 100, 1e-10)]
+
+
+def _host_cg(rp, col, val, b, precond, max_iters, rel, parts, ranks_here, plans, comm):
+    """Runs the driver over HostRank stand-ins for the ranks in ranks_here;
+    returns (info, [x of each rank])."""
     import torch
+    from dist_host_rank import HostRank, HostSolverControl
+    rks, xs, bs, scs = [], [], [], []
+    for k in ranks_here:
+        lrp, lcol, lval = D.setup_local(rp, col, val, parts, k, plans[k])
+        rks.append(HostRank(plans[k], lrp, lcol, lval, precond))
+        r0, r1 = parts[k]
+        xs.append(torch.zeros(r1 - r0, dtype=torch.float64))
+        bs.append(torch.tensor(b[r0:r1]))
+        scs.append(HostSolverControl(precond, max_iters, rel, 0.0))
+    info = D.dist_cg(rks, comm, xs, bs, scs, check_every=4)
+    return info, [x.numpy() for x in xs]
+
+
+def _rank_main(rank, world, port, q):
+    """Row-partitioned CG (gloo, CPU stand-in kernels), then the batched
+    sharding, on one gloo group."""
     dist = _init(rank, world, port)
     try:
-        rp, col, val, b = _problem()
-        n = len(rp) - 1
-        parts = D.row_partition(rp, world)
-        r0, r1 = parts[rank]
-        lrp, lcol, lval = D.local_rows(rp, col, val, r0, r1)
-        Aloc = sp.csr_matrix((lval, lcol.astype(np.int64), lrp.astype(np.int64)), shape=(r1 - r0, n))
-        A = sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64)), shape=(n, n))
-        dinv = torch.tensor(1.0 / A.diagonal()[r0:r1])
-
-        def spmv(p_full):
-            return torch.from_numpy(Aloc @ p_full.numpy())
-
-        x, it, res = D.dist_cg(spmv, torch.tensor(b[r0:r1]), dinv, parts, rel_tol=1e-10, max_iters=5000)
-        xs = D.all_gather_rows(x, parts).numpy()
+        out = {}
+        for name, rp, col, val, b, pre, mi, rel in _cg_problems():
+            parts = D.row_partition(rp, world)
+            r0, r1 = parts[rank]
+            _, lcol, _ = D.local_rows(rp, col, val, r0, r1)
+            plan = D.plan_for_rank(lcol, parts, rank)
+            plans = {rank: plan}
+            info, (x,) = _host_cg(rp, col, val, b, pre, mi, rel, parts, [rank], plans, D.TorchComm())
+            out[name] = (info, x, plan.mode)
 
         def solve_share(idx):
             return [[10.0 * i, float(rank)] for i in idx]
 
         gathered = D.dist_batched(solve_share, [7, 1, 5, 5, 2, 9, 3])
-        q.put((rank, it, res, xs, gathered))
+        q.put((rank, out, gathered))
     finally:
         dist.destroy_process_group()
         _finish(q)
@@ -106,29 +131,6 @@ def _spawn(target, world):
     return sorted(out, key=lambda t: t[0]), procs
 
 
-def _serial_cg(A, b, tol=1e-10, max_iters=5000):
-    """The same Jacobi-PCG on one process (reference for the iteration count)."""
-    dinv = 1.0 / A.diagonal()
-    x = np.zeros_like(b)
-    r = b.copy()
-    z = r * dinv
-    p = z.copy()
-    rz = r @ z
-    nb = np.linalg.norm(b)
-    for it in range(1, max_iters + 1):
-        q = A @ p
-        alpha = rz / (p @ q)
-        x += alpha * p
-        r -= alpha * q
-        z = r * dinv
-        rz_new = r @ z
-        if np.linalg.norm(r) / nb <= tol:
-            return x, it
-        p = z + (rz_new / rz) * p
-        rz = rz_new
-    return x, max_iters
-
-
 def test_row_partition_balances_nonzeros():
     rp, _, _ = matgen.irregular(50_000, n_dense=3, dense_len=10_000, seed=3)
     for world in (1, 2, 3, 8):
@@ -157,25 +159,80 @@ def two_ranks():
     return out
 
 
-def test_distributed_cg_matches_single_rank(two_ranks):
-    rp, col, val, b = _problem()
+@pytest.mark.parametrize("name", ["stencil", "irregular", "limit", "none", "zero_b"])
+def test_distributed_cg_matches_single_rank(two_ranks, orc, name):
+    """The gloo world-size-2 run (one process per rank, CPU stand-in kernels)
+    against the same driver with one rank and with both ranks in one process
+    (LocalComm), and against the oracle's reference-order CG."""
+    (_, rp, col, val, b, pre, mi, rel), = [p for p in _cg_problems() if p[0] == name]
     n = len(rp) - 1
-    A = sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64)), shape=(n, n))
-    _, it1 = _serial_cg(A, b)
-    its = {t[1] for t in two_ranks}
-    assert len(its) == 1  # every rank took the same stop decision
-    assert abs(its.pop() - it1) <= 1 and all(t[2] <= 1e-10 for t in two_ranks)
-    xd = spla.spsolve(A.tocsc(), b)
-    for t in two_ranks:
-        assert np.linalg.norm(t[3] - xd) / np.linalg.norm(xd) <= 1e-7
-        np.testing.assert_array_equal(t[3], two_ranks[0][3])
+    parts1 = D.row_partition(rp, 1)
+    plans1 = D.make_plans([D.needed_columns(col, 0, n)], parts1)
+    info1, (x1,) = _host_cg(rp, col, val, b, pre, mi, rel, parts1, [0], plans1, D.LocalComm())
+    parts2 = D.row_partition(rp, 2)
+    needed = [D.needed_columns(D.local_rows(rp, col, val, *parts2[k])[1], *parts2[k]) for k in range(2)]
+    plans2 = D.make_plans(needed, parts2)
+    info2, xs2 = _host_cg(rp, col, val, b, pre, mi, rel, parts2, [0, 1], plans2, D.LocalComm())
+    x2 = np.concatenate(xs2)
+    want_mode = {"irregular": D.ALLGATHER}.get(name, D.HALO)
+    for rank, out, _ in two_ranks:
+        info, x, mode = out[name]
+        assert mode == want_mode
+        r0, r1 = parts2[rank]
+        # the process-per-rank run is the in-process two-rank run, bit for bit
+        assert info == info2
+        np.testing.assert_array_equal(x, x2[r0:r1])
+    assert info2["nIters"] == info1["nIters"]
+    assert info2["initialResidual"] == pytest.approx(info1["initialResidual"], rel=1e-13)
+    scale = max(np.abs(x1).max(), 1e-300)
+    assert np.abs(x2 - x1).max() <= 1e-9 * scale
+    xo, oi = orc.solve("cg", np.float64, rp, col, val, np.zeros(n), b, pre, mi, rel, 0.0)
+    assert abs(info1["nIters"] - oi.nIters) <= 1, (info1, oi.nIters)
+    assert info1["initialResidual"] == pytest.approx(oi.initialResidual, rel=1e-13)
+    if name == "zero_b":
+        assert info1["nIters"] == 0 and not x1.any()
+    elif name == "limit":
+        assert info1["nIters"] == 5
+    else:
+        assert info1["currentResidual"] <= rel
+        assert np.abs(x1 - xo).max() <= 1e-6 * max(np.abs(xo).max(), 1e-300)
+
+
+def test_exchange_plans_cover_every_column():
+    """Every column a rank's rows reference maps into its extended vector,
+    onto the entry that holds that global column after the exchange."""
+    for rp, col, val in (matgen.poisson2d(40), matgen.random_spd(2000, seed=2),
+                         matgen.irregular(3000, n_dense=3, dense_len=1000, seed=1)):
+        n = len(rp) - 1
+        for world in (2, 3, 5):
+            parts = D.row_partition(rp, world)
+            needed = [D.needed_columns(D.local_rows(rp, col, val, *parts[k])[1], *parts[k]) for k in range(world)]
+            for mode in (D.HALO, D.ALLGATHER):
+                plans = D.make_plans(needed, parts, mode)
+                g = np.arange(n, dtype=np.float64)  # entry value = global column
+                for k in range(world):
+                    p = plans[k]
+                    ext = np.full(p.ext_len, -1.0)
+                    r0, r1 = parts[k]
+                    ext[p.own:p.own + r1 - r0] = g[r0:r1]
+                    if mode == D.HALO:
+                        for q, (off, cnt) in p.recv.items():
+                            src = plans[q].send[k] + parts[q][0]
+                            assert len(src) == cnt
+                            ext[off:off + cnt] = g[src]
+                    else:
+                        for q in range(world):
+                            a, b = parts[q]
+                            ext[q * p.chunk:q * p.chunk + b - a] = g[a:b]
+                    _, lcol, _ = D.local_rows(rp, col, val, r0, r1)
+                    np.testing.assert_array_equal(ext[p.ext_columns(lcol)], lcol.astype(np.float64))
 
 
 def test_distributed_batched_gathers_every_system(two_ranks):
     shares = D.lpt_partition([7, 1, 5, 5, 2, 9, 3], 2)
     owner = {int(i): r for r, s in enumerate(shares) for i in s}
     for t in two_ranks:
-        res = t[4]
+        res = t[2]
         np.testing.assert_array_equal(res[:, 0], 10.0 * np.arange(7))
         np.testing.assert_array_equal(res[:, 1], [owner[i] for i in range(7)])
 
