@@ -1111,22 +1111,9 @@ clsparseStatus build_graph(_clsparseB200Spai* net, const clsparseCsrMatrix* A, c
     node_features<<<nblk(n, 256), 256, 0, s>>>(gr.rp, gr.cols, gr.ehat, gr.F, n);
     if (cudaGetLastError() != cudaSuccess || !read_info(gr, s, h)) return clsparseInvalidKernelExecution;
     if (h[0] != 0) return clsparseInvalidValue;
-    {
-        clsparseCsrMatrix pat;
-        std::memset(&pat, 0, sizeof(pat));
-        pat.num_rows = n;
-        pat.num_cols = n;
-        pat.num_nonzeros = gr.nnzL;
-        pat.row_pointer = gr.Lrp;
-        pat.col_indices = gr.Lcol;
-        if (clsparseCsrMetaCreate(&pat, c) != clsparseSuccess) return clsparseOutOfResources;
-        gr.metaL = static_cast<matrix_meta*>(pat.meta);
-        pat.meta = nullptr;
-        pat.row_pointer = gr.LTrp;
-        pat.col_indices = gr.LTrow;
-        if (clsparseCsrMetaCreate(&pat, c) != clsparseSuccess) return clsparseOutOfResources;
-        gr.metaLT = static_cast<matrix_meta*>(pat.meta);
-    }
+    // The CSR-Adaptive metas of the patterns of G and G^T are made when a
+    // CSR solve first needs them (spai_ensure_metas): their row blocks are
+    // computed on the host, and the banded inner solves do without them.
     gr.built = true;
     return clsparseSuccess;
 }
@@ -1196,7 +1183,9 @@ bool umma_failed() {
     return h != 0;
 }
 
-void forward(_clsparseB200Spai* net, int bf16, cudaStream_t s) {
+// keep_act: store the pre-activations Au the backward pass reads (training);
+// the factor build skips those writes.
+void forward(_clsparseB200Spai* net, int bf16, cudaStream_t s, bool keep_act = true) {
     Graph& gr = net->gr;
     const Offsets& o = net->o;
     const float* P = net->prm;
@@ -1216,8 +1205,8 @@ void forward(_clsparseB200Spai* net, int bf16, cudaStream_t s) {
         message_fwd<<<warps_grid(n), 256, 0, s>>>(gr.rp, gr.cols, gr.ehat, gr.Hu[l], P + o.w[l], P + o.c[l],
                                                   gr.S[l], gr.n, bf16);
         if (bf16)
-            launch_umma<H, H, H>(gr.Hs[l], gr.S[l], P + o.V[l], P + o.d[l], gr.Hs[l], gr.Hs[l + 1], gr.Au[l], n, 1,
-                                 dev, s);
+            launch_umma<H, H, H>(gr.Hs[l], gr.S[l], P + o.V[l], P + o.d[l], gr.Hs[l], gr.Hs[l + 1],
+                                 keep_act ? gr.Au[l] : nullptr, n, 1, dev, s);
         else
             linear_fwd<H, H, H><<<tiles, 256, 0, s>>>(gr.Hs[l], gr.S[l], P + o.V[l], P + o.d[l], gr.Hs[l],
                                                       gr.Hs[l + 1], gr.Au[l], n, 1, bf16);
@@ -1489,7 +1478,7 @@ clsparseStatus clsparseB200SpaiBuild(clsparseB200Spai net, clsparseControl contr
     clsparseStatus st = check_net(net, control, true);
     if (st != clsparseSuccess) return st;
     DeviceGuard g(control->device);
-    forward(net, 1, control->stream);
+    forward(net, 1, control->stream, false);
     export_g(net, control->stream);
     if (cudaStreamSynchronize(control->stream) != cudaSuccess || umma_failed())
         return clsparseInvalidKernelExecution;
@@ -1563,7 +1552,34 @@ clsparseStatus clsparseB200SpaiLoad(clsparseB200Spai net, const char* path) {
 
 namespace clsp {
 
-// Views of the exported factor for the solvers (mixed.cu).
+// The CSR-Adaptive metas of the patterns of G (tril(A)) and G^T, made on
+// first use after a graph build.
+clsparseStatus spai_ensure_metas(clsparseB200Spai net, clsparseControl c) {
+    if (net == nullptr || !net->gr.built) return clsparseStructInvalid;
+    Graph& gr = net->gr;
+    if (gr.metaL != nullptr && gr.metaLT != nullptr) return clsparseSuccess;
+    delete gr.metaL;
+    delete gr.metaLT;
+    gr.metaL = gr.metaLT = nullptr;
+    clsparseCsrMatrix pat;
+    std::memset(&pat, 0, sizeof(pat));
+    pat.num_rows = gr.n;
+    pat.num_cols = gr.n;
+    pat.num_nonzeros = gr.nnzL;
+    pat.row_pointer = gr.Lrp;
+    pat.col_indices = gr.Lcol;
+    if (clsparseCsrMetaCreate(&pat, c) != clsparseSuccess) return clsparseOutOfResources;
+    gr.metaL = static_cast<matrix_meta*>(pat.meta);
+    pat.meta = nullptr;
+    pat.row_pointer = gr.LTrp;
+    pat.col_indices = gr.LTrow;
+    if (clsparseCsrMetaCreate(&pat, c) != clsparseSuccess) return clsparseOutOfResources;
+    gr.metaLT = static_cast<matrix_meta*>(pat.meta);
+    return clsparseSuccess;
+}
+
+// Views of the exported factor for the solvers (mixed.cu); the metas are null
+// until spai_ensure_metas.
 bool spai_factor_views(clsparseB200Spai net, CsrView<__nv_bfloat16>& G16, CsrView<__nv_bfloat16>& GT16,
                        CsrView<float>& G32, CsrView<float>& GT32, CsrView<double>& G64, CsrView<double>& GT64) {
     if (net == nullptr || !net->gr.built) return false;

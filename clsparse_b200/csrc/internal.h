@@ -246,6 +246,8 @@ clsparseStatus pcg_factor_typed(cldenseVector* x, const clsparseCsrMatrix* A, co
                                 clsparseControl c, WarmStart* ws = nullptr);
 
 // Device views of a learned factor G (L = tril(A) order) and G^T (gnn.cu).
+// CSR-Adaptive metas of the factor's patterns, made on first use (gnn.cu).
+clsparseStatus spai_ensure_metas(clsparseB200Spai net, clsparseControl c);
 bool spai_factor_views(clsparseB200Spai net, CsrView<__nv_bfloat16>& G16, CsrView<__nv_bfloat16>& GT16,
                        CsrView<float>& G32, CsrView<float>& GT32, CsrView<double>& G64,
                        CsrView<double>& GT64);

@@ -84,6 +84,7 @@ MixedWork& work_of(clsparseControl c) {
 // Learned factor M^-1 = G^T G for the inner solves (null: Jacobi).
 struct Factor {
     CsrView<__nv_bfloat16> G, GT;
+    clsparseB200Spai net = nullptr;  // owner of the views (metas made on first CSR use)
 };
 
 // The inner CG solves on diagonal storage (dia.cu) when A -- and the learned
@@ -223,6 +224,18 @@ clsparseStatus refine(cldenseVector* xv, const clsparseCsrMatrix* A, const clden
     if (method == Inner::Cg)
         setup_banded<V>(bi, A, factor, w, sc->preconditioner == DIAGONAL, c);
     if (!bi.on) round_values_kernel<V><<<grid_for(nnz, c->sm_count), kThreads, 0, s>>>(Avals, lv, nnz);
+    Factor csr_factor;
+    if (factor != nullptr && !bi.on && factor->net != nullptr && (!factor->G.meta || !factor->GT.meta)) {
+        // the CSR inner solves apply G and G^T with their CSR-Adaptive metas
+        const clsparseStatus ms = spai_ensure_metas(factor->net, c);
+        if (ms != clsparseSuccess) return ms;
+        CsrView<float> g32, gt32;
+        CsrView<double> g64, gt64;
+        csr_factor.net = factor->net;
+        if (!spai_factor_views(factor->net, csr_factor.G, csr_factor.GT, g32, gt32, g64, gt64))
+            return clsparseStructInvalid;
+        factor = &csr_factor;
+    }
 
     // FP64 operator and the low-precision copy sharing its structure and meta
     CsrView<double> A64{Avals, dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices),
@@ -413,6 +426,9 @@ clsparseStatus clsparseDcsrcgLearned(cldenseVector* x, const clsparseCsrMatrix* 
     int fb = 0;
     DeviceGuard g(control->device);
     if (innerPrecision == 2) {
+        st = spai_ensure_metas(spai, control);
+        if (st != clsparseSuccess) return st;
+        spai_factor_views(spai, G16, GT16, G32, GT32, G64, GT64);
         // plain FP64 PCG with M^-1 = G^T G, L2 stop test on the recursive residual
         _solverControl sc = *solverControl;
         sc.normType = 1;
@@ -429,7 +445,7 @@ clsparseStatus clsparseDcsrcgLearned(cldenseVector* x, const clsparseCsrMatrix* 
         return clsparseSuccess;
     }
     if (innerPrecision != 0 && innerPrecision != 1) return clsparseInvalidType;
-    Factor f{G16, GT16};
+    Factor f{G16, GT16, spai};
     if (innerPrecision == 0)
         st = refine<float>(x, A, b, solverControl, innerTolerance, info, control, &f, &fb);
     else
