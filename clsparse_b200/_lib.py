@@ -262,3 +262,14 @@ SIGNATURES.update({
     "clsparseB200DistCgState": (clsparseStatus, [C.c_void_p, P(cl_int), C.c_void_p, C.c_void_p]),
     "clsparseB200DistCgGather": (clsparseStatus, [C.c_void_p, C.c_void_p, C.c_void_p, cl_uint, C.c_void_p]),
 })
+
+SIGNATURES.update({
+    "clsparseB200SolverSetHistory": (clsparseStatus, [C.c_void_p, C.c_void_p, cl_uint]),
+    "clsparseB200SolverGetHistoryLength": (clsparseStatus, [C.c_void_p, P(cl_uint)]),
+    "clsparseB200SolverSetSnapshots": (clsparseStatus, [C.c_void_p, P(cl_int), cl_int, C.c_void_p]),
+})
+
+SIGNATURES.update({
+    "clsparseB200SpaiGradient": (clsparseStatus, [C.c_void_p, P(P(C.c_float)), P(C.c_size_t)]),
+    "clsparseB200SpaiAdamStep": (clsparseStatus, [C.c_void_p, C.c_double, C.c_double, C.c_void_p]),
+})

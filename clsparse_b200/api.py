@@ -217,6 +217,34 @@ class SolverControl:
         """1: the reference's ||r||_1/||b||_1 stop test, 2: ||r||_2/||b||_2."""
         check(lib().clsparseB200SolverSetNormType(self.handle, norm), "clsparseB200SolverSetNormType")
 
+    def set_history(self, hist: torch.Tensor | None):
+        """Records the residuum of the start and of every iteration of the
+        next solves into the FP64 device tensor hist (None: off)."""
+        if hist is None:
+            check(lib().clsparseB200SolverSetHistory(self.handle, None, 0), "clsparseB200SolverSetHistory")
+            return
+        assert hist.dtype == torch.float64 and hist.is_cuda and hist.is_contiguous()
+        self._hist = hist
+        check(lib().clsparseB200SolverSetHistory(self.handle, C.c_void_p(hist.data_ptr()), hist.numel()),
+              "clsparseB200SolverSetHistory")
+
+    def history_length(self) -> int:
+        n = L.cl_uint()
+        check(lib().clsparseB200SolverGetHistoryLength(self.handle, C.byref(n)), "GetHistoryLength")
+        return n.value
+
+    def set_snapshots(self, iterations, vectors: torch.Tensor | None):
+        """Keeps the CG residual vector after each listed iteration count in
+        the rows of vectors (len(iterations) x n, the solve's dtype)."""
+        if vectors is None or not len(iterations):
+            check(lib().clsparseB200SolverSetSnapshots(self.handle, None, 0, None), "clsparseB200SolverSetSnapshots")
+            return
+        assert vectors.is_cuda and vectors.is_contiguous() and vectors.shape[0] == len(iterations)
+        self._snap = vectors
+        its = (L.cl_int * len(iterations))(*[int(k) for k in iterations])
+        check(lib().clsparseB200SolverSetSnapshots(self.handle, its, len(iterations), C.c_void_p(vectors.data_ptr())),
+              "clsparseB200SolverSetSnapshots")
+
     def device_status(self) -> int:
         b = L.cl_uint()
         check(lib().clsparseB200SolverGetDeviceStatus(self.handle, C.byref(b)), "GetDeviceStatus")
@@ -360,6 +388,31 @@ class Spai:
         check(lib().clsparseB200SpaiTrainStep(self.handle, pv, K, lam, lr, C.byref(loss), ctrl.handle),
               "clsparseB200SpaiTrainStep")
         return loss.value
+
+    def loss_grad_device(self, ctrl: Control, probes: torch.Tensor | None = None, lam: float = 0.0) -> float:
+        """Loss and gradient at the current weights, the gradient left in the
+        network's device buffer (grad_buffer) with no host copy."""
+        pv, K = self._probes(probes)
+        loss = C.c_double()
+        check(lib().clsparseB200SpaiLossGrad(self.handle, pv, K, lam, 0, C.byref(loss), None, 0, ctrl.handle),
+              "clsparseB200SpaiLossGrad")
+        return loss.value
+
+    def grad_buffer(self) -> torch.Tensor:
+        """The device gradient buffer as a float32 tensor (a view)."""
+        p = C.POINTER(C.c_float)()
+        n = C.c_size_t()
+        check(lib().clsparseB200SpaiGradient(self.handle, C.byref(p), C.byref(n)), "clsparseB200SpaiGradient")
+
+        class _View:
+            pass
+        v = _View()
+        v.__cuda_array_interface__ = {"shape": (n.value,), "typestr": "<f4",
+                                      "data": (C.cast(p, C.c_void_p).value, False), "version": 3, "strides": None}
+        return torch.as_tensor(v, device="cuda")
+
+    def adam_step(self, ctrl: Control, lr: float, grad_scale: float = 1.0):
+        check(lib().clsparseB200SpaiAdamStep(self.handle, lr, grad_scale, ctrl.handle), "clsparseB200SpaiAdamStep")
 
     def build(self, ctrl: Control):
         check(lib().clsparseB200SpaiBuild(self.handle, ctrl.handle), "clsparseB200SpaiBuild")

@@ -263,6 +263,36 @@ clsparseStatus clsparseB200SolverGetInfo(clSParseSolverControl s, cl_int* nIters
     return clsparseSuccess;
 }
 
+clsparseStatus clsparseB200SolverSetHistory(clSParseSolverControl s, cl_double* history, cl_uint capacity) {
+    if (s == nullptr) return clsparseInvalidSolverControlObject;
+    if (history == nullptr && capacity != 0) return clsparseInvalidValue;
+    if (capacity > 0x7fffffffu) return clsparseInvalidSize;
+    s->history = history;
+    s->historyCapacity = history ? capacity : 0;
+    s->historyLength = 0;
+    return clsparseSuccess;
+}
+
+clsparseStatus clsparseB200SolverGetHistoryLength(clSParseSolverControl s, cl_uint* length) {
+    if (s == nullptr) return clsparseInvalidSolverControlObject;
+    if (length == nullptr) return clsparseInvalidValue;
+    *length = s->historyLength;
+    return clsparseSuccess;
+}
+
+clsparseStatus clsparseB200SolverSetSnapshots(clSParseSolverControl s, const cl_int* iterations, cl_int count,
+                                              void* vectors) {
+    if (s == nullptr) return clsparseInvalidSolverControlObject;
+    if (count < 0 || count > 8) return clsparseInvalidSize;
+    if (count > 0 && (iterations == nullptr || vectors == nullptr)) return clsparseInvalidValue;
+    for (int k = 0; k < count; ++k)
+        if (iterations[k] < 0) return clsparseInvalidValue;
+    s->snapshotCount = count;
+    for (int k = 0; k < 8; ++k) s->snapshotIters[k] = k < count ? iterations[k] : -1;
+    s->snapshots = count > 0 ? vectors : nullptr;
+    return clsparseSuccess;
+}
+
 clsparseStatus clsparseB200SolverGetDeviceStatus(clSParseSolverControl s, cl_uint* bits) {
     if (s == nullptr) return clsparseInvalidSolverControlObject;
     if (bits) *bits = s->deviceStatus;

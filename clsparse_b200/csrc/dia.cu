@@ -163,6 +163,23 @@ __global__ void dia_fill_kernel(const uint32_t* __restrict__ rp, const uint32_t*
     }
 }
 
+// diag32[i] = a_ii + sum_{j != i} (a_ij - round_V(a_ij)) (FP64 sum, FP32
+// result); the main diagonal of the V copy (index d0) set to zero.
+template <typename V>
+__global__ void dia_comp_diag_kernel(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols,
+                                     const double* __restrict__ vals, uint32_t n, V* __restrict__ main_diag,
+                                     float* __restrict__ diag32) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double d = 0.0;
+        for (uint32_t k = rp[i]; k < rp[i + 1]; ++k) {
+            const double a = vals[k];
+            d += cols[k] == i ? a : a - static_cast<double>(widen(narrow<V>(a)));
+        }
+        diag32[i] = static_cast<float>(d);
+        main_diag[i] = narrow<V>(0.0);
+    }
+}
+
 // invD[i] = 1 / a_ii from the main diagonal of a DIA matrix; status |=
 // kStatusZeroDiag where it is zero.
 template <typename V>
@@ -210,6 +227,7 @@ __device__ __forceinline__ float dia_row(const DiaMat<V>& M, uint32_t n, uint32_
     float s = 0.f;
 #pragma unroll
     for (int d = 0; d < ND; ++d) s = fmaf(av[d], xv[d], s);
+    if (M.diag32 != nullptr) s = fmaf(__ldg(M.diag32 + i), xf(i), s);
     return s;
 }
 
@@ -517,15 +535,40 @@ clsparseStatus dia_build(const uint32_t* rp, const uint32_t* cols, const VI* val
     return clsparseSuccess;
 }
 
+// Index of the main diagonal among a DIA matrix's offsets: the first zero
+// offset (padding diagonals, also at offset 0, come after the real ones).
+template <typename V>
+int main_diag_index(const DiaMat<V>& A) {
+    int d0 = -1;
+    for (int d = A.nd - 1; d >= 0; --d)
+        if (A.off[d] == 0) d0 = d;
+    return d0;
+}
+
 template <typename VA>
 clsparseStatus dia_jacobi(const DiaMat<VA>& A, uint32_t n, float* invD, int* status, cudaStream_t s) {
-    int d0 = -1;
-    for (int d = 0; d < A.nd; ++d)
-        if (A.off[d] == 0) d0 = d;
-    if (d0 < 0) return clsparseInvalidValue;  // no main diagonal: the CSR path reports it
     const uint32_t grid = std::min<uint32_t>((n + 255) / 256, 1184);
+    if (A.diag32 != nullptr) {
+        dia_inv_diag_kernel<float><<<grid, 256, 0, s>>>(A.diag32, n, invD, status);
+        return cudaGetLastError() == cudaSuccess ? clsparseSuccess : clsparseInvalidKernelExecution;
+    }
+    const int d0 = main_diag_index(A);
+    if (d0 < 0) return clsparseInvalidValue;  // no main diagonal: the CSR path reports it
     dia_inv_diag_kernel<VA><<<grid, 256, 0, s>>>(A.vals + static_cast<size_t>(d0) * n, n, invD, status);
     return cudaGetLastError() == cudaSuccess ? clsparseSuccess : clsparseInvalidKernelExecution;
+}
+
+template <typename V>
+clsparseStatus dia_compensate_diag(const uint32_t* rp, const uint32_t* cols, const double* vals, uint32_t n,
+                                   DiaMat<V>& A, float* diag32, cudaStream_t s) {
+    const int d0 = main_diag_index(A);
+    if (d0 < 0 || diag32 == nullptr) return clsparseInvalidValue;
+    V* main_diag = const_cast<V*>(A.vals) + static_cast<size_t>(d0) * n;
+    const uint32_t grid = std::min<uint32_t>((n + 255) / 256, 1184);
+    dia_comp_diag_kernel<V><<<grid, 256, 0, s>>>(rp, cols, vals, n, main_diag, diag32);
+    if (cudaGetLastError() != cudaSuccess) return clsparseInvalidKernelExecution;
+    A.diag32 = diag32;
+    return clsparseSuccess;
 }
 
 void dia_classes(int nda, int ndg, bool learned, int& ca, int& cg) {
@@ -623,6 +666,10 @@ template clsparseStatus dia_build<__nv_bfloat16, __nv_bfloat16>(const uint32_t*,
                                                                 const __nv_bfloat16*, uint32_t, const DiaOffsets&,
                                                                 int, DeviceBuffer&, cudaStream_t,
                                                                 DiaMat<__nv_bfloat16>&);
+template clsparseStatus dia_compensate_diag<float>(const uint32_t*, const uint32_t*, const double*, uint32_t,
+                                                    DiaMat<float>&, float*, cudaStream_t);
+template clsparseStatus dia_compensate_diag<__nv_bfloat16>(const uint32_t*, const uint32_t*, const double*, uint32_t,
+                                                            DiaMat<__nv_bfloat16>&, float*, cudaStream_t);
 template clsparseStatus dia_jacobi<float>(const DiaMat<float>&, uint32_t, float*, int*, cudaStream_t);
 template clsparseStatus dia_jacobi<__nv_bfloat16>(const DiaMat<__nv_bfloat16>&, uint32_t, float*, int*,
                                                   cudaStream_t);

@@ -27,6 +27,9 @@ struct DiaMat {
     const V* vals = nullptr;
     int nd = 0;
     int32_t off[kMaxDiags] = {};
+    // When set, the main diagonal in FP32 (its entries in vals are zero):
+    // the row-sum-compensated diagonal of a BF16-valued copy (dia_compensate_diag).
+    const float* diag32 = nullptr;
 };
 
 // In/out block of one inner solve (device copy written before the launch,
@@ -81,6 +84,18 @@ void dia_classes(int nda, int ndg, bool learned, int& ca, int& cg);
 template <typename VI, typename VO>
 clsparseStatus dia_build(const uint32_t* rp, const uint32_t* cols, const VI* vals, uint32_t n,
                          const DiaOffsets& offs, int nd_pad, DeviceBuffer& buf, cudaStream_t s, DiaMat<VO>& out);
+
+// Row-sum-compensated rounding of a DIA copy of A (its values rounded to V):
+// diag32[i] = a_ii + sum_{j != i} (a_ij - round_V(a_ij)) in FP32, and A's
+// main diagonal in V set to zero with A.diag32 = diag32. The copy keeps A's
+// row sums, so the rounding perturbation E has zero row sums and, for an
+// M-matrix A, |x^T E x| <= u x^T A x (u the unit roundoff of V): the copy
+// stays SPD and spectrally within 1 +- u of A, where plain rounding of every
+// entry can make a nearly singular diffusion operator indefinite.
+// clsparseInvalidValue if A has no main diagonal.
+template <typename V>
+clsparseStatus dia_compensate_diag(const uint32_t* rp, const uint32_t* cols, const double* vals, uint32_t n,
+                                   DiaMat<V>& A, float* diag32, cudaStream_t s);
 
 // invD = 1 / diag(A) (FP32) from a DIA matrix; status |= kStatusZeroDiag on
 // a zero; clsparseInvalidValue without a main diagonal.

@@ -114,6 +114,7 @@ __device__ void store_state(SolverState<T>* dst, const SolverState<T>& S) {
     dst->done = S.done;
     dst->zero_b = S.zero_b;
     atomicOr(&dst->status_bits, S.status_bits);
+    atomicMax(&dst->hist_len, S.hist_len);  // only CTA 0 records the history
 }
 
 // invD[row] = 1 / A[row,row] for this CTA's rows (first matching entry, as
@@ -165,6 +166,7 @@ __device__ void init_test(SolverState<T>& S, double nb, double nr, int l2) {
     S.init_res = static_cast<double>(S.res);
     S.cur_res = S.init_res;
     S.iteration = 0;
+    if (blockIdx.x == 0) record_residual(&S, 0, S.init_res);
     // the stop test sees the iteration count the solver control held before
     // this solve, as the reference's does
     if (solver_finished(S, S.init_res)) {
@@ -182,6 +184,7 @@ __device__ void step_test(SolverState<T>& S, double nr, int l2) {
     S.nIters = S.iteration;
     S.iteration += 1;
     S.cur_res = static_cast<double>(S.res);
+    if (blockIdx.x == 0) record_residual(&S, S.iteration, S.cur_res);
     if (!isfinite(S.cur_res)) S.status_bits |= kStatusNonFinite;
     S.done = solver_finished(S, S.cur_res) ? 1 : 0;
 }

@@ -651,6 +651,11 @@ __global__ void probe_grad(const uint32_t* __restrict__ Lrp, const uint32_t* __r
         }
 }
 
+// g *= scale (the data-parallel mean of summed gradients).
+__global__ void scale_kernel(float* g, uint32_t n, float scale) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) g[i] *= scale;
+}
+
 __global__ void adam_step(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
                           float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1,
                           float c2) {
@@ -1471,6 +1476,29 @@ clsparseStatus clsparseB200SpaiTrainStep(clsparseB200Spai net, const cldenseVect
     adam_step<<<nblk(net->o.total, 256), 256, 0, control->stream>>>(net->prm, net->grad, net->m, net->v,
                                                                     net->o.total, float(lr), b1, b2, 1e-8f, c1,
                                                                     c2);
+    return finish_call(control);
+}
+
+clsparseStatus clsparseB200SpaiGradient(clsparseB200Spai net, cl_float** deviceGrad, size_t* count) {
+    if (net == nullptr || deviceGrad == nullptr) return clsparseInvalidValue;
+    *deviceGrad = net->grad;
+    if (count) *count = static_cast<size_t>(net->o.total);
+    return clsparseSuccess;
+}
+
+clsparseStatus clsparseB200SpaiAdamStep(clsparseB200Spai net, cl_double lr, cl_double gradScale,
+                                        clsparseControl control) {
+    if (net == nullptr) return clsparseInvalidValue;
+    if (control == nullptr) return clsparseInvalidControlObject;
+    if (!(lr >= 0.0) || !std::isfinite(gradScale)) return clsparseInvalidValue;
+    DeviceGuard g(control->device);
+    const uint32_t P = static_cast<uint32_t>(net->o.total);
+    if (gradScale != 1.0) scale_kernel<<<nblk(P, 256), 256, 0, control->stream>>>(net->grad, P, float(gradScale));
+    net->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, float(net->step)), c2 = 1.f - std::pow(b2, float(net->step));
+    adam_step<<<nblk(P, 256), 256, 0, control->stream>>>(net->prm, net->grad, net->m, net->v, P, float(lr), b1, b2,
+                                                         1e-8f, c1, c2);
     return finish_call(control);
 }
 

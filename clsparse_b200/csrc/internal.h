@@ -142,6 +142,13 @@ struct _solverControl {
     cl_uint deviceStatus = 0;
     cl_int normType = 0;  // 0: reference L1 stop test, 1: L2 (clsparseB200SolverSetNormType)
     cl_int stopOnNonFinite = 0;  // internal: inner solves of the refinement end on a non-finite residual
+    // optional device-resident records of the next solves
+    cl_double* history = nullptr;   // residuum per iteration (clsparseB200SolverSetHistory)
+    cl_uint historyCapacity = 0;
+    cl_uint historyLength = 0;      // entries the last solve wrote
+    cl_int snapshotCount = 0;       // residual vectors after given iterations (clsparseB200SolverSetSnapshots)
+    cl_int snapshotIters[8] = {};
+    void* snapshots = nullptr;
     void printSummary(clsparseStatus status) const;
 };
 

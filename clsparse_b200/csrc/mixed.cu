@@ -18,6 +18,7 @@
 // the FP64 iteration count; the continued one stays close to it.
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "device_common.cuh"
 #include "dia.h"
@@ -135,15 +136,24 @@ bool setup_banded(BandedInner<V>& bi, const clsparseCsrMatrix* A, const Factor* 
                                                            cg, dw.GT, s, bi.GT) != clsparseSuccess))
         return false;
     const size_t stride = (static_cast<size_t>(n) + 63) & ~size_t(63);
-    if (dw.vecs.ensure(8 * stride * sizeof(float) + 256) != cudaSuccess) {
+    if (dw.vecs.ensure(9 * stride * sizeof(float) + 256) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
     float* base = static_cast<float*>(dw.vecs.ptr);
     bi.invD = base;
     for (int k = 0; k < 7; ++k) bi.vec[k] = base + (k + 1) * stride;
-    bi.status = reinterpret_cast<int*>(base + 8 * stride);
+    bi.status = reinterpret_cast<int*>(base + 9 * stride);
     cudaMemsetAsync(bi.status, 0, sizeof(int), s);
+    if constexpr (std::is_same_v<V, __nv_bfloat16>) {
+        // BF16 values: the main diagonal in FP32 carrying each row's rounding
+        // (row sums kept), so the inner operator stays SPD and within 1 +- 2^-9
+        // of A in the energy norm; plain rounding can make a nearly singular
+        // diffusion operator indefinite
+        if (dia_compensate_diag<V>(rp, cols, dev_ptr<const double>(A->values, A->off_values), n, bi.A,
+                                   base + 8 * stride, s) != clsparseSuccess)
+            return false;
+    }
     if (jacobi) {
         // a zero diagonal entry: the CSR path runs and reports it
         int zero = 0;

@@ -21,6 +21,8 @@ enum : int {
     kStatusBarrierTimeout = 32,  // a persistent solver's grid barrier wait ran out
 };
 
+constexpr int kMaxSnapshots = 8;
+
 template <typename T>
 struct SolverState {
     // parameters (written by the host before each solve)
@@ -42,7 +44,32 @@ struct SolverState {
     int zero_b;    // ||b||_1 == 0: x = b and stop (conjugate-gradients.hpp:87-95)
     int exit_s;    // BiCGStab stopped on ||s|| (biconjugate-gradients-stabilized.hpp:183-195)
     int status_bits;
+    // optional records (clsparseB200SolverSetHistory / SetSnapshots)
+    double* hist;      // residuum of the start and of every iteration, FP64
+    int hist_cap;
+    int hist_len;      // entries written by this solve
+    int snap_count;    // residual vectors r kept after snap_iter[k] iterations (CG)
+    int snap_iter[kMaxSnapshots];
+    T* snap;           // snap_count vectors of n values
 };
+
+// Stores the residuum the stop test sees after `iterations` loop iterations
+// (0: the start) into the history, when one is attached and has room.
+template <typename T>
+__device__ __forceinline__ void record_residual(SolverState<T>* st, int iterations, double res) {
+    if (st->hist != nullptr && iterations >= 0 && iterations < st->hist_cap) {
+        st->hist[iterations] = res;
+        st->hist_len = iterations + 1;
+    }
+}
+
+// Slot of the residual snapshot taken after `iterations` iterations, or -1.
+template <typename T>
+__device__ __forceinline__ int snapshot_slot(const SolverState<T>* st, int iterations) {
+    for (int k = 0; k < st->snap_count; ++k)
+        if (st->snap_iter[k] == iterations) return k;
+    return -1;
+}
 
 // The reference's stop test (solver-control.hpp:47-64): converged if
 // res <= relTol or res <= absTol * initial residual, or out of iterations.

@@ -144,12 +144,14 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) cg_init_kernel(CgArgs<T> a) {
     double acc[3] = {0.0, 0.0, 0.0};
     const int l2 = a.st->norm_type;
+    const int slot = a.st->snap != nullptr ? snapshot_slot(a.st, 0) : -1;
     const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
     for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
         const T bi = a.b[i];
         const T ri = a.warm ? bi : bi - a.y[i];
         const T zi = apply_m(a.invD, i, ri);
         a.r[i] = ri;
+        if (slot >= 0) a.st->snap[static_cast<size_t>(slot) * a.n + i] = ri;
         if (!a.warm) a.p[i] = zi;
         acc[0] += norm_term(bi, l2);
         acc[1] += norm_term(ri, l2);
@@ -173,6 +175,7 @@ __global__ void __launch_bounds__(kThreads) cg_init_kernel(CgArgs<T> a) {
         st->rz = static_cast<T>(tot[2]);
         if (a.warm) st->beta = st->rz / st->rz_old;
         st->iteration = 0;
+        record_residual(st, 0, st->init_res);
         // The stop test sees the iteration count the solver control held
         // before this solve, as the reference's does.
         if (solver_finished(*st, st->init_res)) {
@@ -192,6 +195,8 @@ __global__ void __launch_bounds__(kThreads) cg_update_kernel(CgArgs<T> a) {
     if (a.st->done) return;
     const T alpha = a.st->alpha;
     const int l2 = a.st->norm_type;
+    // iterations done after this update (read before the last CTA counts it)
+    const int slot = a.st->snap != nullptr ? snapshot_slot(a.st, a.st->iteration + 1) : -1;
     double acc[2] = {0.0, 0.0};
     const size_t stride = static_cast<size_t>(gridDim.x) * kThreads;
     for (size_t i = static_cast<size_t>(blockIdx.x) * kThreads + threadIdx.x; i < a.n; i += stride) {
@@ -200,6 +205,7 @@ __global__ void __launch_bounds__(kThreads) cg_update_kernel(CgArgs<T> a) {
         const T zi = apply_m(a.invD, i, ri);
         a.x[i] = xi;
         a.r[i] = ri;
+        if (slot >= 0) a.st->snap[static_cast<size_t>(slot) * a.n + i] = ri;
         acc[0] += static_cast<double>(ri) * static_cast<double>(zi);
         acc[1] += norm_term(ri, l2);
     }
@@ -214,6 +220,7 @@ __global__ void __launch_bounds__(kThreads) cg_update_kernel(CgArgs<T> a) {
         st->nIters = st->iteration;
         st->iteration += 1;
         st->cur_res = static_cast<double>(st->res);
+        record_residual(st, st->iteration, st->cur_res);
         if (!isfinite(st->cur_res)) st->status_bits |= kStatusNonFinite;
         const bool fin = solver_finished(*st, st->cur_res);
         st->done = fin ? 1 : 0;
@@ -297,6 +304,7 @@ __global__ void __launch_bounds__(kThreads) bicg_init_kernel(BicgArgs<T> a) {
         st->res = st->norm_r / st->norm_b;
         st->init_res = static_cast<double>(st->res);
         st->cur_res = st->init_res;
+        record_residual(st, 0, st->init_res);
         st->rsr_old = static_cast<T>(tot[2]);
         st->iteration = 0;
         if (solver_finished(*st, st->init_res)) {
@@ -333,6 +341,7 @@ __global__ void __launch_bounds__(kThreads) bicg_s_kernel(BicgArgs<T> a) {
         st->cur_res = static_cast<double>(st->res);
         if (!isfinite(st->cur_res)) st->status_bits |= kStatusNonFinite;
         if (solver_finished(*st, st->cur_res)) {
+            record_residual(st, st->iteration + 1, st->cur_res);  // the s residual it stopped on
             st->nIters = st->iteration;
             st->exit_s = 1;
             st->done = 2;
@@ -375,6 +384,7 @@ __global__ void __launch_bounds__(kThreads) bicg_x_kernel(BicgArgs<T> a) {
         st->norm_r = static_cast<T>(norm_finish(tot[0], l2));
         st->res = st->norm_r / st->norm_b;
         st->cur_res = static_cast<double>(st->res);
+        record_residual(st, st->iteration + 1, st->cur_res);
         if (!isfinite(st->cur_res)) st->status_bits |= kStatusNonFinite;
         if (solver_finished(*st, st->cur_res)) {
             st->nIters = st->iteration;
@@ -462,6 +472,7 @@ __global__ void __launch_bounds__(kThreads) pcg_init_kernel(PcgArgs<T> a) {
         st->init_res = static_cast<double>(st->res);
         st->cur_res = st->init_res;
         st->iteration = 0;
+        record_residual(st, 0, st->init_res);
         if (solver_finished(*st, st->init_res)) {
             st->nIters = 0;
             st->done = 1;
@@ -502,6 +513,7 @@ __global__ void __launch_bounds__(kThreads) pcg_update_kernel(PcgArgs<T> a) {
         st->nIters = st->iteration;
         st->iteration += 1;
         st->cur_res = static_cast<double>(st->res);
+        record_residual(st, st->iteration, st->cur_res);
         if (!isfinite(st->cur_res)) st->status_bits |= kStatusNonFinite;
         const bool fin = solver_finished(*st, st->cur_res);
         st->done = fin ? 1 : 0;
@@ -653,6 +665,11 @@ void init_state(SolverState<T>& h, clSParseSolverControl sc) {
     h.nIters = sc->nIters;
     h.one = T(1);
     h.zero = T(0);
+    h.hist = sc->history;
+    h.hist_cap = sc->history ? static_cast<int>(sc->historyCapacity) : 0;
+    h.snap_count = sc->snapshots ? sc->snapshotCount : 0;
+    for (int k = 0; k < h.snap_count; ++k) h.snap_iter[k] = sc->snapshotIters[k];
+    h.snap = static_cast<T*>(sc->snapshots);
 }
 
 // Copies the device state back into the solver control the way the
@@ -664,6 +681,7 @@ clsparseStatus read_back(clsparseControl c, SolverCache& cache, clSParseSolverCo
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return clsparseInvalidKernelExecution;
     if (c->event) cudaEventRecord(c->event, c->stream);
     sc->deviceStatus = static_cast<cl_uint>(h->status_bits);
+    sc->historyLength = static_cast<cl_uint>(h->hist_len);
     if (h->status_bits & kStatusBarrierTimeout) return clsparseInvalidKernelExecution;
     if (h->zero_b) {
         // conjugate-gradients.hpp:87-95 resets the tolerances of the control
@@ -887,7 +905,8 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
         sc->nIters = 0;
         return clsparseSuccess;
     }
-    if (fused_ok(c, Av.meta) && !warm) {
+    // residual snapshots are taken by the graph engine's update kernel
+    if (fused_ok(c, Av.meta) && !warm && sc->snapshotCount == 0) {
         FusedCgArgs<V, T, T> fa{};
         fa.x = a.x;
         fa.b = a.b;

@@ -298,6 +298,22 @@ class TorchComm:
         (rk,) = ranks
         dist.all_reduce(rk.sums[:k], group=self.group)
 
+    def world(self, items):
+        return dist.get_world_size(self.group)
+
+    def ranks(self, items):
+        return [dist.get_rank(self.group)]
+
+    def allreduce_tensors(self, tensors):
+        (t,) = tensors
+        dist.all_reduce(t, group=self.group)
+
+    def allreduce_host(self, t: torch.Tensor) -> torch.Tensor:
+        dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(self.group) == "nccl" else None
+        u = t.to(dev) if dev is not None else t.clone()
+        dist.all_reduce(u, group=self.group)
+        return u.cpu()
+
 
 class LocalComm:
     """Several ranks in one process: the exchange copies every rank's needed
@@ -322,11 +338,25 @@ class LocalComm:
     def allreduce(self, ranks, k: int):
         if len(ranks) == 1:
             return
-        tot = ranks[0].sums[:k].clone()
-        for rk in ranks[1:]:
-            tot += rk.sums[:k]
-        for rk in ranks:
-            rk.sums[:k] = tot
+        self.allreduce_tensors([rk.sums[:k] for rk in ranks])
+
+    def world(self, items):
+        return len(items)
+
+    def ranks(self, items):
+        return list(range(len(items)))
+
+    def allreduce_tensors(self, tensors):
+        if len(tensors) == 1:
+            return
+        tot = tensors[0].clone()
+        for t in tensors[1:]:
+            tot += t
+        for t in tensors:
+            t.copy_(tot)
+
+    def allreduce_host(self, t: torch.Tensor) -> torch.Tensor:
+        return t
 
 
 # ---------------------------------------------------------------- the solve
@@ -381,6 +411,52 @@ def plan_for_rank(lcol_global, parts, rank: int, group=None, mode: str | None = 
     gathered = [None] * world
     dist.all_gather_object(gathered, mine, group=group)
     return make_plans(gathered, parts, mode)[rank]
+
+
+# ---------------------------------------------------------------- training
+
+class DeviceNet:
+    """One rank's network for data-parallel training (api.Spai on its GPU)."""
+
+    def __init__(self, spai, ctrl):
+        self.spai, self.ctrl = spai, ctrl
+
+    def loss_grad(self, sample):
+        """Loss of `sample` (an object with A and probes); the gradient stays
+        in grad()."""
+        self.spai.set_matrix(sample.A, self.ctrl)
+        return self.spai.loss_grad_device(self.ctrl, sample.probes, self.lam)
+
+    def grad(self) -> torch.Tensor:
+        return self.spai.grad_buffer()
+
+    def adam_step(self, lr, scale):
+        self.spai.adam_step(self.ctrl, lr, scale)
+
+
+def dp_train(nets, comm, samples, steps: int, lr: float, lam: float = 0.2):
+    """Data-parallel training: at step t rank r takes sample (t * world + r)
+    mod len(samples), every rank's gradient is summed over the ranks (one
+    all-reduce of the FP32 gradient, in place on the device) and each rank
+    applies the same Adam step to the mean, so the replicas stay identical.
+    nets: this process's rank(s) (one per process with TorchComm; all with
+    LocalComm). Returns the mean loss per step."""
+    world = comm.world(nets)
+    ranks = comm.ranks(nets)
+    losses = []
+    for net in nets:
+        net.lam = lam
+    for t in range(steps):
+        ls = torch.zeros(1, dtype=torch.float64)
+        for net, r in zip(nets, ranks):
+            ls += net.loss_grad(samples[(t * world + r) % len(samples)])
+        comm.allreduce_tensors([net.grad() for net in nets])
+        ls = comm.allreduce_host(ls)
+        lr_t = lr * (0.1 ** (t / max(steps, 1)))
+        for net in nets:
+            net.adam_step(lr_t, 1.0 / world)
+        losses.append(float(ls) / world)
+    return losses
 
 
 def dist_batched(solve_share, weights, group=None):

@@ -186,6 +186,14 @@ CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiLossGrad(clsparseB200Spai spai, c
 CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiTrainStep(clsparseB200Spai spai, const cldenseVector* probes,
                                                          cl_int K, cl_double lambda, cl_double lr,
                                                          cl_double* loss, clsparseControl control);
+/* The network's device gradient buffer (FP32, *count values), which
+ * clsparseB200SpaiLossGrad fills: data-parallel training sums it over ranks
+ * in place (e.g. one NCCL all-reduce) before clsparseB200SpaiAdamStep. */
+CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiGradient(clsparseB200Spai spai, cl_float** deviceGrad, size_t* count);
+/* One Adam step (learning rate lr) on gradScale times the gradient buffer
+ * (1 / ranks after an all-reduce of summed gradients). */
+CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiAdamStep(clsparseB200Spai spai, cl_double lr, cl_double gradScale,
+                                                        clsparseControl control);
 /* Runs the network on the current matrix and exports G and G^T for the solver. */
 CLSPARSE_EXPORT clsparseStatus clsparseB200SpaiBuild(clsparseB200Spai spai, clsparseControl control);
 /* Copies the exported G (FP64) and its pattern (row pointers n+1, columns). */
@@ -236,6 +244,26 @@ cldenseDdotNoAlloc(clsparseScalar* r, const cldenseVector* x, const cldenseVecto
  * iterates equal up to reduction order). */
 CLSPARSE_EXPORT clsparseStatus
 clsparseB200SetSolverLoopMode(clsparseControl control, cl_int mode);
+
+/* Device-resident residual history of the next CG / BiCGStab solves with this
+ * solver control (the reference prints these residuals in VERBOSE mode,
+ * src/library/solvers/solver-control.hpp:66-106): history[0] = the initial
+ * residuum, history[k] = the residuum the stop test saw after k iterations
+ * (BiCGStab: ||r||, or ||s|| at the iteration that stopped on it), FP64,
+ * written on the device without host reads, up to capacity entries.
+ * NULL (capacity 0) turns it off. */
+CLSPARSE_EXPORT clsparseStatus
+clsparseB200SolverSetHistory(clSParseSolverControl solverControl, cl_double* deviceHistory, cl_uint capacity);
+/* Entries the last solve wrote into the history. */
+CLSPARSE_EXPORT clsparseStatus
+clsparseB200SolverGetHistoryLength(clSParseSolverControl solverControl, cl_uint* length);
+/* Snapshots of the CG residual vector r (the solve's value type, n values
+ * each, back to back in deviceVectors) after each of the listed iteration
+ * counts (0 = r0 = b - A x0), at most 8; count 0 turns them off. The solves
+ * then run on the graph engine (loop modes 0 and 1). */
+CLSPARSE_EXPORT clsparseStatus
+clsparseB200SolverSetSnapshots(clSParseSolverControl solverControl, const cl_int* iterations, cl_int count,
+                               void* deviceVectors);
 
 /* ---- Row-partitioned FP64 CG, one rank's device work (multi-GPU) ----
  * No counterpart in the reference (one queue per control,

@@ -121,3 +121,42 @@ class HostRank:
         if st["done"]:
             sc.nIters, sc.init, sc.cur = st["iters"], st["init"], st["cur"]
         return st["done"], sc.info()
+
+
+class HostNet:
+    """CPU stand-in for a rank's network in data-parallel training: FP32
+    parameters, a least-squares loss per sample 0.5 ||M_s p - c_s||^2 with
+    its gradient in a CPU tensor (what gloo reduces), and the Adam step of
+    the device kernel (beta 0.9 / 0.999, eps 1e-8, bias-corrected)."""
+
+    def __init__(self, nparams: int, seed: int = 1):
+        self.p = np.random.default_rng(seed).normal(0, 0.1, nparams).astype(np.float32)
+        self.m = np.zeros_like(self.p)
+        self.v = np.zeros_like(self.p)
+        self.step = 0
+        self.g = torch.zeros(nparams, dtype=torch.float32)
+
+    def loss_grad(self, sample):
+        M, c = sample
+        res = M @ self.p - c
+        self.g.copy_(torch.from_numpy((M.T @ res).astype(np.float32)))
+        return float(0.5 * res @ res)
+
+    def grad(self):
+        return self.g
+
+    def adam_step(self, lr, scale):
+        g = self.g.numpy() * np.float32(scale)
+        self.step += 1
+        b1, b2 = np.float32(0.9), np.float32(0.999)
+        c1 = np.float32(1.0) - b1 ** self.step
+        c2 = np.float32(1.0) - b2 ** self.step
+        self.m = b1 * self.m + (1 - b1) * g
+        self.v = b2 * self.v + (1 - b2) * g * g
+        self.p = self.p - np.float32(lr) * (self.m / c1) / (np.sqrt(self.v / c2) + np.float32(1e-8))
+
+
+def toy_samples(k: int = 6, nparams: int = 40, seed: int = 3):
+    rng = np.random.default_rng(seed)
+    return [(rng.normal(0, 1, (60, nparams)).astype(np.float32), rng.normal(0, 1, 60).astype(np.float32))
+            for _ in range(k)]

@@ -95,7 +95,10 @@ def _rank_main(rank, world, port, q):
             return [[10.0 * i, float(rank)] for i in idx]
 
         gathered = D.dist_batched(solve_share, [7, 1, 5, 5, 2, 9, 3])
-        q.put((rank, out, gathered))
+        from dist_host_rank import HostNet, toy_samples
+        net = HostNet(40)
+        losses = D.dp_train([net], D.TorchComm(), toy_samples(), steps=30, lr=0.05)
+        q.put((rank, out, gathered, (losses, net.p)))
     finally:
         dist.destroy_process_group()
         _finish(q)
@@ -175,7 +178,7 @@ def test_distributed_cg_matches_single_rank(two_ranks, orc, name):
     info2, xs2 = _host_cg(rp, col, val, b, pre, mi, rel, parts2, [0, 1], plans2, D.LocalComm())
     x2 = np.concatenate(xs2)
     want_mode = {"irregular": D.ALLGATHER}.get(name, D.HALO)
-    for rank, out, _ in two_ranks:
+    for rank, out, *_ in two_ranks:
         info, x, mode = out[name]
         assert mode == want_mode
         r0, r1 = parts2[rank]
@@ -241,3 +244,18 @@ def test_dead_rank_ends_collective_with_error():
     out, _ = _spawn(_dying_rank, 2)
     d = dict(out)
     assert d[1] == "left" and d[0] != "no error"
+
+
+def test_data_parallel_training_keeps_replicas_identical(two_ranks):
+    """Two gloo ranks training the CPU stand-in network on different samples
+    with a gradient all-reduce per step: both replicas end bit for bit equal,
+    equal to the same two ranks run in one process (LocalComm), and the loss
+    falls."""
+    from dist_host_rank import HostNet, toy_samples
+    nets = [HostNet(40), HostNet(40)]
+    losses = D.dp_train(nets, D.LocalComm(), toy_samples(), steps=30, lr=0.05)
+    np.testing.assert_array_equal(nets[0].p, nets[1].p)
+    for _, _, _, (l_r, p_r) in two_ranks:
+        np.testing.assert_array_equal(p_r, nets[0].p)
+        assert l_r == losses
+    assert losses[-1] < 0.75 * losses[0]  # a least-squares floor remains

@@ -36,11 +36,9 @@ def test_mixed_refinement_reaches_fp64_residual(ctrl, orc, inner, sigma):
     sc.release()
     xs = x.cpu().numpy()
     res = true_residual(rp, col, val, xs, b)
-    if inner == "bf16" and sigma == 1.5 and not info["converged"]:
-        # BF16 rounding of a high-contrast operator can stop the refinement
-        # from contracting; the solver must say so instead of claiming success.
-        assert res > 1e-10
-        return
+    # BF16 included: the banded inner copy keeps A's row sums (its FP32
+    # diagonal carries each row's rounding), so even the sigma = 1.5
+    # high-contrast operator stays SPD and the refinement contracts.
     assert info["converged"] == 1, info
     assert res <= 1.5e-10, (res, info)
     assert abs(info["trueResidual"] - res) <= 1e-11 + 1e-3 * res

@@ -23,7 +23,7 @@ RUNS = G.runs()
 TORCH = {"d": torch.float64, "s": torch.float32}
 
 
-def lib_solve(ctrl, run, loop_mode):
+def lib_solve(ctrl, run, loop_mode, history=False):
     name, setting, method, t, pre, path = run
     rp, col, val, x0, b, rel, abs_, max_it = G.inputs(run)
     dt = TORCH[t]
@@ -34,7 +34,13 @@ def lib_solve(ctrl, run, loop_mode):
     x = torch.tensor(x0, dtype=dt, device="cuda")
     bt = torch.tensor(b, dtype=dt, device="cuda")
     sc = api.SolverControl(G.PRECONDS[pre], max_it, rel, abs_)
+    hist = None
+    if history:
+        hist = torch.full((max_it + 8,), -1.0, dtype=torch.float64, device="cuda")
+        sc.set_history(hist)
     info = api.solve(method, x, A, bt, sc, ctrl)
+    if history:
+        info["history"] = hist[: sc.history_length()].cpu().numpy()
     sc.release()
     return x.cpu().numpy().astype(np.float64), info, (rel, abs_, max_it)
 
@@ -51,3 +57,31 @@ def test_library_solver_matches_reference_run(ctrl, run, loop_mode):
     assert c <= rel or c <= abs_ * init or info["nIters"] >= max_it
     dx = np.max(np.abs(x - xr.astype(np.float64))) / np.max(np.abs(xr))
     assert dx <= G.X_TOL[t], dx
+
+
+@pytest.mark.parametrize("loop_mode", [0, 2], ids=["graph", "persistent"])
+@pytest.mark.parametrize("run", RUNS, ids=[G.run_id(r) for r in RUNS])
+def test_residual_history_matches_reference_run(ctrl, run, loop_mode):
+    """The device-resident residual history (clsparseB200SolverSetHistory)
+    against the reference run's residual sequence (what its VERBOSE mode
+    prints, src/library/solvers/solver-control.hpp:66-106)."""
+    name, setting, method, t, pre, path = run
+    xr, it, init, cur, hist = G.reference(D, run)
+    _, info, _ = lib_solve(ctrl, run, loop_mode, history=True)
+    h = info["history"]
+    # the record is the solve's own: first and last entries bit for bit
+    assert h[0] == info["initialResidual"] and h[-1] == info["currentResidual"]
+    if method == "cg":
+        assert len(h) == info["nIters"] + 2 or (info["nIters"] == 0 and len(h) in (1, 2))
+    # The same sequence as the reference's, to the accumulated rounding
+    # difference of the two summation orders, compared while the residual is
+    # above the level where that difference takes over (BiCGStab's and FP32's
+    # sooner than FP64 CG's).
+    cut = {("cg", "d"): 1e-7, ("bicgstab", "d"): 1e-4}.get((method, t), 1e-2) * hist[0]
+    m = min(len(h), len(hist))
+    m = int(np.argmax(hist[:m] < cut)) if np.any(hist[:m] < cut) else m
+    tol = {("cg", "d"): 1e-6, ("bicgstab", "d"): 1e-4}.get((method, t), 2e-2)
+    bad = np.nonzero(np.abs(h[:m] - hist[:m]) > tol * hist[:m])[0]
+    assert len(bad) == 0, (bad[:5], h[bad[:5]], hist[bad[:5]])
+    if info["nIters"] == it:
+        assert len(h) == len(hist)

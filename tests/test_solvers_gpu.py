@@ -214,3 +214,44 @@ def test_solver_argument_errors(ctrl):
         api.solve("cg", x, A, b, sc, ctrl)
     assert e.value.status == L.clsparseInvalidSystemSize
     sc.release()
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+def test_residual_snapshots_are_the_residuals_of_capped_solves(ctrl, dtype):
+    """clsparseB200SolverSetSnapshots keeps r after k iterations; a solve
+    capped after k iterations (maxIters = k - 1: the reference's loop stops
+    when nIters >= maxIters after an update) leaves x_k with b - A x_k = r_k
+    up to the recursion's rounding."""
+    import scipy.sparse as sp
+    rp, col, val = matgen.diffusion3d_lognormal(16, sigma=1.0, seed=2)
+    n = len(rp) - 1
+    b = np.random.default_rng(9).uniform(-1, 1, n)
+    t = NP[dtype]
+    A = api.CsrMatrix.from_numpy(rp, col, val, dtype=dtype)
+    A.create_meta(ctrl)
+    bt = torch.tensor(b, dtype=dtype, device="cuda")
+    ks = [0, 1, 5, 20, 37]
+    snaps = torch.zeros(len(ks), n, dtype=dtype, device="cuda")
+    x = torch.zeros(n, dtype=dtype, device="cuda")
+    sc = api.SolverControl(L.DIAGONAL, max(ks) - 1, 0.0, 0.0)
+    sc.set_snapshots(ks, snaps)
+    hist = torch.zeros(64, dtype=torch.float64, device="cuda")
+    sc.set_history(hist)
+    info = api.solve("cg", x, A, bt, sc, ctrl)
+    assert sc.history_length() == max(ks) + 1 and info["nIters"] == max(ks) - 1
+    sc.release()
+    Am = sp.csr_matrix((np.asarray(val, t).astype(np.float64), col.astype(np.int64), rp.astype(np.int64)))
+    bb = np.asarray(b, t).astype(np.float64)
+    nb = np.abs(bb).sum()
+    for j, k in enumerate(ks):
+        xk = torch.zeros(n, dtype=dtype, device="cuda")
+        if k > 0:
+            sck = api.SolverControl(L.DIAGONAL, k - 1, 0.0, 0.0)
+            api.solve("cg", xk, A, bt, sck, ctrl)
+            sck.release()
+        true_r = bb - Am @ xk.cpu().numpy().astype(np.float64)
+        s = snaps[j].cpu().numpy().astype(np.float64)
+        tol = 1e-11 if dtype == torch.float64 else 2e-4
+        assert np.abs(s - true_r).sum() <= tol * nb, (k, np.abs(s - true_r).sum() / nb)
+        # the history's L1 residuum is this vector's norm
+        assert hist[k].item() == pytest.approx(np.abs(s).sum() / nb, rel=1e-6 if dtype == torch.float64 else 1e-3)

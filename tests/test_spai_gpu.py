@@ -279,3 +279,27 @@ def test_device_graph_build_rejects_unsuitable_matrices(ctrl):
             spai.set_matrix(A, ctrl)
         assert e.value.status == L.clsparseInvalidValue
         spai.release()
+
+
+def test_data_parallel_training_on_device(ctrl):
+    """clsparse_b200.distributed.dp_train with two network replicas on one GPU
+    (LocalComm sums the device gradient buffers in rank order): the replicas
+    stay bit for bit equal. One rank reproduces clsparseB200SpaiTrainStep
+    exactly (the same loss, gradient and Adam step), and the residual
+    snapshots that make the probes come from one solve."""
+    from clsparse_b200 import distributed as D
+    samples = [learn.Sample(ctrl, 32, s) for s in range(4)]
+    assert samples[0].probes.shape == (4, 32 * 32)
+    reps = [api.Spai(77), api.Spai(77)]
+    nets = [D.DeviceNet(s, ctrl) for s in reps]
+    losses = D.dp_train(nets, D.LocalComm(), samples, steps=12, lr=3e-3)
+    np.testing.assert_array_equal(reps[0].params(), reps[1].params())
+    assert all(np.isfinite(losses)) and losses[-1] < losses[0]
+    # one rank == the fused train step
+    a, b = api.Spai(5), api.Spai(5)
+    D.dp_train([D.DeviceNet(a, ctrl)], D.LocalComm(), samples, steps=6, lr=2e-3, lam=0.2)
+    for t in range(6):
+        smp = samples[t % len(samples)]
+        b.set_matrix(smp.A, ctrl)
+        b.train_step(ctrl, smp.probes, 0.2, 2e-3 * (0.1 ** (t / 6)))
+    np.testing.assert_array_equal(a.params(), b.params())
