@@ -254,6 +254,65 @@ def learned_profile(iters: int):
     ctrl.release()
 
 
+def dist_cg_section(rank: int, world: int):
+    """Row-partitioned FP64 Jacobi-CG (clsparseB200DistCg*) on the C3 matrix
+    (128^3 log-normal diffusion, 2,097,152 rows) over the ranks of this run:
+    nnz-balanced row blocks, a halo exchange of boundary planes (NCCL
+    send/recv) and one all-reduce of three FP64 sums per iteration, the
+    reference's L1 stop test at 1e-10. Every rank calls it; the time is the
+    max over ranks of the device time of a whole solve (best of two after one
+    warm-up solve). At one rank the same kernels run without collectives."""
+    import torch
+    import torch.distributed as dist
+
+    from clsparse_b200 import api, matgen
+    from clsparse_b200 import distributed as D
+    rp, col, val = matgen.diffusion3d_lognormal(128, sigma=1.5, seed=3)
+    n = len(rp) - 1
+    b = np.random.default_rng(1).uniform(-1, 1, n)
+    parts = D.row_partition(rp, world)
+    r0, r1 = parts[rank]
+    _, lcol, _ = D.local_rows(rp, col, val, r0, r1)
+    if world > 1:
+        plan = D.plan_for_rank(lcol, parts, rank)
+        comm = D.TorchComm()
+    else:
+        plan = D.make_plans([D.needed_columns(lcol, r0, r1)], parts)[0]
+        comm = D.LocalComm()
+    ctrl = api.Control()
+    rk = D.DeviceRank(plan, *D.setup_local(rp, col, val, parts, rank, plan), 1, ctrl)
+    bl = torch.tensor(b[r0:r1], device="cuda")
+    times, info = [], None
+    for _ in range(3):
+        x = torch.zeros(r1 - r0, dtype=torch.float64, device="cuda")
+        sc = api.SolverControl(1, 20000, 1e-10, 0.0)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        info = D.dist_cg([rk], comm, [x], [bl], [sc])
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        sc.release()
+    rk.release()
+    t = torch.tensor([min(times[1:])], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ctrl.release()
+    ms = float(t.item())
+    halo = sum(cnt for _, cnt in plan.recv.values()) if plan.mode == D.HALO else plan.ext_len - plan.chunk
+    return {"workload": "3D 7-point log-normal diffusion 128^3 (n=2,097,152, sigma 1.5), FP64 Jacobi-CG, "
+                        "L1 stop test 1e-10, rows partitioned over the ranks",
+            "ranks": world, "exchange": plan.mode, "iterations": info["nIters"],
+            "relative_residual": info["currentResidual"], "s": round(ms * 1e-3, 5),
+            "us_per_iteration": round(1e3 * ms / max(info["nIters"] + 1, 1), 2),
+            "remote_entries_per_exchange_rank0": int(halo),
+            "collectives_per_iteration": "1 exchange + 1 all-reduce of 3 FP64" if world > 1 else "none (one rank)"}
+
+
 def cg_section(ctrl, with_cpu: bool):
     """Time-to-solution of the solver configurations the headline metric names.
 
@@ -673,6 +732,7 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total_ms, e2e_ms, avg_launch_ms, e2e_serial_ms = t.tolist()
+    dcg = None if args.no_cg else dist_cg_section(rank, world)  # every rank takes part
     if rank != 0:
         ctrl.release()
         return
@@ -705,6 +765,8 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks,
         "gflops": round(2 * nnz * args.steps / (total_ms * 1e-3) / 1e9, 2),
     }
+    if dcg is not None:
+        line["dist_cg"] = dcg
     if world == 1:
         line["fp32"] = spmv_fp32(api, ctrl, stream, rp, col, val, args.steps, peak)
     if world == 1 and not args.no_cpu_baseline:

@@ -221,6 +221,7 @@ clsparseStatus clsparseScsrcgBatched(cldenseVector* x, const clsparseCsrMatrix* 
                                      const clsparseIdx_t* systemOffsets, cl_int numSystems,
                                      const cl_int* lanesPerRow, clSParseSolverControl solverControl,
                                      clsparseB200BatchResult* result, clsparseControl control) {
+    clsp::TraceRange trace_("clsparseScsrcgBatched");
     clsparseStatus st = check_entry(control);
     if (st != clsparseSuccess) return st;
     if (solverControl == nullptr) return clsparseInvalidSolverControlObject;

@@ -11,6 +11,14 @@
 
 namespace clsp {
 
+bool trace_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("CLSPARSE_B200_NVTX");
+        return e != nullptr && e[0] != '\0' && e[0] != '0';
+    }();
+    return on;
+}
+
 std::atomic<int> g_initialized{0};
 
 cudaError_t DeviceBuffer::ensure(size_t need) {

@@ -124,12 +124,14 @@ extern "C" {
 clsparseStatus clsparseScsrmm(const clsparseScalar* alpha, const clsparseCsrMatrix* sparseMatA,
                               const cldenseMatrix* denseMatB, const clsparseScalar* beta, cldenseMatrix* denseMatC,
                               const clsparseControl control) {
+    clsp::TraceRange trace_("clsparseScsrmm");
     return clsp::csrmm_entry<float>(alpha, sparseMatA, denseMatB, beta, denseMatC, control);
 }
 
 clsparseStatus clsparseDcsrmm(const clsparseScalar* alpha, const clsparseCsrMatrix* sparseMatA,
                               const cldenseMatrix* denseMatB, const clsparseScalar* beta, cldenseMatrix* denseMatC,
                               const clsparseControl control) {
+    clsp::TraceRange trace_("clsparseDcsrmm");
     return clsp::csrmm_entry<double>(alpha, sparseMatA, denseMatB, beta, denseMatC, control);
 }
 

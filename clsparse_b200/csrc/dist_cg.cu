@@ -382,6 +382,7 @@ extern "C" {
 
 clsparseStatus clsparseB200DistCgCreate(clsparseB200DistCg* handle, const clsparseCsrMatrix* A, cl_uint extLength,
                                         cl_uint ownOffset, cl_int precond, clsparseControl control) {
+    clsp::TraceRange trace_("clsparseB200DistCgCreate");
     using namespace clsp;
     if (handle == nullptr) return clsparseInvalidValue;
     *handle = nullptr;
@@ -481,6 +482,7 @@ clsparseStatus clsparseB200DistCgBuffers(clsparseB200DistCg h, cl_double** xExt,
 
 clsparseStatus clsparseB200DistCgStart(clsparseB200DistCg h, cldenseVector* x, const cldenseVector* b,
                                        clsparseControl control) {
+    clsp::TraceRange trace_("clsparseB200DistCgStart");
     using namespace clsp;
     if (h == nullptr) return clsparseInvalidValue;
     if (control == nullptr) return clsparseInvalidControlObject;
@@ -497,6 +499,7 @@ clsparseStatus clsparseB200DistCgStart(clsparseB200DistCg h, cldenseVector* x, c
 }
 
 clsparseStatus clsparseB200DistCgResidual(clsparseB200DistCg h, clsparseControl control) {
+    clsp::TraceRange trace_("clsparseB200DistCgResidual");
     if (h == nullptr) return clsparseInvalidValue;
     if (control == nullptr) return clsparseInvalidControlObject;
     if (h->w.x == nullptr) return clsparseInvalidValue;
@@ -505,6 +508,7 @@ clsparseStatus clsparseB200DistCgResidual(clsparseB200DistCg h, clsparseControl 
 }
 
 clsparseStatus clsparseB200DistCgProduct(clsparseB200DistCg h, clsparseControl control) {
+    clsp::TraceRange trace_("clsparseB200DistCgProduct");
     if (h == nullptr) return clsparseInvalidValue;
     if (control == nullptr) return clsparseInvalidControlObject;
     if (h->w.x == nullptr) return clsparseInvalidValue;
@@ -514,6 +518,7 @@ clsparseStatus clsparseB200DistCgProduct(clsparseB200DistCg h, clsparseControl c
 
 clsparseStatus clsparseB200DistCgUpdate(clsparseB200DistCg h, cl_int step, clSParseSolverControl solverControl,
                                         clsparseControl control) {
+    clsp::TraceRange trace_("clsparseB200DistCgUpdate");
     using namespace clsp;
     if (h == nullptr || step < 0) return clsparseInvalidValue;
     if (control == nullptr) return clsparseInvalidControlObject;
@@ -528,6 +533,7 @@ clsparseStatus clsparseB200DistCgUpdate(clsparseB200DistCg h, cl_int step, clSPa
 
 clsparseStatus clsparseB200DistCgState(clsparseB200DistCg h, cl_int* done, clSParseSolverControl solverControl,
                                        clsparseControl control) {
+    clsp::TraceRange trace_("clsparseB200DistCgState");
     using namespace clsp;
     if (h == nullptr) return clsparseInvalidValue;
     if (control == nullptr) return clsparseInvalidControlObject;

@@ -1380,6 +1380,7 @@ clsparseStatus clsparseB200SpaiRelease(clsparseB200Spai net) {
 
 clsparseStatus clsparseB200SpaiSetMatrix(clsparseB200Spai net, const clsparseCsrMatrix* A,
                                          clsparseControl control) {
+    clsp::TraceRange trace_("clsparseB200SpaiSetMatrix");
     clsparseStatus st = check_net(net, control, false);
     if (st != clsparseSuccess) return st;
     if (!A || A->num_rows != A->num_cols || A->num_rows == 0) return clsparseInvalidSystemSize;
@@ -1443,6 +1444,7 @@ clsparseStatus clsparseB200SpaiParams(clsparseB200Spai net, cl_float* host, size
 clsparseStatus clsparseB200SpaiLossGrad(clsparseB200Spai net, const cldenseVector* probes, cl_int K,
                                         cl_double lambda, cl_int fp32Weights, cl_double* loss, cl_float* grad,
                                         size_t capacity, clsparseControl control) {
+    clsp::TraceRange trace_("clsparseB200SpaiLossGrad");
     clsparseStatus st = check_net(net, control, true);
     if (st != clsparseSuccess) return st;
     if (K > 0 && (!probes || probes->num_values < size_t(K) * net->gr.n)) return clsparseInvalidSize;
@@ -1467,6 +1469,7 @@ clsparseStatus clsparseB200SpaiLossGrad(clsparseB200Spai net, const cldenseVecto
 clsparseStatus clsparseB200SpaiTrainStep(clsparseB200Spai net, const cldenseVector* probes, cl_int K,
                                          cl_double lambda, cl_double lr, cl_double* loss,
                                          clsparseControl control) {
+    clsp::TraceRange trace_("clsparseB200SpaiTrainStep");
     clsparseStatus st = clsparseB200SpaiLossGrad(net, probes, K, lambda, 0, loss, nullptr, 0, control);
     if (st != clsparseSuccess) return st;
     DeviceGuard g(control->device);
@@ -1488,6 +1491,7 @@ clsparseStatus clsparseB200SpaiGradient(clsparseB200Spai net, cl_float** deviceG
 
 clsparseStatus clsparseB200SpaiAdamStep(clsparseB200Spai net, cl_double lr, cl_double gradScale,
                                         clsparseControl control) {
+    clsp::TraceRange trace_("clsparseB200SpaiAdamStep");
     if (net == nullptr) return clsparseInvalidValue;
     if (control == nullptr) return clsparseInvalidControlObject;
     if (!(lr >= 0.0) || !std::isfinite(gradScale)) return clsparseInvalidValue;
@@ -1503,6 +1507,7 @@ clsparseStatus clsparseB200SpaiAdamStep(clsparseB200Spai net, cl_double lr, cl_d
 }
 
 clsparseStatus clsparseB200SpaiBuild(clsparseB200Spai net, clsparseControl control) {
+    clsp::TraceRange trace_("clsparseB200SpaiBuild");
     clsparseStatus st = check_net(net, control, true);
     if (st != clsparseSuccess) return st;
     DeviceGuard g(control->device);

@@ -5,6 +5,7 @@
 
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <atomic>
 #include <cstddef>
@@ -153,6 +154,25 @@ struct _solverControl {
 };
 
 namespace clsp {
+
+// Opt-in NVTX ranges around API calls (CLSPARSE_B200_NVTX=1): a profiler's
+// timeline then shows each call under its API name. NVTX 3 is header-only and
+// costs nothing unless a tool is attached; with the switch off not even the
+// push is made.
+bool trace_enabled();
+class TraceRange {
+public:
+    explicit TraceRange(const char* name) : on_(trace_enabled()) {
+        if (on_) nvtxRangePushA(name);
+    }
+    ~TraceRange() {
+        if (on_) nvtxRangePop();
+    }
+    TraceRange(const TraceRange&) = delete;
+    TraceRange& operator=(const TraceRange&) = delete;
+private:
+    bool on_;
+};
 
 // Sets the control's device current for the scope of an API call.
 class DeviceGuard {

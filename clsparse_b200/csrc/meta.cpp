@@ -204,6 +204,7 @@ clsparseMetaSizeResult clsparseCsrMetaSize(clsparseCsrMatrix* csrMatx, clsparseC
 }
 
 clsparseStatus clsparseCsrMetaCreate(clsparseCsrMatrix* csrMatx, clsparseControl control) {
+    clsp::TraceRange trace_("clsparseCsrMetaCreate");
     return clsp::create_meta(csrMatx, control, kBlkSize, kBlockMultiplier, kRowsForVector, clsp::default_cta_threads());
 }
 

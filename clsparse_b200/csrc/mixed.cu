@@ -381,6 +381,7 @@ clsparseStatus clsparseDcsrcgMixed(cldenseVector* x, const clsparseCsrMatrix* A,
                                    clSParseSolverControl solverControl, cl_int innerPrecision,
                                    cl_double innerTolerance, clsparseB200MixedInfo* info,
                                    clsparseControl control) {
+    clsp::TraceRange trace_("clsparseDcsrcgMixed");
     clsparseStatus st = check_entry(control);
     if (st != clsparseSuccess) return st;
     if (solverControl == nullptr) return clsparseInvalidSolverControlObject;
@@ -400,6 +401,7 @@ clsparseStatus clsparseDcsrbicgStabMixed(cldenseVector* x, const clsparseCsrMatr
                                          clSParseSolverControl solverControl, cl_int innerPrecision,
                                          cl_double innerTolerance, clsparseB200MixedInfo* info,
                                          clsparseControl control) {
+    clsp::TraceRange trace_("clsparseDcsrbicgStabMixed");
     clsparseStatus st = check_entry(control);
     if (st != clsparseSuccess) return st;
     if (solverControl == nullptr) return clsparseInvalidSolverControlObject;
@@ -421,6 +423,7 @@ clsparseStatus clsparseDcsrcgLearned(cldenseVector* x, const clsparseCsrMatrix* 
                                      clSParseSolverControl solverControl, clsparseB200Spai spai,
                                      cl_int innerPrecision, cl_double innerTolerance,
                                      clsparseB200MixedInfo* info, cl_int* fellBack, clsparseControl control) {
+    clsp::TraceRange trace_("clsparseDcsrcgLearned");
     clsparseStatus st = check_entry(control);
     if (st != clsparseSuccess) return st;
     if (solverControl == nullptr) return clsparseInvalidSolverControlObject;

@@ -1231,23 +1231,27 @@ extern "C" {
 
 clsparseStatus clsparseScsrcg(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
                               clSParseSolverControl solverControl, clsparseControl control) {
+    clsp::TraceRange trace_("clsparseScsrcg");
     return cg_solve<float, float>(x, A, b, solverControl, control);
 }
 
 clsparseStatus clsparseDcsrcg(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
                               clSParseSolverControl solverControl, clsparseControl control) {
+    clsp::TraceRange trace_("clsparseDcsrcg");
     return cg_solve<double, double>(x, A, b, solverControl, control);
 }
 
 clsparseStatus clsparseScsrbicgStab(cldenseVector* x, const clsparseCsrMatrix* A,
                                     const cldenseVector* b, clSParseSolverControl solverControl,
                                     clsparseControl control) {
+    clsp::TraceRange trace_("clsparseScsrbicgStab");
     return bicg_solve<float, float>(x, A, b, solverControl, control);
 }
 
 clsparseStatus clsparseDcsrbicgStab(cldenseVector* x, const clsparseCsrMatrix* A,
                                     const cldenseVector* b, clSParseSolverControl solverControl,
                                     clsparseControl control) {
+    clsp::TraceRange trace_("clsparseDcsrbicgStab");
     return bicg_solve<double, double>(x, A, b, solverControl, control);
 }
 

@@ -397,12 +397,14 @@ extern "C" {
 clsparseStatus clsparseScsrmv(const clsparseScalar* alpha, const clsparseCsrMatrix* matx,
                               const cldenseVector* x, const clsparseScalar* beta, cldenseVector* y,
                               const clsparseControl control) {
+    clsp::TraceRange trace_("clsparseScsrmv");
     return clsp::csrmv_entry<float>(alpha, matx, x, beta, y, control);
 }
 
 clsparseStatus clsparseDcsrmv(const clsparseScalar* alpha, const clsparseCsrMatrix* matx,
                               const cldenseVector* x, const clsparseScalar* beta, cldenseVector* y,
                               const clsparseControl control) {
+    clsp::TraceRange trace_("clsparseDcsrmv");
     return clsp::csrmv_entry<double>(alpha, matx, x, beta, y, control);
 }
 
