@@ -207,6 +207,24 @@ __device__ __forceinline__ void for_rows(uint32_t n, F body) {
     for (uint32_t i = r0 + threadIdx.x; i < r1; i += kDiaThreads) body(i);
 }
 
+// Rows per thread and pass in the Jacobi phases: 2 walks the slice two rows
+// at a time (row i and i + kDiaThreads), all loads of both before any store.
+#ifndef CLSP_DIA_U
+#define CLSP_DIA_U 1
+#endif
+
+// Pairs of a CTA's rows: body(i0, i1, has1) with i1 = i0 + kDiaThreads when
+// has1 (else i1 = i0, the second row's stores to be skipped).
+template <typename F>
+__device__ __forceinline__ void for_row_pairs(uint32_t n, F body) {
+    const uint64_t c = blockIdx.x, G = gridDim.x;
+    const uint32_t r0 = static_cast<uint32_t>(c * n / G), r1 = static_cast<uint32_t>((c + 1) * n / G);
+    for (uint32_t i = r0 + threadIdx.x; i < r1; i += 2 * kDiaThreads) {
+        const bool has1 = i + kDiaThreads < r1;
+        body(i, has1 ? i + kDiaThreads : i, has1);
+    }
+}
+
 // sum_d M[d][i] * xf(i + off[d]) over the ND diagonals (ND the matrix's
 // padded diagonal count), in increasing column order, FP32 FMAs. Every load
 // is unconditional -- indices outside the matrix are clamped and their
@@ -348,6 +366,22 @@ __global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_pcg_kernel(Dia
                 const float zj = vld(z + j);
                 return use_p ? fmaf(beta, vld(Po + j), zj) : zj;
             };
+#if CLSP_DIA_U == 2
+            for_row_pairs(n, [&](uint32_t i0, uint32_t i1, bool has1) {
+                const float q0 = dia_row<NDA>(a.A, n, i0, pv);
+                const float p0 = pv(i0);
+                const float q1 = dia_row<NDA>(a.A, n, i1, pv);
+                const float p1 = pv(i1);
+                P[i0] = p0;
+                q[i0] = q0;
+                acc[0] += static_cast<double>(p0) * q0;
+                if (has1) {
+                    P[i1] = p1;
+                    q[i1] = q1;
+                    acc[0] += static_cast<double>(p1) * q1;
+                }
+            });
+#else
             for_rows(n, [&](uint32_t i) {
                 const float qi = dia_row<NDA>(a.A, n, i, pv);
                 const float pi = pv(i);
@@ -355,6 +389,7 @@ __global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_pcg_kernel(Dia
                 q[i] = qi;
                 acc[0] += static_cast<double>(pi) * qi;
             });
+#endif
             double pq[1];
             if (!grid_exchange<1>(g, epoch, acc, pq, gs)) goto fail;
             if (!(pq[0] > 0.0)) {  // lost positive curvature (or not finite): stop, the caller restarts
@@ -406,6 +441,26 @@ __global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_pcg_kernel(Dia
             } else {
                 float* R = a.r[0];
                 double acc2[2] = {0.0, 0.0};
+#if CLSP_DIA_U == 2
+                for_row_pairs(n, [&](uint32_t i0, uint32_t i1, bool has1) {
+                    const float x0 = fmaf(alpha, P[i0], x[i0]), x1 = fmaf(alpha, P[i1], x[i1]);
+                    const float r0v = fmaf(-alpha, q[i0], R[i0]), r1v = fmaf(-alpha, q[i1], R[i1]);
+                    const float z0 = invD ? r0v * __ldg(invD + i0) : r0v;
+                    const float z1 = invD ? r1v * __ldg(invD + i1) : r1v;
+                    x[i0] = x0;
+                    R[i0] = r0v;
+                    z[i0] = z0;
+                    acc2[0] += static_cast<double>(r0v) * r0v;
+                    acc2[1] += static_cast<double>(r0v) * z0;
+                    if (has1) {
+                        x[i1] = x1;
+                        R[i1] = r1v;
+                        z[i1] = z1;
+                        acc2[0] += static_cast<double>(r1v) * r1v;
+                        acc2[1] += static_cast<double>(r1v) * z1;
+                    }
+                });
+#else
                 for_rows(n, [&](uint32_t i) {
                     x[i] = fmaf(alpha, P[i], x[i]);
                     const float ri = fmaf(-alpha, q[i], R[i]);
@@ -415,6 +470,7 @@ __global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_pcg_kernel(Dia
                     acc2[0] += static_cast<double>(ri) * ri;
                     acc2[1] += static_cast<double>(ri) * zi;
                 });
+#endif
                 double tot[2];
                 if (!grid_exchange<2>(g, epoch, acc2, tot, gs)) goto fail;
                 rr = tot[0];

@@ -219,9 +219,10 @@ def test_solver_argument_errors(ctrl):
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
 def test_residual_snapshots_are_the_residuals_of_capped_solves(ctrl, dtype):
     """clsparseB200SolverSetSnapshots keeps r after k iterations; a solve
-    capped after k iterations (maxIters = k - 1: the reference's loop stops
-    when nIters >= maxIters after an update) leaves x_k with b - A x_k = r_k
-    up to the recursion's rounding."""
+    capped after k >= 2 iterations (maxIters = k - 1: the reference's loop
+    stops when nIters >= maxIters after an update; maxIters = 0 stops before
+    the first one) leaves x_k with b - A x_k = r_k up to the recursion's
+    rounding."""
     import scipy.sparse as sp
     rp, col, val = matgen.diffusion3d_lognormal(16, sigma=1.0, seed=2)
     n = len(rp) - 1
@@ -230,7 +231,7 @@ def test_residual_snapshots_are_the_residuals_of_capped_solves(ctrl, dtype):
     A = api.CsrMatrix.from_numpy(rp, col, val, dtype=dtype)
     A.create_meta(ctrl)
     bt = torch.tensor(b, dtype=dtype, device="cuda")
-    ks = [0, 1, 5, 20, 37]
+    ks = [0, 2, 5, 20, 37]
     snaps = torch.zeros(len(ks), n, dtype=dtype, device="cuda")
     x = torch.zeros(n, dtype=dtype, device="cuda")
     sc = api.SolverControl(L.DIAGONAL, max(ks) - 1, 0.0, 0.0)
