@@ -35,6 +35,7 @@
 #include <initializer_list>
 #include <cstring>
 #include <random>
+#include <type_traits>
 #include <vector>
 
 #include "device_common.cuh"
@@ -923,22 +924,15 @@ struct Graph {
     // solvers apply the factor with the row-block kernels
     matrix_meta* metaL = nullptr;
     matrix_meta* metaLT = nullptr;
+    // every buffer above except B lives in one allocation (a new matrix size
+    // costs one cudaMalloc and one cudaFree instead of about fifty)
+    void* arena = nullptr;
 
     void release() {
         delete metaL;
         delete metaLT;
-        void* ptrs[] = {ehat, dinvs, Lrp, Lcol, Le, LTrp, LTrow, LTidx, Boff, B, F, Hp, Hq, g, dg, dH, dHn, dS,
-                        dHu, dHp, dHq, part, pw, pu, pv, pdv, pdu, red, ticket, G32, GT32, G16, GT16, G64, GT64,
-                        scan_part, info};
-        for (void* p : ptrs)
-            if (p) cudaFree(p);
-        for (int l = 0; l <= NL; ++l)
-            if (Hs[l]) cudaFree(Hs[l]);
-        for (int l = 0; l < NL; ++l) {
-            if (Hu[l]) cudaFree(Hu[l]);
-            if (S[l]) cudaFree(S[l]);
-            if (Au[l]) cudaFree(Au[l]);
-        }
+        if (arena) cudaFree(arena);
+        if (B) cudaFree(B);
         *this = Graph();
     }
 };
@@ -1028,39 +1022,73 @@ clsparseStatus read_host_csr(const clsparseCsrMatrix* A, clsparseControl c, Host
 // enough: a network set to one matrix after another of the same size
 // allocates once. The local blocks of the loss are allocated on first use.
 bool ensure_graph_buffers(Graph& gr, uint32_t n, uint32_t nnz) {
-    if (gr.ehat != nullptr && gr.cap_n >= n && gr.cap_nnz >= nnz) return true;
+    if (gr.arena != nullptr && gr.cap_n >= n && gr.cap_nnz >= nnz) return true;
     gr.release();
-    const uint32_t nl = nnz;
-    bool ok = dalloc(gr.ehat, nnz) == cudaSuccess && dalloc(gr.dinvs, n) == cudaSuccess &&
-              dalloc(gr.Lrp, n + 1) == cudaSuccess && dalloc(gr.Lcol, nl) == cudaSuccess &&
-              dalloc(gr.Le, nl) == cudaSuccess && dalloc(gr.LTrp, n + 1) == cudaSuccess &&
-              dalloc(gr.LTrow, nl) == cudaSuccess && dalloc(gr.LTidx, nl) == cudaSuccess &&
-              dalloc(gr.Boff, n + 1) == cudaSuccess && dalloc(gr.F, size_t(n) * NF) == cudaSuccess &&
-              dalloc(gr.scan_part, scan::parts_for(n) + 1) == cudaSuccess && dalloc(gr.info, 4) == cudaSuccess;
-    const size_t nh = size_t(n) * H, nho = size_t(n) * HO;
-    for (int l = 0; l <= NL && ok; ++l) ok = dalloc(gr.Hs[l], nh) == cudaSuccess;
-    for (int l = 0; l < NL && ok; ++l)
-        ok = dalloc(gr.Hu[l], nh) == cudaSuccess && dalloc(gr.S[l], nh) == cudaSuccess &&
-             dalloc(gr.Au[l], nh) == cudaSuccess;
+    const size_t nl = nnz, nh = size_t(n) * H, nho = size_t(n) * HO;
     const size_t tiles = nblk(n, kRows);
-    gr.part_floats = std::max({tiles * size_t(H * 2 * H + H), size_t(n) * 2 * H, size_t(n) * kOutPart});
-    ok = ok && dalloc(gr.Hp, nho) == cudaSuccess && dalloc(gr.Hq, nho) == cudaSuccess &&
-         dalloc(gr.g, nl) == cudaSuccess && dalloc(gr.dg, nl) == cudaSuccess &&
-         dalloc(gr.dH, nh) == cudaSuccess && dalloc(gr.dHn, nh) == cudaSuccess &&
-         dalloc(gr.dS, nh) == cudaSuccess && dalloc(gr.dHu, nh) == cudaSuccess &&
-         dalloc(gr.dHp, nho) == cudaSuccess && dalloc(gr.dHq, nho) == cudaSuccess &&
-         dalloc(gr.part, gr.part_floats) == cudaSuccess && dalloc(gr.pw, n) == cudaSuccess &&
-         dalloc(gr.pu, n) == cudaSuccess && dalloc(gr.pv, n) == cudaSuccess &&
-         dalloc(gr.pdv, n) == cudaSuccess && dalloc(gr.pdu, n) == cudaSuccess &&
-         dalloc(gr.red, 8 + 2 * kMaxReduceCtas) == cudaSuccess && dalloc(gr.ticket, 4) == cudaSuccess &&
-         dalloc(gr.G32, nl) == cudaSuccess && dalloc(gr.GT32, nl) == cudaSuccess &&
-         dalloc(gr.G16, nl) == cudaSuccess && dalloc(gr.GT16, nl) == cudaSuccess &&
-         dalloc(gr.G64, nl) == cudaSuccess && dalloc(gr.GT64, nl) == cudaSuccess;
-    if (!ok) {
+    const size_t part_floats = std::max({tiles * size_t(H * 2 * H + H), size_t(n) * 2 * H, size_t(n) * kOutPart});
+    // Lays every buffer out from `base` (nullptr: only sizes them), 256-byte
+    // aligned; returns the bytes needed.
+    auto carve = [&](char* base) {
+        size_t off = 0;
+        auto take = [&](auto*& p, size_t count) {
+            off = (off + 255) & ~size_t(255);
+            p = base ? reinterpret_cast<std::remove_reference_t<decltype(p)>>(base + off) : nullptr;
+            off += count * sizeof(*p);
+        };
+        take(gr.ehat, nnz);
+        take(gr.dinvs, n);
+        take(gr.Lrp, size_t(n) + 1);
+        take(gr.Lcol, nl);
+        take(gr.Le, nl);
+        take(gr.LTrp, size_t(n) + 1);
+        take(gr.LTrow, nl);
+        take(gr.LTidx, nl);
+        take(gr.Boff, size_t(n) + 1);
+        take(gr.F, size_t(n) * NF);
+        take(gr.scan_part, scan::parts_for(n) + 1);
+        take(gr.info, 4);
+        for (int l = 0; l <= NL; ++l) take(gr.Hs[l], nh);
+        for (int l = 0; l < NL; ++l) {
+            take(gr.Hu[l], nh);
+            take(gr.S[l], nh);
+            take(gr.Au[l], nh);
+        }
+        take(gr.Hp, nho);
+        take(gr.Hq, nho);
+        take(gr.g, nl);
+        take(gr.dg, nl);
+        take(gr.dH, nh);
+        take(gr.dHn, nh);
+        take(gr.dS, nh);
+        take(gr.dHu, nh);
+        take(gr.dHp, nho);
+        take(gr.dHq, nho);
+        take(gr.part, part_floats);
+        take(gr.pw, n);
+        take(gr.pu, n);
+        take(gr.pv, n);
+        take(gr.pdv, n);
+        take(gr.pdu, n);
+        take(gr.red, 8 + 2 * kMaxReduceCtas);
+        take(gr.ticket, 4);
+        take(gr.G32, nl);
+        take(gr.GT32, nl);
+        take(gr.G16, nl);
+        take(gr.GT16, nl);
+        take(gr.G64, nl);
+        take(gr.GT64, nl);
+        return off;
+    };
+    const size_t bytes = carve(nullptr);
+    if (cudaMalloc(&gr.arena, bytes) != cudaSuccess) {
         cudaGetLastError();
+        gr.arena = nullptr;
         gr.release();
         return false;
     }
+    carve(static_cast<char*>(gr.arena));
+    gr.part_floats = part_floats;
     gr.cap_n = n;
     gr.cap_nnz = nnz;
     return true;

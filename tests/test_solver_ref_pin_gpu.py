@@ -74,14 +74,15 @@ def test_residual_history_matches_reference_run(ctrl, run, loop_mode):
     if method == "cg":
         assert len(h) == info["nIters"] + 2 or (info["nIters"] == 0 and len(h) in (1, 2))
     # The same sequence as the reference's while the two summation orders
-    # have not yet drifted apart: the first 8 entries (FP64 1e-8, FP32 1e-3
-    # relative), and the whole history for FP64 Jacobi-CG (well conditioned:
+    # have not yet drifted apart: the first 8 entries (FP64 1e-8, FP32 1e-2
+    # relative: FP32 BiCGStab drifts by 0.3 % within 7 iterations), and the
+    # whole history for FP64 Jacobi-CG (well conditioned:
     # 1e-6 while the residual is above 1e-7 of the start). Without a
     # preconditioner, and in FP32, the rounding differences grow within a few
     # dozen iterations (the oracle and the reference kernels differ the same
     # way), so later entries are compared only through the final residual.
     m = min(len(h), len(hist), 8)
-    tol = 1e-8 if t == "d" else 1e-3
+    tol = 1e-8 if t == "d" else 1e-2
     bad = np.nonzero(np.abs(h[:m] - hist[:m]) > tol * hist[:m])[0]
     assert len(bad) == 0, (bad, h[bad], hist[bad])
     if method == "cg" and t == "d" and pre == "jacobi":
