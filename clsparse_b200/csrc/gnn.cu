@@ -627,14 +627,22 @@ __global__ void ahat_spmv(const uint32_t* __restrict__ rp, const uint32_t* __res
 
 // Probe loss pieces. res = v - r scaled: dv = coef * (v - r), and the sum of
 // (v - r)^2 / ||r||^2 goes to `out` through a grid sum.
-__global__ void probe_residual(const float* __restrict__ v, const float* __restrict__ r, float coef,
-                               float inv_rr, float* __restrict__ dv, uint32_t n, double* parts,
+// The probe's weights come from its squared norm rr on the device:
+// coef = 2 lambda / (K rr), inv_rr = lambda / (K rr) (the same double
+// expressions the host evaluated before); a probe with rr not > 0 adds
+// nothing (dv = 0, no loss term).
+__global__ void probe_residual(const float* __restrict__ v, const float* __restrict__ r, const double* rr_p,
+                               double lambda, int K, float* __restrict__ dv, uint32_t n, double* parts,
                                uint32_t* ticket, double* out) {
+    const double rr = *rr_p;
+    const bool on = rr > 0.0;
+    const float coef = on ? static_cast<float>(2.0 * lambda / (K * rr)) : 0.f;
+    const float inv_rr = on ? static_cast<float>(lambda / (K * rr)) : 0.f;
     double acc[1] = {0.0};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float d = v[i] - r[i];
-        dv[i] = coef * d;
-        acc[0] += static_cast<double>(d) * d * inv_rr;
+        dv[i] = on ? coef * d : 0.f;
+        if (on) acc[0] += static_cast<double>(d) * d * inv_rr;
     }
     double tot[1];
     if (dev::grid_reduce_last<1>(acc, parts, ticket, tot) && threadIdx.x == 0) out[0] += tot[0];
@@ -644,7 +652,8 @@ __global__ void probe_residual(const float* __restrict__ v, const float* __restr
 __global__ void probe_grad(const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lcol,
                            const float* __restrict__ dv, const float* __restrict__ u,
                            const float* __restrict__ du, const float* __restrict__ w, float* __restrict__ dg,
-                           uint32_t n) {
+                           uint32_t n, const double* rr_p) {
+    if (!(*rr_p > 0.0)) return;  // a probe without a positive norm contributes nothing
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         for (uint32_t k = Lrp[i]; k < Lrp[i + 1]; ++k) {
             const uint32_t j = Lcol[k];
@@ -1257,8 +1266,9 @@ void forward(_clsparseB200Spai* net, int bf16, cudaStream_t s, bool keep_act = t
                                              gr.n, bf16);
 }
 
-// Loss and dL/dg; returns the loss (host sync).
-double loss_and_dg(_clsparseB200Spai* net, const float* probes, int K, double lambda, cudaStream_t s) {
+// Loss and dL/dg; the loss is read back (a host sync) only when want_loss.
+double loss_and_dg(_clsparseB200Spai* net, const float* probes, int K, double lambda, cudaStream_t s,
+                   bool want_loss) {
     Graph& gr = net->gr;
     const uint32_t n = gr.n;
     double* parts = gr.red + 8;
@@ -1266,30 +1276,27 @@ double loss_and_dg(_clsparseB200Spai* net, const float* probes, int K, double la
     kaporin_sum<<<rg, 256, 0, s>>>(gr.Lrp, gr.Boff, gr.B, gr.g, n, parts, gr.ticket, gr.red);
     kaporin_grad<<<rg, 256, 0, s>>>(gr.Lrp, gr.Boff, gr.B, gr.g, n, gr.red, gr.dg);
     cudaMemsetAsync(gr.red + 2, 0, sizeof(double), s);
-    std::vector<double> rnorm(K, 0.0);
     if (K > 0 && lambda > 0.0) {
-        // squared norms of the probes on the device, K words read back
+        // squared norms of the probes on the device, four at a time; the
+        // probe kernels read them there (nothing comes back to the host)
         double* dnorm = gr.red + 4;  // [4..7]; red[0..3] hold the loss sums
         for (int k0 = 0; k0 < K; k0 += 4) {
             const int kk = std::min(4, K - k0);
             for (int k = 0; k < kk; ++k)
                 probe_norm<<<rg, 256, 0, s>>>(probes + size_t(k0 + k) * n, n, parts, gr.ticket, dnorm + k);
-            cudaMemcpyAsync(rnorm.data() + k0, dnorm, size_t(kk) * sizeof(double), cudaMemcpyDeviceToHost, s);
-            cudaStreamSynchronize(s);
-        }
-        for (int k = 0; k < K; ++k) {
-            if (!(rnorm[k] > 0.0)) continue;
-            const float* r = probes + size_t(k) * n;
-            ahat_spmv<<<warps_grid(n), 256, 0, s>>>(gr.rp, gr.cols, gr.ehat, r, gr.pw, n);
-            lspmv<<<warps_grid(n), 256, 0, s>>>(gr.Lrp, gr.Lcol, nullptr, gr.g, gr.pw, gr.pu, n);
-            lspmv<<<warps_grid(n), 256, 0, s>>>(gr.LTrp, gr.LTrow, gr.LTidx, gr.g, gr.pu, gr.pv, n);
-            const float coef = static_cast<float>(2.0 * lambda / (K * rnorm[k]));
-            probe_residual<<<rg, 256, 0, s>>>(gr.pv, r, coef, static_cast<float>(lambda / (K * rnorm[k])),
-                                              gr.pdv, n, parts, gr.ticket, gr.red + 2);
-            lspmv<<<warps_grid(n), 256, 0, s>>>(gr.Lrp, gr.Lcol, nullptr, gr.g, gr.pdv, gr.pdu, n);
-            probe_grad<<<rg, 256, 0, s>>>(gr.Lrp, gr.Lcol, gr.pdv, gr.pu, gr.pdu, gr.pw, gr.dg, n);
+            for (int k = 0; k < kk; ++k) {
+                const float* r = probes + size_t(k0 + k) * n;
+                ahat_spmv<<<warps_grid(n), 256, 0, s>>>(gr.rp, gr.cols, gr.ehat, r, gr.pw, n);
+                lspmv<<<warps_grid(n), 256, 0, s>>>(gr.Lrp, gr.Lcol, nullptr, gr.g, gr.pw, gr.pu, n);
+                lspmv<<<warps_grid(n), 256, 0, s>>>(gr.LTrp, gr.LTrow, gr.LTidx, gr.g, gr.pu, gr.pv, n);
+                probe_residual<<<rg, 256, 0, s>>>(gr.pv, r, dnorm + k, lambda, K, gr.pdv, n, parts, gr.ticket,
+                                                  gr.red + 2);
+                lspmv<<<warps_grid(n), 256, 0, s>>>(gr.Lrp, gr.Lcol, nullptr, gr.g, gr.pdv, gr.pdu, n);
+                probe_grad<<<rg, 256, 0, s>>>(gr.Lrp, gr.Lcol, gr.pdv, gr.pu, gr.pdu, gr.pw, gr.dg, n, dnorm + k);
+            }
         }
     }
+    if (!want_loss) return 0.0;
     double h[3];
     cudaMemcpyAsync(h, gr.red, 3 * sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
@@ -1482,7 +1489,7 @@ clsparseStatus clsparseB200SpaiLossGrad(clsparseB200Spai net, const cldenseVecto
     const int bf16 = fp32Weights ? 0 : 1;
     forward(net, bf16, control->stream);
     const double L = loss_and_dg(net, K > 0 ? dev_ptr<const float>(probes->values, probes->off_values) : nullptr,
-                                 K, lambda, control->stream);
+                                 K, lambda, control->stream, loss != nullptr);
     backward(net, bf16, control->stream);
     if (loss) *loss = L;
     if (grad) {
