@@ -933,14 +933,20 @@ struct Graph {
     // solvers apply the factor with the row-block kernels
     matrix_meta* metaL = nullptr;
     matrix_meta* metaLT = nullptr;
-    // every buffer above except B lives in one allocation (a new matrix size
-    // costs one cudaMalloc and one cudaFree instead of about fifty)
+    // The buffers above live in two allocations: `arena` holds what the graph
+    // and the factor build need (patterns, features, the factor copies and
+    // four activation buffers the layers share: Hs[l] alternates between two,
+    // every layer's Hu and S are one each); `train_arena`, made on the first
+    // training call for the graph, gives every layer its own activations and
+    // adds Au and the gradient buffers. B (Kaporin blocks) is separate.
     void* arena = nullptr;
+    void* train_arena = nullptr;
 
     void release() {
         delete metaL;
         delete metaLT;
         if (arena) cudaFree(arena);
+        if (train_arena) cudaFree(train_arena);
         if (B) cudaFree(B);
         *this = Graph();
     }
@@ -1030,76 +1036,114 @@ clsparseStatus read_host_csr(const clsparseCsrMatrix* A, clsparseControl c, Host
 // hold at most nnz entries), or keeps the present ones when they are large
 // enough: a network set to one matrix after another of the same size
 // allocates once. The local blocks of the loss are allocated on first use.
+// Lays buffers out from `base` (nullptr: only sizes them), 256-byte aligned.
+struct Carver {
+    char* base;
+    size_t off = 0;
+    template <typename T>
+    void take(T*& p, size_t count) {
+        off = (off + 255) & ~size_t(255);
+        p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+        off += count * sizeof(T);
+    }
+};
+
+// One allocation for the layout `lay` describes: sized by a dry run, then
+// laid out from the new block.
+template <typename F>
+bool allocate_laid_out(void*& block, F lay) {
+    Carver dry{nullptr};
+    lay(dry);
+    if (cudaMalloc(&block, dry.off) != cudaSuccess) {
+        cudaGetLastError();
+        block = nullptr;
+        return false;
+    }
+    Carver c{static_cast<char*>(block)};
+    lay(c);
+    return true;
+}
+
 bool ensure_graph_buffers(Graph& gr, uint32_t n, uint32_t nnz) {
     if (gr.arena != nullptr && gr.cap_n >= n && gr.cap_nnz >= nnz) return true;
     gr.release();
     const size_t nl = nnz, nh = size_t(n) * H, nho = size_t(n) * HO;
-    const size_t tiles = nblk(n, kRows);
-    const size_t part_floats = std::max({tiles * size_t(H * 2 * H + H), size_t(n) * 2 * H, size_t(n) * kOutPart});
-    // Lays every buffer out from `base` (nullptr: only sizes them), 256-byte
-    // aligned; returns the bytes needed.
-    auto carve = [&](char* base) {
-        size_t off = 0;
-        auto take = [&](auto*& p, size_t count) {
-            off = (off + 255) & ~size_t(255);
-            p = base ? reinterpret_cast<std::remove_reference_t<decltype(p)>>(base + off) : nullptr;
-            off += count * sizeof(*p);
-        };
-        take(gr.ehat, nnz);
-        take(gr.dinvs, n);
-        take(gr.Lrp, size_t(n) + 1);
-        take(gr.Lcol, nl);
-        take(gr.Le, nl);
-        take(gr.LTrp, size_t(n) + 1);
-        take(gr.LTrow, nl);
-        take(gr.LTidx, nl);
-        take(gr.Boff, size_t(n) + 1);
-        take(gr.F, size_t(n) * NF);
-        take(gr.scan_part, scan::parts_for(n) + 1);
-        take(gr.info, 4);
-        for (int l = 0; l <= NL; ++l) take(gr.Hs[l], nh);
-        for (int l = 0; l < NL; ++l) {
-            take(gr.Hu[l], nh);
-            take(gr.S[l], nh);
-            take(gr.Au[l], nh);
-        }
-        take(gr.Hp, nho);
-        take(gr.Hq, nho);
-        take(gr.g, nl);
-        take(gr.dg, nl);
-        take(gr.dH, nh);
-        take(gr.dHn, nh);
-        take(gr.dS, nh);
-        take(gr.dHu, nh);
-        take(gr.dHp, nho);
-        take(gr.dHq, nho);
-        take(gr.part, part_floats);
-        take(gr.pw, n);
-        take(gr.pu, n);
-        take(gr.pv, n);
-        take(gr.pdv, n);
-        take(gr.pdu, n);
-        take(gr.red, 8 + 2 * kMaxReduceCtas);
-        take(gr.ticket, 4);
-        take(gr.G32, nl);
-        take(gr.GT32, nl);
-        take(gr.G16, nl);
-        take(gr.GT16, nl);
-        take(gr.G64, nl);
-        take(gr.GT64, nl);
-        return off;
-    };
-    const size_t bytes = carve(nullptr);
-    if (cudaMalloc(&gr.arena, bytes) != cudaSuccess) {
-        cudaGetLastError();
-        gr.arena = nullptr;
+    float *act0 = nullptr, *act1 = nullptr, *hu = nullptr, *sb = nullptr;
+    const bool ok = allocate_laid_out(gr.arena, [&](Carver& c) {
+        c.take(gr.ehat, nnz);
+        c.take(gr.dinvs, n);
+        c.take(gr.Lrp, size_t(n) + 1);
+        c.take(gr.Lcol, nl);
+        c.take(gr.Le, nl);
+        c.take(gr.LTrp, size_t(n) + 1);
+        c.take(gr.LTrow, nl);
+        c.take(gr.LTidx, nl);
+        c.take(gr.Boff, size_t(n) + 1);
+        c.take(gr.F, size_t(n) * NF);
+        c.take(gr.scan_part, scan::parts_for(n) + 1);
+        c.take(gr.info, 4);
+        c.take(act0, nh);
+        c.take(act1, nh);
+        c.take(hu, nh);
+        c.take(sb, nh);
+        c.take(gr.Hp, nho);
+        c.take(gr.Hq, nho);
+        c.take(gr.g, nl);
+        c.take(gr.red, 8 + 2 * kMaxReduceCtas);
+        c.take(gr.ticket, 4);
+        c.take(gr.G32, nl);
+        c.take(gr.GT32, nl);
+        c.take(gr.G16, nl);
+        c.take(gr.GT16, nl);
+        c.take(gr.G64, nl);
+        c.take(gr.GT64, nl);
+    });
+    if (!ok) {
         gr.release();
         return false;
     }
-    carve(static_cast<char*>(gr.arena));
-    gr.part_floats = part_floats;
+    for (int l = 0; l <= NL; ++l) gr.Hs[l] = (l & 1) ? act1 : act0;
+    for (int l = 0; l < NL; ++l) {
+        gr.Hu[l] = hu;
+        gr.S[l] = sb;
+    }
     gr.cap_n = n;
     gr.cap_nnz = nnz;
+    return true;
+}
+
+// The training layout of the current graph: every layer's activations kept
+// for the backward pass, the pre-activations Au and the gradient buffers.
+bool ensure_training_buffers(Graph& gr) {
+    if (gr.train_arena != nullptr) return true;
+    const size_t n = gr.cap_n, nl = gr.cap_nnz, nh = n * H, nho = n * HO;
+    const size_t tiles = nblk(n, kRows);
+    const size_t part_floats = std::max({tiles * size_t(H * 2 * H + H), n * 2 * H, n * kOutPart});
+    Graph t = gr;  // laid out on a copy, adopted only when the allocation succeeded
+    const bool ok = allocate_laid_out(t.train_arena, [&](Carver& c) {
+        for (int l = 0; l <= NL; ++l) c.take(t.Hs[l], nh);
+        for (int l = 0; l < NL; ++l) {
+            c.take(t.Hu[l], nh);
+            c.take(t.S[l], nh);
+            c.take(t.Au[l], nh);
+        }
+        c.take(t.dg, nl);
+        c.take(t.dH, nh);
+        c.take(t.dHn, nh);
+        c.take(t.dS, nh);
+        c.take(t.dHu, nh);
+        c.take(t.dHp, nho);
+        c.take(t.dHq, nho);
+        c.take(t.part, part_floats);
+        c.take(t.pw, n);
+        c.take(t.pu, n);
+        c.take(t.pv, n);
+        c.take(t.pdv, n);
+        c.take(t.pdu, n);
+    });
+    if (!ok) return false;
+    t.part_floats = part_floats;
+    gr = t;
     return true;
 }
 
@@ -1484,6 +1528,7 @@ clsparseStatus clsparseB200SpaiLossGrad(clsparseB200Spai net, const cldenseVecto
     if (st != clsparseSuccess) return st;
     if (K > 0 && (!probes || probes->num_values < size_t(K) * net->gr.n)) return clsparseInvalidSize;
     DeviceGuard g(control->device);
+    if (!ensure_training_buffers(net->gr)) return clsparseOutOfResources;
     st = ensure_blocks(net->gr, control->stream);
     if (st != clsparseSuccess) return st;
     const int bf16 = fp32Weights ? 0 : 1;
