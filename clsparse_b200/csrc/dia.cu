@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_pcg_kernel(Dia
     // ---- r = b, x = 0, z = M r, <r,z>, <r,r>
     {
         double acc[2] = {0.0, 0.0};
-        if constexpr (PK == 1) {
+        if constexpr (PK >= 1) {
             for_rows(n, [&](uint32_t i) {
                 float ti;
                 const float zi =
@@ -404,7 +404,51 @@ __global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_pcg_kernel(Dia
             }
             const float alpha = static_cast<float>(rz / pq[0]);
             // ---- B
-            if constexpr (PK == 1) {
+            if constexpr (PK == 2) {
+                // t = G r_new for this CTA's rows and the gt_halo rows after
+                // them, into shared memory (t_j needs only q and r, complete
+                // since A's exchange), then z = G^T t from there: G^T's
+                // offsets are >= 0, so no other CTA's t is needed and one
+                // grid exchange per iteration goes away
+                extern __shared__ float ts[];
+                const uint64_t c = blockIdx.x, G = gridDim.x;
+                const uint32_t r0 = static_cast<uint32_t>(c * n / G), r1 = static_cast<uint32_t>((c + 1) * n / G);
+                const uint32_t hi = static_cast<uint32_t>(
+                    std::min<uint64_t>(n, static_cast<uint64_t>(r1) + a.gt_halo));
+                const float* Rc = a.r[cur];
+                float* Rn = a.r[cur ^ 1];
+                double acc2[2] = {0.0, 0.0};
+                auto rnew = [&](uint32_t k) { return fmaf(-alpha, vld(q + k), vld(Rc + k)); };
+                for (uint32_t i = r0 + tid; i < hi; i += kDiaThreads) {
+                    const float ti = dia_row<NDG>(a.G, n, i, rnew);
+                    ts[i - r0] = ti;
+                    if (i < r1) {
+                        x[i] = fmaf(alpha, P[i], x[i]);
+                        const float rn = fmaf(-alpha, q[i], Rc[i]);
+                        Rn[i] = rn;
+                        acc2[0] += static_cast<double>(rn) * rn;
+                        acc2[1] += static_cast<double>(ti) * ti;
+                    }
+                }
+                __syncthreads();
+                for (uint32_t i = r0 + tid; i < r1; i += kDiaThreads)
+                    z[i] = dia_row<NDG>(a.GT, n, i, [&](uint32_t k) { return ts[k - r0]; });
+                double tot[2];
+                if (!grid_exchange<2>(g, epoch, acc2, tot, gs)) goto fail;
+                rr = tot[0];
+                cur ^= 1;
+                ++iters;
+                pold = pn;
+                use_p = true;
+                if (!isfinite(rr)) {
+                    status |= kStatusNonFinite;
+                    break;
+                }
+                if (rr <= tol2 * rr0 || iters >= in.max_iters) break;
+                beta = static_cast<float>(tot[1] / rz);
+                rz = tot[1];
+                continue;
+            } else if constexpr (PK == 1) {
                 const float* Rc = a.r[cur];
                 float* Rn = a.r[cur ^ 1];
                 double acc2[2] = {0.0, 0.0};
@@ -510,25 +554,28 @@ fail:
 }
 
 template <typename VA, typename VG, int PK, int NDA, int NDG>
-int dia_grid(int sm_count) {
-    static int per_sm = [] {
-        int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dia_pcg_kernel<VA, VG, PK, NDA, NDG>, kDiaThreads,
-                                                          0) != cudaSuccess) {
-            cudaGetLastError();
-            b = 1;
-        }
-        return std::max(1, std::min(b, kDiaCtasPerSm));
-    }();
-    return std::max(1, sm_count) * per_sm;
+int dia_grid(int sm_count, size_t smem) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dia_pcg_kernel<VA, VG, PK, NDA, NDG>, kDiaThreads,
+                                                      smem) != cudaSuccess) {
+        cudaGetLastError();
+        b = 1;
+    }
+    return std::max(1, sm_count) * std::max(1, std::min(b, kDiaCtasPerSm));
 }
 
+// smem: dynamic shared memory of the launch (the local-t learned form).
 template <typename VA, typename VG, int PK, int NDA, int NDG>
-cudaError_t dia_launch(DiaPcgArgs<VA, VG>& a, int sm_count, cudaStream_t s, uint32_t& grid) {
-    grid = static_cast<uint32_t>(dia_grid<VA, VG, PK, NDA, NDG>(sm_count));
+cudaError_t dia_launch(DiaPcgArgs<VA, VG>& a, int sm_count, cudaStream_t s, uint32_t& grid, size_t smem = 0) {
+    const void* k = reinterpret_cast<const void*>(dia_pcg_kernel<VA, VG, PK, NDA, NDG>);
+    if (smem > 0) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+    }
+    grid = static_cast<uint32_t>(dia_grid<VA, VG, PK, NDA, NDG>(sm_count, smem));
     void* args[] = {&a};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(dia_pcg_kernel<VA, VG, PK, NDA, NDG>),
-                                       dim3(grid), dim3(kDiaThreads), args, 0, s);
+    return cudaLaunchCooperativeKernel(k, dim3(grid), dim3(kDiaThreads), args, smem, s);
 }
 
 // Padded diagonal counts the kernel is built for: A alone (Jacobi / none),
@@ -654,6 +701,22 @@ void dia_classes(int nda, int ndg, bool learned, int& ca, int& cg) {
 namespace {
 
 // One inner solve as one cooperative launch.
+// Shared memory of the local-t learned form (t for a CTA's rows and the
+// gt_halo rows after them), or 0 when that form does not apply: an offset of
+// G^T below zero, more than kLocalTMaxSmem bytes, or CLSPARSE_B200_DIA_LOCAL_T=0.
+constexpr size_t kLocalTMaxSmem = 160 * 1024;
+template <typename VA, typename VG>
+size_t local_t_smem(const DiaPcgArgs<VA, VG>& a, int sm_count) {
+    const char* env = std::getenv("CLSPARSE_B200_DIA_LOCAL_T");
+    if (env && std::atoi(env) == 0) return 0;
+    for (int e = 0; e < a.GT.nd; ++e)
+        if (a.GT.off[e] < 0) return 0;
+    const uint64_t G = static_cast<uint64_t>(std::max(1, sm_count));  // one CTA per SM
+    const uint64_t rows = (a.n + G - 1) / G + a.gt_halo;
+    const size_t bytes = static_cast<size_t>(rows) * sizeof(float);
+    return bytes <= kLocalTMaxSmem ? bytes : 0;
+}
+
 template <typename VA, typename VG>
 clsparseStatus dia_persistent_solve(DiaPcgArgs<VA, VG> a, bool learned, DiaWork& w, clsparseControl c,
                                     DiaPcgState& st) {
@@ -687,6 +750,13 @@ clsparseStatus dia_persistent_solve(DiaPcgArgs<VA, VG> a, bool learned, DiaWork&
         else if (na == 7) e = dia_launch<VA, VG, 0, 7, 3>(a, sms, s, grid);
         else if (na == 9) e = dia_launch<VA, VG, 0, 9, 3>(a, sms, s, grid);
         else if (na == kMaxDiags) e = dia_launch<VA, VG, 0, kMaxDiags, 3>(a, sms, s, grid);
+    } else if (local_t_smem(a, sms) > 0) {
+        // t kept per CTA in shared memory: two grid exchanges per iteration
+        const size_t sm = local_t_smem(a, sms);
+        if (na == 5 && ng == 3) e = dia_launch<VA, VG, 2, 5, 3>(a, sms, s, grid, sm);
+        else if (na == 7 && ng == 4) e = dia_launch<VA, VG, 2, 7, 4>(a, sms, s, grid, sm);
+        else if (na == 9 && ng == 5) e = dia_launch<VA, VG, 2, 9, 5>(a, sms, s, grid, sm);
+        else if (na == kMaxDiags && ng == kMaxDiags) e = dia_launch<VA, VG, 2, kMaxDiags, kMaxDiags>(a, sms, s, grid, sm);
     } else {
         if (na == 5 && ng == 3) e = dia_launch<VA, VG, 1, 5, 3>(a, sms, s, grid);
         else if (na == 7 && ng == 4) e = dia_launch<VA, VG, 1, 7, 4>(a, sms, s, grid);

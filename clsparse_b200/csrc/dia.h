@@ -62,6 +62,7 @@ struct DiaPcgArgs {
     float* z;
     uint32_t n;
     int gt_diag;            // index of G^T's main diagonal (learned solves)
+    uint32_t gt_halo;       // largest column offset of G^T (its offsets are >= 0: G is lower triangular)
     FusedSync sync;
     DiaPcgState* st;
 };

@@ -188,8 +188,11 @@ clsparseStatus banded_solve(BandedInner<V>& bi, bool learned, bool jacobi, float
     a.z = bi.vec[6];
     a.n = n;
     a.gt_diag = 0;
-    for (int d = bi.GT.nd - 1; d >= 0; --d)  // the first zero offset: the real diagonal, padding comes after
+    a.gt_halo = 0;
+    for (int d = bi.GT.nd - 1; d >= 0; --d) {  // the first zero offset: the real diagonal, padding comes after
         if (bi.GT.off[d] == 0) a.gt_diag = d;
+        if (bi.GT.off[d] > 0) a.gt_halo = std::max<uint32_t>(a.gt_halo, static_cast<uint32_t>(bi.GT.off[d]));
+    }
     DiaPcgState st;
     st.tol = tol;
     st.max_iters = inner.maxIters;

@@ -96,6 +96,32 @@ def test_banded_learned_matches_csr(ctrl, monkeypatch):
     assert np.linalg.norm(xb - xc) / np.linalg.norm(xc) <= 1e-7
 
 
+@pytest.mark.parametrize("m", [96, 300])
+def test_local_t_form_equals_three_phase_form(ctrl, monkeypatch, m):
+    """The learned iteration with t = G r kept per CTA in shared memory (two
+    grid exchanges per iteration) computes every value the three-phase form
+    computes, in the same order: the solves agree bit for bit. 300^2 rows
+    gives slices whose halo reaches into the next CTA's rows."""
+    spai, _ = learn.train(ctrl, sizes=(32,), seeds=range(2), steps=40, lr=3e-3)
+    smp = learn.Sample(ctrl, m, 7, with_probes=False)
+    spai.set_matrix(smp.A, ctrl)
+    spai.build(ctrl)
+    out = {}
+    for local in ("1", "0"):
+        monkeypatch.setenv("CLSPARSE_B200_DIA_LOCAL_T", local)
+        x = torch.zeros(smp.A.num_rows, dtype=torch.float64, device="cuda")
+        sc = api.SolverControl(L.DIAGONAL, 100000, 1e-10, 0.0)
+        out[local] = (api.cg_learned(x, smp.A, smp.b, sc, spai, ctrl, inner="fp32", inner_tol=0.3),
+                      x.cpu().numpy())
+        sc.release()
+    spai.release()
+    (i1, x1), (i0, x0) = out["1"], out["0"]
+    assert i1["converged"] == 1 and i1["fell_back"] == 0
+    assert i1["innerIterations"] == i0["innerIterations"]
+    np.testing.assert_array_equal(x1, x0)
+    assert residual(*smp.np, x1, smp.b.cpu().numpy()) <= 1.5e-10
+
+
 def test_matrix_with_many_diagonals_stays_on_csr(ctrl, monkeypatch):
     mat = matgen.random_spd(3000, seed=5)
     n = len(mat[0]) - 1
