@@ -732,7 +732,14 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total_ms, e2e_ms, avg_launch_ms, e2e_serial_ms = t.tolist()
-    dcg = None if args.no_cg else dist_cg_section(rank, world)  # every rank takes part
+    dcg = None
+    if not args.no_cg:
+        # every rank takes part; an error (raised alike on every rank: the
+        # ranks run the same stages) is reported instead of the entry
+        try:
+            dcg = dist_cg_section(rank, world)
+        except Exception as exc:  # noqa: BLE001
+            dcg = {"error": f"{type(exc).__name__}: {exc}"[:300]}
     if rank != 0:
         ctrl.release()
         return
