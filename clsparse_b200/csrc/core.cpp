@@ -213,7 +213,7 @@ clsparseStatus clsparseReleaseControl(clsparseControl control) {
 
 clsparseStatus clsparseB200SetSolverLoopMode(clsparseControl control, cl_int mode) {
     if (control == nullptr) return clsparseInvalidControlObject;
-    if (mode < 0 || mode > 2) return clsparseInvalidValue;
+    if (mode < 0 || mode > 3) return clsparseInvalidValue;
     control->solver_loop_mode = mode;
     return clsparseSuccess;
 }

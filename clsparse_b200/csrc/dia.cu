@@ -553,6 +553,257 @@ fail:
     if (tid == 0) atomicOr(&a.st->status, kStatusBarrierTimeout);
 }
 
+// ---- the drop-in CG (clsparse{S,D}csrcg, solver loop mode 3)
+
+// In/out block of one drop-in solve.
+struct DiaCgState {
+    // in: the solver control
+    double rel_tol = 0.0, abs_tol = 0.0;
+    int max_iters = 0;
+    int n_iters_in = 0;  // nIters the control held before the solve (the first stop test sees it)
+    int l2 = 0;          // 0: ||.||_1 stop test as the reference, 1: ||.||_2
+    int stop_nonfinite = 0;
+    // out
+    int n_iters = 0;
+    int zero_b = 0;      // ||b|| == 0: x = b, nothing else done
+    int zero_diag = 0;   // Jacobi with a zero on the main diagonal: nothing written to x
+    int status = 0;      // kStatusCurvature / kStatusNonFinite / kStatusBarrierTimeout
+    double init_res = 0.0, cur_res = 0.0;
+};
+
+// Rows [r0, r1) whose CSR-Adaptive block reduces a row over g > 1 lanes.
+struct LaneRange {
+    uint32_t r0, r1, g;
+};
+constexpr int kMaxLaneRanges = 8;
+
+template <typename T>
+struct DiaCgArgs {
+    DiaMat<T> A;
+    // CSR arrays of A, for the rows of lane ranges
+    const uint32_t* rp;
+    const uint32_t* cols;
+    const T* vals;
+    LaneRange lanes[kMaxLaneRanges];
+    int nlanes;
+    int d0;         // index of the main diagonal (Jacobi)
+    T* invD;        // Jacobi: 1 / a_ii, formed in the prologue; nullptr: no preconditioner
+    const T* b;
+    T* x;           // initial guess in, solution out
+    T* r;
+    T* p[2];        // direction of iteration k in p[k & 1]
+    T* q;           // A p
+    T* z;           // M r (== r without preconditioner)
+    uint32_t n;
+    FusedSync sync;
+    DiaCgState* st;
+};
+
+// Separately rounded products and sums (no contraction into FMAs): the
+// arithmetic of the reference's kernels as compiled for its CPU runs.
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+using dev::mul_rn;
+
+// sum_d M[d][i] * xf(i + off[d]) in T: products rounded, then summed one by
+// one in increasing column order from zero -- the order of a CSR-Adaptive
+// STREAM block that reduces each row on one lane
+// (src/library/kernels/csrmv_adaptive.cl:312-420); the zeros of entries a
+// CSR row does not hold add nothing. Loads are unconditional with
+// out-of-matrix columns clamped and zeroed (as dia_row).
+template <int ND, typename T, typename XF>
+__device__ __forceinline__ T dia_row_seq(const DiaMat<T>& M, uint32_t n, uint32_t i, XF xf) {
+    T av[ND], xv[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        const int64_t j = static_cast<int64_t>(i) + M.off[d];
+        const bool in = j >= 0 && j < static_cast<int64_t>(n);
+        const uint32_t jc = in ? static_cast<uint32_t>(j) : i;
+        av[d] = __ldg(M.vals + static_cast<size_t>(d) * n + i);
+        const T v = xf(jc);
+        xv[d] = in ? v : T(0);
+    }
+    T s = T(0);
+#pragma unroll
+    for (int d = 0; d < ND; ++d) s = add_rn(s, mul_rn(av[d], xv[d]));
+    return s;
+}
+
+// Row i of a CSR-Adaptive STREAM block that reduces a row over g lanes (g a
+// power of two): lane l sums the row's products l, l + g, ... one by one,
+// then the lanes combine pairwise at distances g/2, ..., 1. A banded row
+// holds at most kMaxDiags entries, so lanes from kMaxDiags on hold zero.
+template <typename T, typename XF>
+__device__ __noinline__ T csr_row_lanes(const uint32_t* rp, const uint32_t* cols, const T* vals, uint32_t i,
+                                        uint32_t g, XF xf) {
+    T v[kMaxDiags];
+#pragma unroll
+    for (int l = 0; l < kMaxDiags; ++l) v[l] = T(0);
+    g = g > static_cast<uint32_t>(kMaxDiags) ? static_cast<uint32_t>(kMaxDiags) : g;
+    const uint32_t b = rp[i], e = rp[i + 1];
+    for (uint32_t k = b; k < e; ++k) {
+        const uint32_t l = (k - b) & (g - 1);
+        v[l] = add_rn(v[l], mul_rn(__ldg(vals + k), xf(cols[k])));
+    }
+    for (uint32_t off = g / 2; off > 0; off >>= 1)
+        for (uint32_t l = 0; l < off; ++l) v[l] = add_rn(v[l], v[l + off]);
+    return v[0];
+}
+
+// q_i = (A xf)_i in the reference's order for row i.
+template <int ND, typename T, typename XF>
+__device__ __forceinline__ T cg_row(const DiaCgArgs<T>& a, uint32_t i, XF xf) {
+    for (int k = 0; k < a.nlanes; ++k)
+        if (i >= a.lanes[k].r0 && i < a.lanes[k].r1) return csr_row_lanes(a.rp, a.cols, a.vals, i, a.lanes[k].g, xf);
+    return dia_row_seq<ND>(a.A, a.n, i, xf);
+}
+
+// The reference's CG (src/library/solvers/conjugate-gradients.hpp:73-226) as
+// one cooperative launch over a matrix stored by diagonal. Scalars in T as
+// the reference's clsparse::scalar<T>, reductions accumulated in FP64:
+//   prologue: r = b - A x, z = M r, p = z; ||b||, ||r||, <r,z>   -> exchange
+//             ||b|| == 0: x = b, stop; res = ||r|| / ||b||; stop test with
+//             the control's previous nIters
+//   A: p_k = z + beta p_{k-1} (k > 0; a neighbour's p_k formed on the fly
+//      from its z and p_{k-1}), q = A p_k, <q,p_k>          -> exchange: alpha
+//   B: x += alpha p_k, r -= alpha q, z = M r; <r,z>, ||r||   -> exchange:
+//      beta = <r,z>_new / <r,z>_old, res, nIters = k, stop test
+// The exchanges are bounded waits; a timeout leaves every CTA and sets
+// kStatusBarrierTimeout.
+template <typename T, int ND>
+__global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_cg_ref_kernel(DiaCgArgs<T> a) {
+    __shared__ GridSmem gs;
+    const FusedSync g = a.sync;
+    unsigned long long epoch = 0;
+    const uint32_t n = a.n;
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    // No __restrict__: these vectors are read at neighbouring rows by other CTAs.
+    T* x = a.x;
+    T* r = a.r;
+    T* q = a.q;
+    T* z = a.z;
+    T* invD = a.invD;
+    const T* b = a.b;
+    const DiaCgState in = *a.st;
+    const int l2 = in.l2;
+    auto term = [l2](T v) {
+        const double d = static_cast<double>(v);
+        return l2 ? mul_rn(d, d) : fabs(d);
+    };
+    auto finish_norm = [l2](double s) { return l2 ? sqrt(s) : s; };
+
+    // ---- prologue
+    double tot0[4];
+    {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        T* p0 = a.p[0];
+        for_rows(n, [&](uint32_t i) {
+            const T y = cg_row<ND>(a, i, [&](uint32_t j) { return x[j]; });
+            const T bi = __ldg(b + i);
+            const T ri = add_rn(bi, -y);
+            T zi = ri;
+            if (invD != nullptr) {
+                const T d = __ldg(a.A.vals + static_cast<size_t>(a.d0) * n + i);
+                const T inv = T(1) / d;
+                invD[i] = inv;
+                zi = mul_rn(ri, inv);
+                acc[3] += d == T(0) ? 1.0 : 0.0;
+                z[i] = zi;
+            }
+            r[i] = ri;
+            p0[i] = zi;
+            acc[0] = add_rn(acc[0], term(bi));
+            acc[1] = add_rn(acc[1], term(ri));
+            acc[2] = add_rn(acc[2], mul_rn(static_cast<double>(ri), static_cast<double>(zi)));
+        });
+        if (!grid_exchange<4>(g, epoch, acc, tot0, gs)) goto fail;
+    }
+    if (tot0[3] > 0.0) {
+        if (lead) a.st->zero_diag = 1;
+        return;
+    }
+    {
+        const T norm_b = static_cast<T>(finish_norm(tot0[0]));
+        if (norm_b == T(0)) {
+            for_rows(n, [&](uint32_t i) { x[i] = __ldg(b + i); });
+            if (lead) {
+                a.st->zero_b = 1;
+                a.st->n_iters = 0;
+            }
+            return;
+        }
+        const T norm_r0 = static_cast<T>(finish_norm(tot0[1]));
+        const double init_res = static_cast<double>(norm_r0 / norm_b);
+        auto finished = [&](double res, int n_iters) {
+            return res <= in.rel_tol || res <= in.abs_tol * init_res || n_iters >= in.max_iters ||
+                   (in.stop_nonfinite && !isfinite(res));
+        };
+        T rz = static_cast<T>(tot0[2]);
+        T beta = T(0);
+        double cur_res = init_res;
+        int n_iters = 0, status = 0;
+        bool done = finished(init_res, in.n_iters_in);
+        for (int k = 0; !done; ++k) {
+            T* pk = a.p[k & 1];
+            const T* pprev = a.p[(k + 1) & 1];
+            // ---- A: p_k, q = A p_k, <q, p_k>
+            double pq[1] = {0.0};
+            for_rows(n, [&](uint32_t i) {
+                T pi;
+                if (k == 0) {
+                    pi = pk[i];
+                } else {
+                    pi = add_rn(z[i], mul_rn(beta, pprev[i]));
+                    pk[i] = pi;
+                }
+                const T qi = k == 0 ? cg_row<ND>(a, i, [&](uint32_t j) { return pk[j]; })
+                                    : cg_row<ND>(a, i, [&](uint32_t j) { return add_rn(z[j], mul_rn(beta, pprev[j])); });
+                q[i] = qi;
+                pq[0] = add_rn(pq[0], mul_rn(static_cast<double>(qi), static_cast<double>(pi)));
+            });
+            double tq[1];
+            if (!grid_exchange<1>(g, epoch, pq, tq, gs)) goto fail;
+            const T yp = static_cast<T>(tq[0]);
+            const T alpha = rz / yp;
+            if (!(yp > T(0))) status |= kStatusCurvature;
+            // ---- B: x, r, z; <r,z>, ||r||
+            double acc[2] = {0.0, 0.0};
+            for_rows(n, [&](uint32_t i) {
+                const T pi = pk[i];
+                x[i] = add_rn(x[i], mul_rn(alpha, pi));
+                const T ri = add_rn(r[i], -mul_rn(alpha, q[i]));
+                r[i] = ri;
+                T zi = ri;
+                if (invD != nullptr) {
+                    zi = mul_rn(ri, invD[i]);
+                    z[i] = zi;
+                }
+                acc[0] = add_rn(acc[0], mul_rn(static_cast<double>(ri), static_cast<double>(zi)));
+                acc[1] = add_rn(acc[1], term(ri));
+            });
+            double tb[2];
+            if (!grid_exchange<2>(g, epoch, acc, tb, gs)) goto fail;
+            const T rz_old = rz;
+            rz = static_cast<T>(tb[0]);
+            beta = rz / rz_old;
+            const T res = static_cast<T>(finish_norm(tb[1])) / norm_b;
+            n_iters = k;
+            cur_res = static_cast<double>(res);
+            if (!isfinite(cur_res)) status |= kStatusNonFinite;
+            done = finished(cur_res, n_iters);
+        }
+        if (lead) {
+            a.st->n_iters = n_iters;
+            a.st->init_res = init_res;
+            a.st->cur_res = cur_res;
+            atomicOr(&a.st->status, status);
+        }
+        return;
+    }
+fail:
+    if (threadIdx.x == 0) atomicOr(&a.st->status, kStatusBarrierTimeout);
+}
+
 template <typename VA, typename VG, int PK, int NDA, int NDG>
 int dia_grid(int sm_count, size_t smem) {
     int b = 0;
@@ -781,6 +1032,159 @@ clsparseStatus dia_pcg_solve(DiaPcgArgs<VA, VG> a, bool learned, DiaWork& w, cls
                              DiaPcgState& st) {
     return dia_persistent_solve<VA, VG>(a, learned, w, c, st);
 }
+
+namespace {
+
+template <typename T, int ND>
+cudaError_t dia_cg_launch(DiaCgArgs<T>& a, int sm_count, cudaStream_t s, uint32_t max_grid) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dia_cg_ref_kernel<T, ND>, kDiaThreads, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return cudaErrorInvalidConfiguration;
+    }
+    if (b < 1) return cudaErrorInvalidConfiguration;
+    const uint32_t grid = static_cast<uint32_t>(std::max(1, sm_count) * std::min(b, kDiaCtasPerSm));
+    if (grid > max_grid) return cudaErrorInvalidConfiguration;
+    void* args[] = {&a};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(dia_cg_ref_kernel<T, ND>), dim3(grid),
+                                       dim3(kDiaThreads), args, 0, s);
+}
+
+}  // namespace
+
+template <typename T>
+clsparseStatus dia_cg_dropin(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
+                             clSParseSolverControl sc, clsparseControl c) {
+    const uint32_t n = static_cast<uint32_t>(A->num_rows);
+    const uint32_t nnz = static_cast<uint32_t>(A->num_nonzeros);
+    if (n == 0 || nnz == 0) return clsparseNotImplemented;
+    // The reference's CG multiplies with csrmv_adaptive when the matrix has a
+    // meta (csrmv_general otherwise: the graph engine runs that order). Its
+    // STREAM blocks reduce a row on one lane except in a few blocks (the last
+    // one, with few rows): those row ranges are taken over as CSR rows with
+    // their lane count. A block of another kind, or more such ranges than
+    // kMaxLaneRanges, leaves the solve to the graph engine.
+    const auto* meta = static_cast<const matrix_meta*>(A->meta);
+    if (meta == nullptr || meta->h_rowBlocks.size() < meta->num_words || meta->num_words < 2)
+        return clsparseNotImplemented;
+    LaneRange lanes[kMaxLaneRanges];
+    int nlanes = 0;
+    for (size_t w = 0; w + 1 < meta->num_words; ++w) {
+        const uint64_t w0 = meta->h_rowBlocks[w], w1 = meta->h_rowBlocks[w + 1];
+        const uint32_t r0 = static_cast<uint32_t>(w0 >> 32), r1 = static_cast<uint32_t>(w1 >> 32);
+        if (r1 - r0 <= meta->rows_for_vector) return clsparseNotImplemented;  // not a STREAM block
+        const uint32_t low = static_cast<uint32_t>(w0 & ((1u << kWgBits) - 1u));
+        const uint32_t g = low == 0 ? 1u : std::min(low, 32u);
+        if (g == 1) continue;
+        if ((g & (g - 1)) != 0 || nlanes == kMaxLaneRanges) return clsparseNotImplemented;
+        if (nlanes > 0 && lanes[nlanes - 1].r1 == r0 && lanes[nlanes - 1].g == g)
+            lanes[nlanes - 1].r1 = r1;
+        else
+            lanes[nlanes++] = LaneRange{r0, r1, g};
+    }
+    cudaStream_t s = c->stream;
+    if (!c->dia_cg) c->dia_cg = std::make_unique<DiaWork>();
+    DiaWork& w = *c->dia_cg;
+    const uint32_t* rp = dev_ptr<const uint32_t>(A->row_pointer, A->off_row_pointer);
+    const uint32_t* cols = dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices);
+    const T* vals = dev_ptr<const T>(A->values, A->off_values);
+    DiaOffsets offs;
+    clsparseStatus stt = dia_detect(rp, cols, n, nnz, w, s, offs);
+    if (stt == clsparseInvalidValue) return clsparseNotImplemented;  // not banded
+    if (stt != clsparseSuccess) return stt;
+    int ca = 0, cg = 0;
+    dia_classes(offs.nd, 0, false, ca, cg);
+    const bool jac = sc->preconditioner == DIAGONAL;
+    bool has_main = false;
+    for (int d = 0; d < offs.nd; ++d) has_main |= offs.off[d] == 0;
+    if (ca == 0 || (jac && !has_main)) return clsparseNotImplemented;
+    DiaMat<T> M;
+    stt = dia_build<T, T>(rp, cols, vals, n, offs, ca, w.A, s, M);
+    if (stt != clsparseSuccess) return stt;
+
+    // work vectors: invD, r, p[0], p[1], q, z
+    const size_t vb = align256(static_cast<size_t>(n) * sizeof(T));
+    const uint32_t max_grid = static_cast<uint32_t>(std::max(1, c->sm_count) * kDiaCtasPerSm);
+    const size_t sync_b = align256(fused_sync_bytes(max_grid));
+    if (w.vecs.ensure(6 * vb) != cudaSuccess || w.sync.ensure(sync_b + align256(sizeof(DiaCgState))) != cudaSuccess) {
+        cudaGetLastError();
+        return clsparseOutOfResources;
+    }
+    char* vbase = static_cast<char*>(w.vecs.ptr);
+    auto vec = [&](int k) { return reinterpret_cast<T*>(vbase + static_cast<size_t>(k) * vb); };
+    DiaCgArgs<T> a{};
+    a.A = M;
+    a.rp = rp;
+    a.cols = cols;
+    a.vals = vals;
+    for (int k = 0; k < nlanes; ++k) a.lanes[k] = lanes[k];
+    a.nlanes = nlanes;
+    a.d0 = main_diag_index(M);
+    a.invD = jac ? vec(0) : nullptr;
+    a.b = dev_ptr<const T>(bv->values, bv->off_values);
+    a.x = dev_ptr<T>(xv->values, xv->off_values);
+    a.r = vec(1);
+    a.p[0] = vec(2);
+    a.p[1] = vec(3);
+    a.q = vec(4);
+    a.z = jac ? vec(5) : a.r;
+    a.n = n;
+
+    char* base = static_cast<char*>(w.sync.ptr);
+    DiaCgState h;
+    h.rel_tol = sc->relativeTolerance;
+    h.abs_tol = sc->absoluteTolerance;
+    h.max_iters = sc->maxIters;
+    h.n_iters_in = sc->nIters;
+    h.l2 = sc->normType & 1;
+    h.stop_nonfinite = sc->stopOnNonFinite ? 1 : 0;
+    a.st = reinterpret_cast<DiaCgState*>(base + sync_b);
+    cudaMemsetAsync(base, 0, kFusedSyncHead, s);
+    cudaMemcpyAsync(a.st, &h, sizeof(h), cudaMemcpyHostToDevice, s);
+    a.sync = fused_sync_at(base);
+    // failure-path test switches, as for the other persistent solvers
+    if (const char* e = std::getenv("CLSPARSE_B200_BARRIER_WAIT_NS")) {
+        const unsigned long long v = std::strtoull(e, nullptr, 10);
+        if (v > 0) a.sync.wait_ns = v;
+    }
+    if (const char* e = std::getenv("CLSPARSE_B200_TEST_BARRIER_NEVER_RELEASE")) a.sync.never_release = std::atoi(e) != 0;
+
+    const int sms = c->sm_count;
+    cudaError_t e = cudaErrorInvalidValue;
+    if (ca == 3) e = dia_cg_launch<T, 3>(a, sms, s, max_grid);
+    else if (ca == 5) e = dia_cg_launch<T, 5>(a, sms, s, max_grid);
+    else if (ca == 7) e = dia_cg_launch<T, 7>(a, sms, s, max_grid);
+    else if (ca == 9) e = dia_cg_launch<T, 9>(a, sms, s, max_grid);
+    else if (ca == kMaxDiags) e = dia_cg_launch<T, kMaxDiags>(a, sms, s, max_grid);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return clsparseInvalidKernelExecution;
+    }
+    if (cudaMemcpyAsync(&h, a.st, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return clsparseInvalidKernelExecution;
+    if (c->event) cudaEventRecord(c->event, s);
+    sc->deviceStatus = static_cast<cl_uint>(h.status);
+    sc->historyLength = 0;
+    if (h.status & kStatusBarrierTimeout) return clsparseInvalidKernelExecution;
+    if (h.zero_diag) return clsparseNotImplemented;  // x untouched; the graph engine reports the zero
+    if (h.zero_b) {
+        // conjugate-gradients.hpp:87-95 resets the tolerances of the control
+        sc->nIters = 0;
+        sc->absoluteTolerance = 0.0;
+        sc->relativeTolerance = 0.0;
+        return clsparseSuccess;
+    }
+    sc->initialResidual = h.init_res;
+    sc->currentResidual = h.cur_res;
+    sc->nIters = h.n_iters;
+    return clsparseSuccess;
+}
+
+template clsparseStatus dia_cg_dropin<float>(cldenseVector*, const clsparseCsrMatrix*, const cldenseVector*,
+                                             clSParseSolverControl, clsparseControl);
+template clsparseStatus dia_cg_dropin<double>(cldenseVector*, const clsparseCsrMatrix*, const cldenseVector*,
+                                              clSParseSolverControl, clsparseControl);
 
 #define CLSP_DIA_INST(VA, VG)                                                                                 \
     template clsparseStatus dia_pcg_solve<VA, VG>(DiaPcgArgs<VA, VG>, bool, DiaWork&, clsparseControl,       \

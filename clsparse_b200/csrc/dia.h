@@ -70,6 +70,17 @@ struct DiaPcgArgs {
 // CLSPARSE_B200_DIA=0 keeps every inner solve on CSR.
 bool dia_enabled();
 
+// The drop-in clsparse{S,D}csrcg on the banded engine (solver loop mode 3):
+// the reference's CG (operation order, scalar type T, L1 or L2 stop test,
+// nIters bookkeeping, x as initial guess, x = b for a zero right-hand side)
+// as one cooperative launch for a matrix with at most kMaxDiags distinct
+// diagonals. clsparseNotImplemented when the matrix does not qualify (not
+// banded, or with Jacobi a missing or zero diagonal entry): the caller then
+// runs the graph engine, which reports those cases.
+template <typename T>
+clsparseStatus dia_cg_dropin(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                             clSParseSolverControl sc, clsparseControl c);
+
 // The distinct column offsets of a CSR matrix when there are at most
 // kMaxDiags and they hold at least half of the stored diagonal entries
 // (clsparseSuccess), otherwise clsparseInvalidValue (the caller stays on CSR).

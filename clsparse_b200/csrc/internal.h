@@ -81,7 +81,7 @@ struct _clsparseControl {
     size_t l2_bytes = 0;
     bool async = false;
     bool extended_precision = false;
-    int solver_loop_mode = 0;       // 0 graph while-loop, 1 host chunks, 2 persistent kernel
+    int solver_loop_mode = 0;       // 0 graph while-loop, 1 host chunks, 2 persistent kernel, 3 banded CG
     cudaEvent_t event = nullptr;    // recorded after each call
     cudaStream_t capture_stream = nullptr;  // private stream used for graph capture
     // Reduction scratch: kMaxReduceCtas doubles x 4 partial slots + a ticket.
@@ -91,6 +91,7 @@ struct _clsparseControl {
     std::unique_ptr<clsp::SolverCache> solver_cache;
     std::unique_ptr<clsp::MixedWork> mixed_work;
     std::unique_ptr<clsp::BatchWork> batch_work;
+    std::unique_ptr<clsp::DiaWork> dia_cg;  // banded drop-in CG (solver loop mode 3)
 };
 
 // CSR-Adaptive meta attached to clsparseCsrMatrix::meta (reference

@@ -27,8 +27,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <type_traits>
 
 #include "device_common.cuh"
+#include "dia.h"
 #include "internal.h"
 #include "fused.h"
 #include "solver_cache.h"
@@ -832,6 +834,18 @@ clsparseStatus cg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const cld
     if (stt != clsparseSuccess) return stt;
     DeviceGuard guard(c->device);
     const size_t n = A->num_rows;
+    // Loop mode 3: a banded matrix runs the reference's CG as one cooperative
+    // launch over a diagonal-storage copy (dia.cu); other matrices, and the
+    // options that engine does not carry (history, snapshots, extended
+    // precision, the refinement's continued solves), stay on the engines below.
+    if (c->solver_loop_mode == 3 && std::is_same_v<V, T> && ws == nullptr && n > 0 && !c->extended_precision &&
+        sc->history == nullptr && sc->snapshotCount == 0 && dia_enabled()) {
+        stt = dia_cg_dropin<T>(xv, A, bv, sc, c);
+        if (stt != clsparseNotImplemented) {
+            sc->printSummary(stt);
+            return stt;
+        }
+    }
     if (!c->solver_cache) c->solver_cache = std::make_unique<SolverCache>();
     SolverCache& cache = *c->solver_cache;
     const CsrView<V> Av = view_of<V>(A);

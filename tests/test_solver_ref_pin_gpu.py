@@ -4,7 +4,9 @@ reference's OWN kernels (tests/golden/solvers_ref.npz): the reference's
 solver-test settings (src/tests/test-solvers.cpp:267-277) and a tighter set,
 FP64 and FP32, Jacobi and no preconditioner, a matrix without a meta
 (the reference test's csrmv_general path) and with one (csrmv_adaptive).
-Every run also goes through the persistent engine. The bars are stated in
+Every run also goes through the persistent engine and the banded loop mode
+(CG on the stencil matrices; the other runs fall through to the graph
+engine). The bars are stated in
 tests/solver_golden.py; the library's reductions sum in a different order
 from the reference's, as two GPUs would."""
 from __future__ import annotations
@@ -45,7 +47,7 @@ def lib_solve(ctrl, run, loop_mode, history=False):
     return x.cpu().numpy().astype(np.float64), info, (rel, abs_, max_it)
 
 
-@pytest.mark.parametrize("loop_mode", [0, 2], ids=["graph", "persistent"])
+@pytest.mark.parametrize("loop_mode", [0, 2, 3], ids=["graph", "persistent", "banded"])
 @pytest.mark.parametrize("run", RUNS, ids=[G.run_id(r) for r in RUNS])
 def test_library_solver_matches_reference_run(ctrl, run, loop_mode):
     name, setting, method, t, pre, path = run
