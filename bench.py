@@ -327,6 +327,8 @@ def cg_section(ctrl, with_cpu: bool):
         (clsparseDcsrcgLearned); the network is trained on the GPU by the
         library's kernels on 128^2 matrices of the family (different seeds)
         before the timed solves; training time is reported separately.
+    Beside each FP64 Jacobi-CG entry, banded_loop_mode3 times the same
+    clsparseDcsrcg call with solver loop mode 3 (the banded drop-in engine).
     Each solve is timed on its second call (the first captures the graph).
     Every solution's error against the FP64 oracle solution is stated
     (error_vs_fp64_oracle, relative 2-norm): C1 against the serial oracle
@@ -340,7 +342,7 @@ def cg_section(ctrl, with_cpu: bool):
     out = {}
     solutions = {}  # config -> {entry: x on the host}, compared with the oracle at the end
 
-    def fp64_cg(A, b, x, l2=True, max_iters=200000):
+    def fp64_cg(A, b, x, l2=True, max_iters=200000, loop_mode=0):
         def run():
             x.zero_()
             sc = api.SolverControl(L.DIAGONAL, max_iters, 1e-10, 0.0)
@@ -349,7 +351,22 @@ def cg_section(ctrl, with_cpu: bool):
             info = api.solve("cg", x, A, b, sc, ctrl)
             sc.release()
             return info
-        return _timed(run)
+        ctrl.set_solver_loop_mode(loop_mode)
+        try:
+            return _timed(run)
+        finally:
+            ctrl.set_solver_loop_mode(0)
+
+    # The same drop-in clsparseDcsrcg call with the banded engine (solver loop
+    # mode 3): one cooperative launch over a diagonal-storage copy rebuilt at
+    # every call (inside the timing), rows in the reference's CSR-Adaptive
+    # order; its x against the default engine's.
+    def banded_entry(A, b, x, l2, t_default):
+        x_default = x.clone()
+        t, info = fp64_cg(A, b, x, l2=l2, loop_mode=3)
+        d = float((x - x_default).abs().max() / x_default.abs().max())
+        return {"s": round(t, 5), "iterations": info["nIters"] + (1 if l2 else 0),
+                "speedup_vs_default_engine": round(t_default / t, 3), "max_rel_diff_vs_default_engine": d}
 
     def true_res(np_mat, x, b):
         import scipy.sparse as sp
@@ -380,6 +397,10 @@ def cg_section(ctrl, with_cpu: bool):
         c1_out["speedup_vs_cpu"] = round(tc / t, 1)
         xg = x.cpu().numpy()
         c1_out["error_vs_fp64_oracle"] = float(np.linalg.norm(xg - xo) / np.linalg.norm(xo))
+    c1_banded = banded_entry(A, b, x, False, t)
+    if with_cpu:
+        c1_banded["speedup_vs_cpu"] = round(tc / c1_banded["s"], 1)
+    c1_out["banded_loop_mode3"] = c1_banded
     out["C1"] = c1_out
     del A
 
@@ -393,6 +414,7 @@ def cg_section(ctrl, with_cpu: bool):
     t64, i64 = fp64_cg(A, b, x)
     r64 = true_res(c3, x, b)
     solutions["C3"] = {"fp64_jacobi": x.cpu().numpy()}
+    c3_banded = banded_entry(A, b, x, True, t64)
 
     def mixed():
         x.zero_()
@@ -424,7 +446,8 @@ def cg_section(ctrl, with_cpu: bool):
     if ibf["converged"]:
         solutions["C3"]["mixed_bf16"] = x.cpu().numpy()
     out["C3"] = {"workload": "3D 7-point log-normal diffusion 128^3 (n=2,097,152, sigma 1.5), rel. L2 residual 1e-10",
-                 "fp64_jacobi": {"s": round(t64, 5), "iterations": i64["nIters"] + 1, "true_residual": r64},
+                 "fp64_jacobi": {"s": round(t64, 5), "iterations": i64["nIters"] + 1, "true_residual": r64,
+                                 "banded_loop_mode3": c3_banded},
                  "mixed_fp32": {"s": round(tm, 5), "inner_iterations": im["innerIterations"],
                                 "refinements": im["outerIterations"], "true_residual": r3},
                  "mixed_bf16": bf16_out,
@@ -468,6 +491,7 @@ def cg_section(ctrl, with_cpu: bool):
     t64, i64 = fp64_cg(A, b, x)
     r64 = true_res(c5, x, b)
     solutions["C5"] = {"fp64_jacobi": x.cpu().numpy()}
+    c5_banded = banded_entry(A, b, x, True, t64)
 
     def mixed5():
         x.zero_()
@@ -504,7 +528,8 @@ def cg_section(ctrl, with_cpu: bool):
     solutions["C5"]["learned_mixed_fp32"] = x.cpu().numpy()
     spai.release()
     out["C5"] = {"workload": "2D GRF diffusion 1024^2 (n=1,048,576, corr 0.05, sigma 2), rel. L2 residual 1e-10",
-                 "fp64_jacobi": {"s": round(t64, 5), "iterations": i64["nIters"] + 1, "true_residual": r64},
+                 "fp64_jacobi": {"s": round(t64, 5), "iterations": i64["nIters"] + 1, "true_residual": r64,
+                                 "banded_loop_mode3": c5_banded},
                  "mixed_fp32": {"s": round(tm, 5), "inner_iterations": im["innerIterations"],
                                 "refinements": im["outerIterations"], "true_residual": rm,
                                 "speedup": round(t64 / tm, 3)},

@@ -586,6 +586,11 @@ struct DiaCgArgs {
     const T* vals;
     LaneRange lanes[kMaxLaneRanges];
     int nlanes;
+    // A symmetric bit for bit with its offsets symmetric (the kernel's SYM
+    // form): the value of lower diagonal d at row i is read as A[j][i] from
+    // its upper partner nd_real - 1 - d at row j = i + off[d], and the lower
+    // diagonals are not read at all
+    int nd_real;
     int d0;         // index of the main diagonal (Jacobi)
     T* invD;        // Jacobi: 1 / a_ii, formed in the prologue; nullptr: no preconditioner
     const T* b;
@@ -605,23 +610,30 @@ __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 using dev::mul_rn;
 
-// sum_d M[d][i] * xf(i + off[d]) in T: products rounded, then summed one by
+// sum_d A[d][i] * xf(i + off[d]) in T: products rounded, then summed one by
 // one in increasing column order from zero -- the order of a CSR-Adaptive
 // STREAM block that reduces each row on one lane
 // (src/library/kernels/csrmv_adaptive.cl:312-420); the zeros of entries a
 // CSR row does not hold add nothing. Loads are unconditional with
-// out-of-matrix columns clamped and zeroed (as dia_row).
-template <int ND, typename T, typename XF>
-__device__ __forceinline__ T dia_row_seq(const DiaMat<T>& M, uint32_t n, uint32_t i, XF xf) {
+// out-of-matrix columns clamped and their products zero; a mirrored
+// diagonal's value is read from the upper one at the column's row.
+template <int ND, bool SYM, typename T, typename XF>
+__device__ __forceinline__ T dia_row_seq(const DiaCgArgs<T>& a, uint32_t i, XF xf) {
+    const uint32_t n = a.n;
     T av[ND], xv[ND];
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
-        const int64_t j = static_cast<int64_t>(i) + M.off[d];
+        const int64_t j = static_cast<int64_t>(i) + a.A.off[d];
         const bool in = j >= 0 && j < static_cast<int64_t>(n);
         const uint32_t jc = in ? static_cast<uint32_t>(j) : i;
-        av[d] = __ldg(M.vals + static_cast<size_t>(d) * n + i);
-        const T v = xf(jc);
-        xv[d] = in ? v : T(0);
+        T v;
+        if (SYM && a.A.off[d] < 0)
+            v = __ldg(a.A.vals + static_cast<size_t>(a.nd_real - 1 - d) * n + jc);
+        else
+            v = __ldg(a.A.vals + static_cast<size_t>(d) * n + i);
+        const T xj = xf(jc);
+        av[d] = in ? v : T(0);
+        xv[d] = in ? xj : T(0);
     }
     T s = T(0);
 #pragma unroll
@@ -651,11 +663,11 @@ __device__ __noinline__ T csr_row_lanes(const uint32_t* rp, const uint32_t* cols
 }
 
 // q_i = (A xf)_i in the reference's order for row i.
-template <int ND, typename T, typename XF>
+template <int ND, bool SYM, typename T, typename XF>
 __device__ __forceinline__ T cg_row(const DiaCgArgs<T>& a, uint32_t i, XF xf) {
     for (int k = 0; k < a.nlanes; ++k)
         if (i >= a.lanes[k].r0 && i < a.lanes[k].r1) return csr_row_lanes(a.rp, a.cols, a.vals, i, a.lanes[k].g, xf);
-    return dia_row_seq<ND>(a.A, a.n, i, xf);
+    return dia_row_seq<ND, SYM>(a, i, xf);
 }
 
 // The reference's CG (src/library/solvers/conjugate-gradients.hpp:73-226) as
@@ -670,7 +682,7 @@ __device__ __forceinline__ T cg_row(const DiaCgArgs<T>& a, uint32_t i, XF xf) {
 //      beta = <r,z>_new / <r,z>_old, res, nIters = k, stop test
 // The exchanges are bounded waits; a timeout leaves every CTA and sets
 // kStatusBarrierTimeout.
-template <typename T, int ND>
+template <typename T, int ND, bool SYM>
 __global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_cg_ref_kernel(DiaCgArgs<T> a) {
     __shared__ GridSmem gs;
     const FusedSync g = a.sync;
@@ -698,7 +710,7 @@ __global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_cg_ref_kernel(
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
         T* p0 = a.p[0];
         for_rows(n, [&](uint32_t i) {
-            const T y = cg_row<ND>(a, i, [&](uint32_t j) { return x[j]; });
+            const T y = cg_row<ND, SYM>(a, i, [&](uint32_t j) { return x[j]; });
             const T bi = __ldg(b + i);
             const T ri = add_rn(bi, -y);
             T zi = ri;
@@ -748,36 +760,39 @@ __global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_cg_ref_kernel(
             const T* pprev = a.p[(k + 1) & 1];
             // ---- A: p_k, q = A p_k, <q, p_k>
             double pq[1] = {0.0};
-            for_rows(n, [&](uint32_t i) {
-                T pi;
-                if (k == 0) {
-                    pi = pk[i];
-                } else {
-                    pi = add_rn(z[i], mul_rn(beta, pprev[i]));
+            if (k == 0) {
+                for_rows(n, [&](uint32_t i) {
+                    const T pi = pk[i];
+                    const T qi = cg_row<ND, SYM>(a, i, [&](uint32_t j) { return pk[j]; });
+                    q[i] = qi;
+                    pq[0] = add_rn(pq[0], mul_rn(static_cast<double>(qi), static_cast<double>(pi)));
+                });
+            } else {
+                auto pdir = [&](uint32_t j) { return add_rn(z[j], mul_rn(beta, pprev[j])); };
+                for_rows(n, [&](uint32_t i) {
+                    const T pi = pdir(i);
+                    const T qi = cg_row<ND, SYM>(a, i, pdir);
                     pk[i] = pi;
-                }
-                const T qi = k == 0 ? cg_row<ND>(a, i, [&](uint32_t j) { return pk[j]; })
-                                    : cg_row<ND>(a, i, [&](uint32_t j) { return add_rn(z[j], mul_rn(beta, pprev[j])); });
-                q[i] = qi;
-                pq[0] = add_rn(pq[0], mul_rn(static_cast<double>(qi), static_cast<double>(pi)));
-            });
+                    q[i] = qi;
+                    pq[0] = add_rn(pq[0], mul_rn(static_cast<double>(qi), static_cast<double>(pi)));
+                });
+            }
             double tq[1];
             if (!grid_exchange<1>(g, epoch, pq, tq, gs)) goto fail;
             const T yp = static_cast<T>(tq[0]);
             const T alpha = rz / yp;
             if (!(yp > T(0))) status |= kStatusCurvature;
-            // ---- B: x, r, z; <r,z>, ||r||
+            // ---- B: x += alpha p_k, r -= alpha q, z = M r; <r,z>, ||r||
             double acc[2] = {0.0, 0.0};
             for_rows(n, [&](uint32_t i) {
-                const T pi = pk[i];
-                x[i] = add_rn(x[i], mul_rn(alpha, pi));
+                // every load of the row before its first store (the vectors
+                // are not __restrict__, so a store would hold back later loads)
+                const T xi = add_rn(x[i], mul_rn(alpha, pk[i]));
                 const T ri = add_rn(r[i], -mul_rn(alpha, q[i]));
+                const T zi = invD != nullptr ? mul_rn(ri, invD[i]) : ri;
+                x[i] = xi;
                 r[i] = ri;
-                T zi = ri;
-                if (invD != nullptr) {
-                    zi = mul_rn(ri, invD[i]);
-                    z[i] = zi;
-                }
+                if (invD != nullptr) z[i] = zi;
                 acc[0] = add_rn(acc[0], mul_rn(static_cast<double>(ri), static_cast<double>(zi)));
                 acc[1] = add_rn(acc[1], term(ri));
             });
@@ -1035,10 +1050,66 @@ clsparseStatus dia_pcg_solve(DiaPcgArgs<VA, VG> a, bool learned, DiaWork& w, cls
 
 namespace {
 
-template <typename T, int ND>
+// flag |= 1 when A[i][i + off_l] (diagonal dl, off_l < 0) differs bitwise
+// from A[i + off_l][i] (diagonal du at -off_l) for a row i inside the matrix.
+template <typename T>
+__global__ void dia_sym_check_kernel(const T* __restrict__ vals, uint32_t n, int dl, int du, int32_t off_l,
+                                     int* flag) {
+    using U = std::conditional_t<sizeof(T) == 8, unsigned long long, unsigned int>;
+    bool bad = false;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int64_t j = static_cast<int64_t>(i) + off_l;
+        if (j < 0) continue;
+        const T lo = vals[static_cast<size_t>(dl) * n + i];
+        const T up = vals[static_cast<size_t>(du) * n + static_cast<size_t>(j)];
+        U bl, bu;
+        memcpy(&bl, &lo, sizeof(U));
+        memcpy(&bu, &up, sizeof(U));
+        bad |= bl != bu;
+    }
+    if (bad) atomicOr(flag, 1);
+}
+
+// Whether the drop-in CG runs its SYM form: A symmetric bit for bit with
+// symmetric offsets (off[d] = -off[nd - 1 - d]), at most 5 diagonals (the
+// form's register budget), and -- unless CLSPARSE_B200_DIA_SYM=1 asks for it
+// whenever A qualifies (=0: never) -- a working set (the diagonals and the
+// seven work vectors) above half of L2. Measured per iteration on B200: the
+// 1024^2 five-point FP64 matrix (96 MB) 30.0 -> 26.5 us; where the working
+// set stays in L2 the extra index arithmetic costs more than the bytes it
+// saves (512^2 FP64: 11.6 -> 12.0 us, 1024^2 FP32: 19.3 -> 21.9 us).
+template <typename T>
+clsparseStatus dia_symmetric(const DiaMat<T>& M, const DiaOffsets& offs, uint32_t n, int nd_pad, size_t l2_bytes,
+                             DiaWork& w, cudaStream_t s, bool& sym) {
+    sym = false;
+    const char* env = std::getenv("CLSPARSE_B200_DIA_SYM");
+    const int mode = env ? std::atoi(env) : -1;
+    if (mode == 0 || nd_pad > 5) return clsparseSuccess;
+    const size_t working = static_cast<size_t>(nd_pad + 7) * n * sizeof(T);
+    if (mode != 1 && (l2_bytes == 0 || 2 * working <= l2_bytes)) return clsparseSuccess;
+    const int nd = offs.nd;
+    for (int d = 0; d < nd; ++d)
+        if (offs.off[d] != -offs.off[nd - 1 - d]) return clsparseSuccess;
+    if (nd < 2) return clsparseSuccess;
+    int* flag = reinterpret_cast<int*>(static_cast<int32_t*>(w.table.ptr) + kSlots) + 1;
+    cudaMemsetAsync(flag, 0, sizeof(int), s);
+    const uint32_t grid = std::min<uint32_t>((n + 255) / 256, 1184);
+    for (int d = 0; offs.off[d] < 0; ++d)
+        dia_sym_check_kernel<T><<<grid, 256, 0, s>>>(M.vals, n, d, nd - 1 - d, offs.off[d], flag);
+    int h = 1;
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return clsparseInvalidKernelExecution;
+    sym = h == 0;
+    return clsparseSuccess;
+}
+
+template <typename T, int ND, bool SYM>
 cudaError_t dia_cg_launch(DiaCgArgs<T>& a, int sm_count, cudaStream_t s, uint32_t max_grid) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dia_cg_ref_kernel<T, ND>, kDiaThreads, 0) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dia_cg_ref_kernel<T, ND, SYM>, kDiaThreads, 0) !=
+        cudaSuccess) {
         cudaGetLastError();
         return cudaErrorInvalidConfiguration;
     }
@@ -1046,7 +1117,7 @@ cudaError_t dia_cg_launch(DiaCgArgs<T>& a, int sm_count, cudaStream_t s, uint32_
     const uint32_t grid = static_cast<uint32_t>(std::max(1, sm_count) * std::min(b, kDiaCtasPerSm));
     if (grid > max_grid) return cudaErrorInvalidConfiguration;
     void* args[] = {&a};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(dia_cg_ref_kernel<T, ND>), dim3(grid),
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(dia_cg_ref_kernel<T, ND, SYM>), dim3(grid),
                                        dim3(kDiaThreads), args, 0, s);
 }
 
@@ -1119,6 +1190,10 @@ clsparseStatus dia_cg_dropin(cldenseVector* xv, const clsparseCsrMatrix* A, cons
     a.vals = vals;
     for (int k = 0; k < nlanes; ++k) a.lanes[k] = lanes[k];
     a.nlanes = nlanes;
+    bool sym = false;
+    stt = dia_symmetric<T>(M, offs, n, ca, c->l2_bytes, w, s, sym);
+    if (stt != clsparseSuccess) return stt;
+    a.nd_real = offs.nd;
     a.d0 = main_diag_index(M);
     a.invD = jac ? vec(0) : nullptr;
     a.b = dev_ptr<const T>(bv->values, bv->off_values);
@@ -1151,11 +1226,16 @@ clsparseStatus dia_cg_dropin(cldenseVector* xv, const clsparseCsrMatrix* A, cons
 
     const int sms = c->sm_count;
     cudaError_t e = cudaErrorInvalidValue;
-    if (ca == 3) e = dia_cg_launch<T, 3>(a, sms, s, max_grid);
-    else if (ca == 5) e = dia_cg_launch<T, 5>(a, sms, s, max_grid);
-    else if (ca == 7) e = dia_cg_launch<T, 7>(a, sms, s, max_grid);
-    else if (ca == 9) e = dia_cg_launch<T, 9>(a, sms, s, max_grid);
-    else if (ca == kMaxDiags) e = dia_cg_launch<T, kMaxDiags>(a, sms, s, max_grid);
+    if (sym) {
+        if (ca == 3) e = dia_cg_launch<T, 3, true>(a, sms, s, max_grid);
+        else if (ca == 5) e = dia_cg_launch<T, 5, true>(a, sms, s, max_grid);
+    } else {
+        if (ca == 3) e = dia_cg_launch<T, 3, false>(a, sms, s, max_grid);
+        else if (ca == 5) e = dia_cg_launch<T, 5, false>(a, sms, s, max_grid);
+        else if (ca == 7) e = dia_cg_launch<T, 7, false>(a, sms, s, max_grid);
+        else if (ca == 9) e = dia_cg_launch<T, 9, false>(a, sms, s, max_grid);
+        else if (ca == kMaxDiags) e = dia_cg_launch<T, kMaxDiags, false>(a, sms, s, max_grid);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         return clsparseInvalidKernelExecution;

@@ -3,8 +3,10 @@ against the oracle restatement of the reference CG
 (src/library/solvers/conjugate-gradients.hpp:73-226).
 
 Parity bar as for the other loop modes: the same stop decision (iteration
-counts within a small slack -- the banded kernel sums a row in increasing
-column order and the dot products in another order than the reference),
+counts within a small slack -- the banded kernel forms each row in the
+reference's CSR-Adaptive order with separately rounded operations, but sums
+the dot products in another order), the reference-run pins exactly
+(tests/test_solver_ref_pin_gpu.py),
 the reported residuals agree, and x meets the stop criterion on a fresh FP64
 check. The reference's bookkeeping (maxIters, the previous nIters in the
 first stop test, x = b for a zero right-hand side, an exact initial guess)
@@ -52,6 +54,7 @@ PROBLEMS = {
     "poisson_rect": lambda: matgen.poisson2d(37, 91),
     "diffusion3d": lambda: matgen.diffusion3d_lognormal(16, sigma=1.0, seed=2),
     "banded9": lambda: banded9(6000),
+    "tridiag": lambda: tridiag(5000),
     "random_spd": lambda: matgen.random_spd(5000, seed=3),  # not banded: graph engine
 }
 
@@ -231,3 +234,46 @@ def test_banded_cg_barrier_timeout_is_reported_and_recovers(ctrl, orc, monkeypat
     _, oi = orc.solve("cg", np.float64, rp, col, val, np.zeros(n), b, L.DIAGONAL, 2000, 1e-10, 0.0)
     assert abs(info["nIters"] - oi.nIters) <= max(3, int(0.03 * oi.nIters))
     assert l1_residual(rp, col, val, x, b) <= 1e-9
+
+
+def tridiag(n: int, seed: int = 6):
+    rng = np.random.default_rng(seed)
+    w = -rng.uniform(0.5, 1.5, n - 1)
+    d = np.zeros(n)
+    d[:-1] -= w
+    d[1:] -= w
+    A = sp.diags([w, d + 0.01, w], [-1, 0, 1], format="csr")
+    A.sort_indices()
+    return A.indptr.astype(np.uint32), A.indices.astype(np.uint32), A.data.astype(np.float64)
+
+
+def convdiff5(m: int = 40):
+    """Five-point convection-diffusion: a banded matrix that is not symmetric."""
+    rp, col, val = matgen.poisson2d(m)
+    A = sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64)))
+    A = (A + 0.3 * sp.eye(A.shape[0], k=1) - 0.3 * sp.eye(A.shape[0], k=-1)).tocsr()
+    A.eliminate_zeros()
+    A.sort_indices()
+    return A.indptr.astype(np.uint32), A.indices.astype(np.uint32), A.data.astype(np.float64)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+@pytest.mark.parametrize("prob", ["poisson64", "tridiag", "convdiff5", "diffusion3d"])
+def test_banded_cg_symmetric_form_is_bitwise_equal(ctrl, monkeypatch, prob, dtype):
+    """The form that reads a symmetric matrix's lower diagonals from the upper
+    ones (forced on; by default it runs only when the working set exceeds half
+    of L2) gives the same x bit for bit; a non-symmetric matrix, or one with
+    more diagonals than the form takes, runs the plain form."""
+    rp, col, val = {"poisson64": lambda: matgen.poisson2d(64), "tridiag": lambda: tridiag(5000),
+                    "convdiff5": convdiff5,
+                    "diffusion3d": lambda: matgen.diffusion3d_lognormal(16, sigma=1.0, seed=2)}[prob]()
+    n = len(rp) - 1
+    b = np.random.default_rng(9).uniform(-1, 1, n)
+    rel = 1e-10 if dtype == torch.float64 else 1e-5
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("CLSPARSE_B200_DIA_SYM", mode)
+        out[mode] = run(ctrl, rp, col, val, np.zeros(n), b, dtype, L.DIAGONAL, 60 if prob == "convdiff5" else 5000,
+                        rel, 0.0)
+    assert out["0"][1] == out["1"][1]
+    np.testing.assert_array_equal(out["0"][0], out["1"][0])
