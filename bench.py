@@ -202,6 +202,32 @@ def cg_profile(iters: int):
     ctrl.release()
 
 
+def dia_cg_profile(iters: int):
+    """Two FP64 Jacobi-CG calls of ITERS iterations on the C5 matrix through
+    the banded drop-in engine (solver loop mode 3): per call the offset
+    detection, the diagonal-layout fill, the symmetry check and one launch
+    of the cooperative CG kernel."""
+    import torch
+    from clsparse_b200 import _lib as L
+    from clsparse_b200 import api, matgen
+    api.setup()
+    ctrl = api.Control()
+    ctrl.set_solver_loop_mode(3)
+    A = api.CsrMatrix.from_numpy(*matgen.diffusion2d_grf(1024, corr_len=0.05, sigma=2.0, seed=1005))
+    A.create_meta(ctrl)
+    n = A.num_rows
+    b = torch.tensor(np.random.default_rng(1).uniform(-1, 1, n), device="cuda")
+    for _ in range(2):
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        sc = api.SolverControl(L.DIAGONAL, iters, 0.0, 0.0)
+        sc.set_norm(2)
+        info = api.solve("cg", x, A, b, sc, ctrl)
+        sc.release()
+    torch.cuda.synchronize()
+    print(json.dumps({"dia_cg_profile_iterations": info["nIters"]}), flush=True)
+    ctrl.release()
+
+
 def gnn_profile(builds: int):
     """BF16 factor builds of the learned preconditioner on the C5 matrix
     (1,048,576 rows): the network's forward pass with its dense layers on the
@@ -828,8 +854,14 @@ def main():
     ap.add_argument("--cg-profile", type=int, default=0, metavar="ITERS",
                     help="only run ITERS iterations of FP64 Jacobi-CG on the C5 matrix with directly launched "
                          "kernels (for a profiler's launch list), then exit")
+    ap.add_argument("--dia-cg-profile", type=int, default=0, metavar="ITERS",
+                    help="only run two FP64 Jacobi-CG calls of ITERS iterations on the C5 matrix through the "
+                         "banded drop-in engine (loop mode 3), then exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.dia_cg_profile:
+        dia_cg_profile(args.dia_cg_profile)
+        return
     if args.gnn_profile:
         gnn_profile(args.gnn_profile)
         return
