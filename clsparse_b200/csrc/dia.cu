@@ -423,8 +423,11 @@ __global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_pcg_kernel(Dia
                     const float ti = dia_row<NDG>(a.G, n, i, rnew);
                     ts[i - r0] = ti;
                     if (i < r1) {
-                        x[i] = fmaf(alpha, P[i], x[i]);
+                        // the row's loads before its stores (x, r, q are not
+                        // __restrict__: a store would hold back later loads)
+                        const float xn = fmaf(alpha, P[i], x[i]);
                         const float rn = fmaf(-alpha, q[i], Rc[i]);
+                        x[i] = xn;
                         Rn[i] = rn;
                         acc2[0] += static_cast<double>(rn) * rn;
                         acc2[1] += static_cast<double>(ti) * ti;
