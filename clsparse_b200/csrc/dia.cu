@@ -43,12 +43,20 @@
 // r = b and keeps the previous solve's last direction:
 // p = z + (<r,z> / rz_prev) p_prev.
 //
+// Drop-in solves (solver loop mode 3): clsparse{S,D}csrcg and
+// clsparse{S,D}csrbicgStab on a banded matrix run as one cooperative launch
+// over a diagonal-storage copy in the solve's own type, in the reference's
+// arithmetic (rows in its CSR-Adaptive order, separately rounded operations),
+// with its stop tests and solver-control bookkeeping (dia_cg_ref_kernel,
+// dia_bicg_ref_kernel below).
+//
 // Safety: every barrier wait is bounded (grid_sync.cuh); a timeout leaves
 // the kernel through every CTA and is reported as the barrier-timeout status.
 #include <algorithm>
 #include <climits>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <type_traits>
 #include <vector>
 
@@ -582,6 +590,7 @@ constexpr int kMaxLaneRanges = 8;
 
 template <typename T>
 struct DiaCgArgs {
+    using value_type = T;
     DiaMat<T> A;
     // CSR arrays of A, for the rows of lane ranges
     const uint32_t* rp;
@@ -620,8 +629,9 @@ using dev::mul_rn;
 // CSR row does not hold add nothing. Loads are unconditional with
 // out-of-matrix columns clamped and their products zero; a mirrored
 // diagonal's value is read from the upper one at the column's row.
-template <int ND, bool SYM, typename T, typename XF>
-__device__ __forceinline__ T dia_row_seq(const DiaCgArgs<T>& a, uint32_t i, XF xf) {
+template <int ND, bool SYM, typename Args, typename XF>
+__device__ __forceinline__ typename Args::value_type dia_row_seq(const Args& a, uint32_t i, XF xf) {
+    using T = typename Args::value_type;
     const uint32_t n = a.n;
     T av[ND], xv[ND];
 #pragma unroll
@@ -666,8 +676,8 @@ __device__ __noinline__ T csr_row_lanes(const uint32_t* rp, const uint32_t* cols
 }
 
 // q_i = (A xf)_i in the reference's order for row i.
-template <int ND, bool SYM, typename T, typename XF>
-__device__ __forceinline__ T cg_row(const DiaCgArgs<T>& a, uint32_t i, XF xf) {
+template <int ND, bool SYM, typename Args, typename XF>
+__device__ __forceinline__ typename Args::value_type cg_row(const Args& a, uint32_t i, XF xf) {
     for (int k = 0; k < a.nlanes; ++k)
         if (i >= a.lanes[k].r0 && i < a.lanes[k].r1) return csr_row_lanes(a.rp, a.cols, a.vals, i, a.lanes[k].g, xf);
     return dia_row_seq<ND, SYM>(a, i, xf);
@@ -809,6 +819,242 @@ __global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_cg_ref_kernel(
             cur_res = static_cast<double>(res);
             if (!isfinite(cur_res)) status |= kStatusNonFinite;
             done = finished(cur_res, n_iters);
+        }
+        if (lead) {
+            a.st->n_iters = n_iters;
+            a.st->init_res = init_res;
+            a.st->cur_res = cur_res;
+            atomicOr(&a.st->status, status);
+        }
+        return;
+    }
+fail:
+    if (threadIdx.x == 0) atomicOr(&a.st->status, kStatusBarrierTimeout);
+}
+
+// ---- the drop-in BiCGStab (clsparse{S,D}csrbicgStab, solver loop mode 3)
+
+template <typename T>
+struct DiaBicgArgs {
+    using value_type = T;
+    DiaMat<T> A;
+    const uint32_t* rp;
+    const uint32_t* cols;
+    const T* vals;
+    LaneRange lanes[kMaxLaneRanges];
+    int nlanes;
+    int nd_real;
+    int d0;
+    T* invD;        // Jacobi: 1 / a_ii, formed in the prologue; nullptr: no preconditioner
+    const T* b;
+    T* x;
+    T* r;
+    T* rs;          // r*
+    T* p[2];        // direction of iteration k in p[k & 1]
+    T* AMp[2];      // A M p_k in AMp[k & 1]
+    T* Mp;          // M p_k (== p_k without preconditioner)
+    T* s;
+    T* Ms;          // M s (== s without preconditioner)
+    T* AMs;
+    uint32_t n;
+    FusedSync sync;
+    DiaCgState* st;
+};
+
+// The reference's BiCGStab (src/library/solvers/biconjugate-gradients-
+// stabilized.hpp:61-266) as one cooperative launch, in the arithmetic and row
+// order of the drop-in CG above. Per iteration k:
+//   1: p_k = (r + beta p_{k-1}) - (beta omega) AMp_{k-1}, Mp = M p_k (a
+//      neighbour's M p_k formed on the fly), AMp_k = A Mp, <r*, AMp_k>
+//                                                         -> exchange: alpha
+//   2: s = r - alpha AMp_k, Ms = M s (a neighbour's formed on the fly),
+//      AMs = A Ms; ||s||, <AMs, s>, <AMs, AMs>           -> exchange: the
+//      stop test on s (then x += alpha Mp and stop), omega
+//   3: x = (x + alpha Mp) + omega Ms, r = s - omega AMs; ||r||, <r*, r>
+//                                       -> exchange: stop test, beta
+// The reference tests ||s|| before forming A M s; here A M s is formed in the
+// same pass and dropped when the test stops the solve. The stop tests of the
+// first iteration see the nIters the control held before the solve.
+template <typename T, int ND, bool SYM>
+__global__ void __launch_bounds__(kDiaThreads, kDiaCtasPerSm) dia_bicg_ref_kernel(DiaBicgArgs<T> a) {
+    __shared__ GridSmem gs;
+    const FusedSync g = a.sync;
+    unsigned long long epoch = 0;
+    const uint32_t n = a.n;
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    T* x = a.x;
+    T* r = a.r;
+    T* rs = a.rs;
+    T* s = a.s;
+    T* Ms = a.Ms;
+    T* AMs = a.AMs;
+    T* Mp = a.Mp;
+    T* invD = a.invD;
+    const T* b = a.b;
+    const DiaCgState in = *a.st;
+    const int l2 = in.l2;
+    auto term = [l2](T v) {
+        const double d = static_cast<double>(v);
+        return l2 ? mul_rn(d, d) : fabs(d);
+    };
+    auto finish_norm = [l2](double v) { return l2 ? sqrt(v) : v; };
+    auto dot = [](T u, T v) { return mul_rn(static_cast<double>(u), static_cast<double>(v)); };
+    auto apply_m = [invD](T v, uint32_t j) { return invD != nullptr ? mul_rn(v, invD[j]) : v; };
+
+    // ---- prologue: r = b - A x, r* = r, p = r, Mp = M p
+    double tot0[4];
+    {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        T* p0 = a.p[0];
+        for_rows(n, [&](uint32_t i) {
+            const T y = cg_row<ND, SYM>(a, i, [&](uint32_t j) { return x[j]; });
+            const T bi = __ldg(b + i);
+            const T ri = add_rn(bi, -y);
+            T mi = ri;
+            if (invD != nullptr) {
+                const T d = __ldg(a.A.vals + static_cast<size_t>(a.d0) * n + i);
+                const T inv = T(1) / d;
+                invD[i] = inv;
+                mi = mul_rn(ri, inv);
+                acc[3] += d == T(0) ? 1.0 : 0.0;
+                Mp[i] = mi;
+            }
+            r[i] = ri;
+            rs[i] = ri;
+            p0[i] = ri;
+            acc[0] = add_rn(acc[0], term(bi));
+            acc[1] = add_rn(acc[1], term(ri));
+            acc[2] = add_rn(acc[2], dot(ri, ri));
+        });
+        if (!grid_exchange<4>(g, epoch, acc, tot0, gs)) goto fail;
+    }
+    if (tot0[3] > 0.0) {
+        if (lead) a.st->zero_diag = 1;
+        return;
+    }
+    {
+        const T norm_b = static_cast<T>(finish_norm(tot0[0]));
+        if (norm_b <= std::numeric_limits<T>::min()) {
+            for_rows(n, [&](uint32_t i) { x[i] = __ldg(b + i); });
+            if (lead) {
+                a.st->zero_b = 1;
+                a.st->n_iters = 0;
+            }
+            return;
+        }
+        const double init_res = static_cast<double>(static_cast<T>(finish_norm(tot0[1])) / norm_b);
+        auto finished = [&](double res, int n_iters) {
+            return res <= in.rel_tol || res <= in.abs_tol * init_res || n_iters >= in.max_iters ||
+                   (in.stop_nonfinite && !isfinite(res));
+        };
+        T rsr_old = static_cast<T>(tot0[2]);
+        T beta = T(0), omega = T(0);
+        double cur_res = init_res;
+        int n_iters = in.n_iters_in, status = 0;
+        bool done = finished(init_res, n_iters);
+        if (done) n_iters = 0;
+        for (int k = 0; !done; ++k) {
+            T* pk = a.p[k & 1];
+            const T* pprev = a.p[(k + 1) & 1];
+            T* amp = a.AMp[k & 1];
+            const T* amp_prev = a.AMp[(k + 1) & 1];
+            // with no preconditioner M p_k is p_k itself
+            T* mp = invD != nullptr ? Mp : pk;
+            // ---- 1: p_k, M p_k, AMp_k = A M p_k, <r*, AMp_k>
+            double acc1[1] = {0.0};
+            {
+                const T bw = mul_rn(beta, omega);
+                auto pdir = [&](uint32_t j) {
+                    return add_rn(add_rn(r[j], mul_rn(beta, pprev[j])), -mul_rn(bw, amp_prev[j]));
+                };
+                if (k == 0) {
+                    for_rows(n, [&](uint32_t i) {
+                        const T ai = cg_row<ND, SYM>(a, i, [&](uint32_t j) { return mp[j]; });
+                        const T rsi = rs[i];
+                        amp[i] = ai;
+                        acc1[0] = add_rn(acc1[0], dot(ai, rsi));
+                    });
+                } else {
+                    for_rows(n, [&](uint32_t i) {
+                        const T pi = pdir(i);
+                        const T mi = apply_m(pi, i);
+                        const T ai = cg_row<ND, SYM>(a, i, [&](uint32_t j) { return apply_m(pdir(j), j); });
+                        const T rsi = rs[i];
+                        pk[i] = pi;
+                        if (invD != nullptr) Mp[i] = mi;
+                        amp[i] = ai;
+                        acc1[0] = add_rn(acc1[0], dot(ai, rsi));
+                    });
+                }
+            }
+            double t1[1];
+            if (!grid_exchange<1>(g, epoch, acc1, t1, gs)) goto fail;
+            const T rs_amp = static_cast<T>(t1[0]);
+            const T alpha = rsr_old / rs_amp;
+            if (rs_amp == T(0)) status |= kStatusBicgBreakdown;
+            // ---- 2: s, M s, AMs = A M s; ||s||, <AMs, s>, <AMs, AMs>
+            double acc2[3] = {0.0, 0.0, 0.0};
+            {
+                auto sdir = [&](uint32_t j) { return add_rn(r[j], -mul_rn(alpha, amp[j])); };
+                for_rows(n, [&](uint32_t i) {
+                    const T si = sdir(i);
+                    const T msi = apply_m(si, i);
+                    const T ai = cg_row<ND, SYM>(a, i, [&](uint32_t j) { return apply_m(sdir(j), j); });
+                    s[i] = si;
+                    if (invD != nullptr) Ms[i] = msi;
+                    AMs[i] = ai;
+                    acc2[0] = add_rn(acc2[0], term(si));
+                    acc2[1] = add_rn(acc2[1], dot(ai, si));
+                    acc2[2] = add_rn(acc2[2], dot(ai, ai));
+                });
+            }
+            double t2[3];
+            if (!grid_exchange<3>(g, epoch, acc2, t2, gs)) goto fail;
+            {
+                const T res_s = static_cast<T>(finish_norm(t2[0])) / norm_b;
+                cur_res = static_cast<double>(res_s);
+                if (!isfinite(cur_res)) status |= kStatusNonFinite;
+                if (finished(cur_res, n_iters)) {
+                    // biconjugate-gradients-stabilized.hpp:183-195: x += alpha M p
+                    for_rows(n, [&](uint32_t i) { x[i] = add_rn(x[i], mul_rn(alpha, mp[i])); });
+                    n_iters = k;
+                    break;
+                }
+            }
+            const T amss = static_cast<T>(t2[1]);
+            const T amsams = static_cast<T>(t2[2]);
+            omega = amss / amsams;
+            if (omega == T(0)) status |= kStatusBicgBreakdown;
+            // ---- 3: x, r; ||r||, <r*, r>
+            double acc3[2] = {0.0, 0.0};
+            {
+                const T* msv = invD != nullptr ? Ms : s;
+                for_rows(n, [&](uint32_t i) {
+                    const T x1 = add_rn(x[i], mul_rn(alpha, mp[i]));
+                    const T xi = add_rn(x1, mul_rn(omega, msv[i]));
+                    const T ri = add_rn(s[i], -mul_rn(omega, AMs[i]));
+                    const T rsi = rs[i];
+                    x[i] = xi;
+                    r[i] = ri;
+                    acc3[0] = add_rn(acc3[0], term(ri));
+                    acc3[1] = add_rn(acc3[1], dot(rsi, ri));
+                });
+            }
+            double t3[2];
+            if (!grid_exchange<2>(g, epoch, acc3, t3, gs)) goto fail;
+            const T res = static_cast<T>(finish_norm(t3[0])) / norm_b;
+            cur_res = static_cast<double>(res);
+            if (!isfinite(cur_res)) status |= kStatusNonFinite;
+            if (finished(cur_res, n_iters)) {
+                n_iters = k;
+                break;
+            }
+            const T rsr_new = static_cast<T>(t3[1]);
+            beta = rsr_new / rsr_old;
+            beta = beta * alpha;
+            beta = beta / omega;
+            rsr_old = rsr_new;
+            n_iters = k + 1;
         }
         if (lead) {
             a.st->n_iters = n_iters;
@@ -1108,11 +1354,21 @@ clsparseStatus dia_symmetric(const DiaMat<T>& M, const DiaOffsets& offs, uint32_
     return clsparseSuccess;
 }
 
+// The cooperative kernel of a drop-in solve for an argument block.
 template <typename T, int ND, bool SYM>
-cudaError_t dia_cg_launch(DiaCgArgs<T>& a, int sm_count, cudaStream_t s, uint32_t max_grid) {
+const void* dropin_kernel(const DiaCgArgs<T>*) {
+    return reinterpret_cast<const void*>(dia_cg_ref_kernel<T, ND, SYM>);
+}
+template <typename T, int ND, bool SYM>
+const void* dropin_kernel(const DiaBicgArgs<T>*) {
+    return reinterpret_cast<const void*>(dia_bicg_ref_kernel<T, ND, SYM>);
+}
+
+template <typename T, int ND, bool SYM, typename Args>
+cudaError_t dropin_launch(Args& a, int sm_count, cudaStream_t s, uint32_t max_grid) {
+    const void* k = dropin_kernel<T, ND, SYM>(&a);
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dia_cg_ref_kernel<T, ND, SYM>, kDiaThreads, 0) !=
-        cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kDiaThreads, 0) != cudaSuccess) {
         cudaGetLastError();
         return cudaErrorInvalidConfiguration;
     }
@@ -1120,20 +1376,20 @@ cudaError_t dia_cg_launch(DiaCgArgs<T>& a, int sm_count, cudaStream_t s, uint32_
     const uint32_t grid = static_cast<uint32_t>(std::max(1, sm_count) * std::min(b, kDiaCtasPerSm));
     if (grid > max_grid) return cudaErrorInvalidConfiguration;
     void* args[] = {&a};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(dia_cg_ref_kernel<T, ND, SYM>), dim3(grid),
-                                       dim3(kDiaThreads), args, 0, s);
+    return cudaLaunchCooperativeKernel(k, dim3(grid), dim3(kDiaThreads), args, 0, s);
 }
 
-}  // namespace
-
-template <typename T>
-clsparseStatus dia_cg_dropin(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
-                             clSParseSolverControl sc, clsparseControl c) {
+// The drop-in solves (clsparse{S,D}csrcg with BICG false, clsparse{S,D}csrbicgStab
+// with BICG true) on the banded engine.
+template <typename T, bool BICG>
+clsparseStatus dia_dropin(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
+                          clSParseSolverControl sc, clsparseControl c) {
+    using Args = std::conditional_t<BICG, DiaBicgArgs<T>, DiaCgArgs<T>>;
     const uint32_t n = static_cast<uint32_t>(A->num_rows);
     const uint32_t nnz = static_cast<uint32_t>(A->num_nonzeros);
     if (n == 0 || nnz == 0) return clsparseNotImplemented;
-    // The reference's CG multiplies with csrmv_adaptive when the matrix has a
-    // meta (csrmv_general otherwise: the graph engine runs that order). Its
+    // The reference's solvers multiply with csrmv_adaptive when the matrix has
+    // a meta (csrmv_general otherwise: the graph engine runs that order). Its
     // STREAM blocks reduce a row on one lane except in a few blocks (the last
     // one, with few rows): those row ranges are taken over as CSR rows with
     // their lane count. A block of another kind, or more such ranges than
@@ -1172,41 +1428,65 @@ clsparseStatus dia_cg_dropin(cldenseVector* xv, const clsparseCsrMatrix* A, cons
     bool has_main = false;
     for (int d = 0; d < offs.nd; ++d) has_main |= offs.off[d] == 0;
     if (ca == 0 || (jac && !has_main)) return clsparseNotImplemented;
+    // BiCGStab forms a neighbour's M p and M s from three to four vectors
+    // each: it pays while the diagonals and the eleven work vectors stay in
+    // L2. Measured per iteration on B200 against the graph engine (FP64):
+    // 512^2 five-point (33 MB) 25.0 vs 34.0 us; 1024^2 five-point (134 MB)
+    // 82.6 vs 81.6; 128^3 seven-point (288 MB) 191 vs 161. Larger systems
+    // run the graph engine.
+    if (BICG && static_cast<size_t>(ca + 11) * n * sizeof(T) > c->l2_bytes) return clsparseNotImplemented;
     DiaMat<T> M;
     stt = dia_build<T, T>(rp, cols, vals, n, offs, ca, w.A, s, M);
     if (stt != clsparseSuccess) return stt;
+    bool sym = false;
+    if (!BICG) {
+        stt = dia_symmetric<T>(M, offs, n, ca, c->l2_bytes, w, s, sym);
+        if (stt != clsparseSuccess) return stt;
+    }
 
-    // work vectors: invD, r, p[0], p[1], q, z
+    // work vectors -- CG: invD, r, p[0], p[1], q, z; BiCGStab: invD, r, r*,
+    // p[0], p[1], AMp[0], AMp[1], Mp, s, Ms, AMs
+    const int nvec = BICG ? 11 : 6;
     const size_t vb = align256(static_cast<size_t>(n) * sizeof(T));
     const uint32_t max_grid = static_cast<uint32_t>(std::max(1, c->sm_count) * kDiaCtasPerSm);
     const size_t sync_b = align256(fused_sync_bytes(max_grid));
-    if (w.vecs.ensure(6 * vb) != cudaSuccess || w.sync.ensure(sync_b + align256(sizeof(DiaCgState))) != cudaSuccess) {
+    if (w.vecs.ensure(nvec * vb) != cudaSuccess ||
+        w.sync.ensure(sync_b + align256(sizeof(DiaCgState))) != cudaSuccess) {
         cudaGetLastError();
         return clsparseOutOfResources;
     }
     char* vbase = static_cast<char*>(w.vecs.ptr);
     auto vec = [&](int k) { return reinterpret_cast<T*>(vbase + static_cast<size_t>(k) * vb); };
-    DiaCgArgs<T> a{};
+    Args a{};
     a.A = M;
     a.rp = rp;
     a.cols = cols;
     a.vals = vals;
     for (int k = 0; k < nlanes; ++k) a.lanes[k] = lanes[k];
     a.nlanes = nlanes;
-    bool sym = false;
-    stt = dia_symmetric<T>(M, offs, n, ca, c->l2_bytes, w, s, sym);
-    if (stt != clsparseSuccess) return stt;
     a.nd_real = offs.nd;
     a.d0 = main_diag_index(M);
     a.invD = jac ? vec(0) : nullptr;
     a.b = dev_ptr<const T>(bv->values, bv->off_values);
     a.x = dev_ptr<T>(xv->values, xv->off_values);
     a.r = vec(1);
-    a.p[0] = vec(2);
-    a.p[1] = vec(3);
-    a.q = vec(4);
-    a.z = jac ? vec(5) : a.r;
     a.n = n;
+    if constexpr (BICG) {
+        a.rs = vec(2);
+        a.p[0] = vec(3);
+        a.p[1] = vec(4);
+        a.AMp[0] = vec(5);
+        a.AMp[1] = vec(6);
+        a.Mp = vec(7);
+        a.s = vec(8);
+        a.Ms = jac ? vec(9) : a.s;
+        a.AMs = vec(10);
+    } else {
+        a.p[0] = vec(2);
+        a.p[1] = vec(3);
+        a.q = vec(4);
+        a.z = jac ? vec(5) : a.r;
+    }
 
     char* base = static_cast<char*>(w.sync.ptr);
     DiaCgState h;
@@ -1230,14 +1510,16 @@ clsparseStatus dia_cg_dropin(cldenseVector* xv, const clsparseCsrMatrix* A, cons
     const int sms = c->sm_count;
     cudaError_t e = cudaErrorInvalidValue;
     if (sym) {
-        if (ca == 3) e = dia_cg_launch<T, 3, true>(a, sms, s, max_grid);
-        else if (ca == 5) e = dia_cg_launch<T, 5, true>(a, sms, s, max_grid);
+        if constexpr (!BICG) {
+            if (ca == 3) e = dropin_launch<T, 3, true>(a, sms, s, max_grid);
+            else if (ca == 5) e = dropin_launch<T, 5, true>(a, sms, s, max_grid);
+        }
     } else {
-        if (ca == 3) e = dia_cg_launch<T, 3, false>(a, sms, s, max_grid);
-        else if (ca == 5) e = dia_cg_launch<T, 5, false>(a, sms, s, max_grid);
-        else if (ca == 7) e = dia_cg_launch<T, 7, false>(a, sms, s, max_grid);
-        else if (ca == 9) e = dia_cg_launch<T, 9, false>(a, sms, s, max_grid);
-        else if (ca == kMaxDiags) e = dia_cg_launch<T, kMaxDiags, false>(a, sms, s, max_grid);
+        if (ca == 3) e = dropin_launch<T, 3, false>(a, sms, s, max_grid);
+        else if (ca == 5) e = dropin_launch<T, 5, false>(a, sms, s, max_grid);
+        else if (ca == 7) e = dropin_launch<T, 7, false>(a, sms, s, max_grid);
+        else if (ca == 9) e = dropin_launch<T, 9, false>(a, sms, s, max_grid);
+        else if (ca == kMaxDiags) e = dropin_launch<T, kMaxDiags, false>(a, sms, s, max_grid);
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -1252,7 +1534,8 @@ clsparseStatus dia_cg_dropin(cldenseVector* xv, const clsparseCsrMatrix* A, cons
     if (h.status & kStatusBarrierTimeout) return clsparseInvalidKernelExecution;
     if (h.zero_diag) return clsparseNotImplemented;  // x untouched; the graph engine reports the zero
     if (h.zero_b) {
-        // conjugate-gradients.hpp:87-95 resets the tolerances of the control
+        // conjugate-gradients.hpp:87-95 (biconjugate-gradients-stabilized.hpp
+        // alike) resets the tolerances of the control
         sc->nIters = 0;
         sc->absoluteTolerance = 0.0;
         sc->relativeTolerance = 0.0;
@@ -1264,10 +1547,28 @@ clsparseStatus dia_cg_dropin(cldenseVector* xv, const clsparseCsrMatrix* A, cons
     return clsparseSuccess;
 }
 
+}  // namespace
+
+template <typename T>
+clsparseStatus dia_cg_dropin(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
+                             clSParseSolverControl sc, clsparseControl c) {
+    return dia_dropin<T, false>(xv, A, bv, sc, c);
+}
+
+template <typename T>
+clsparseStatus dia_bicg_dropin(cldenseVector* xv, const clsparseCsrMatrix* A, const cldenseVector* bv,
+                               clSParseSolverControl sc, clsparseControl c) {
+    return dia_dropin<T, true>(xv, A, bv, sc, c);
+}
+
 template clsparseStatus dia_cg_dropin<float>(cldenseVector*, const clsparseCsrMatrix*, const cldenseVector*,
                                              clSParseSolverControl, clsparseControl);
 template clsparseStatus dia_cg_dropin<double>(cldenseVector*, const clsparseCsrMatrix*, const cldenseVector*,
                                               clSParseSolverControl, clsparseControl);
+template clsparseStatus dia_bicg_dropin<float>(cldenseVector*, const clsparseCsrMatrix*, const cldenseVector*,
+                                               clSParseSolverControl, clsparseControl);
+template clsparseStatus dia_bicg_dropin<double>(cldenseVector*, const clsparseCsrMatrix*, const cldenseVector*,
+                                                clSParseSolverControl, clsparseControl);
 
 #define CLSP_DIA_INST(VA, VG)                                                                                 \
     template clsparseStatus dia_pcg_solve<VA, VG>(DiaPcgArgs<VA, VG>, bool, DiaWork&, clsparseControl,       \

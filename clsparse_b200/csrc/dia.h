@@ -1,5 +1,6 @@
-// Banded (diagonal-storage) inner solves of the mixed-precision refinement:
-// types shared by dia.cu and mixed.cu. See dia.cu for the storage and the
+// Banded (diagonal-storage) solves -- the inner solves of the mixed-precision
+// refinement and the drop-in CG / BiCGStab of solver loop mode 3: types shared
+// by dia.cu, mixed.cu and solvers.cu. See dia.cu for the storage and the
 // engine.
 #pragma once
 
@@ -80,6 +81,12 @@ bool dia_enabled();
 template <typename T>
 clsparseStatus dia_cg_dropin(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
                              clSParseSolverControl sc, clsparseControl c);
+
+// The drop-in clsparse{S,D}csrbicgStab on the banded engine (solver loop
+// mode 3), with the same rules and fallback as dia_cg_dropin.
+template <typename T>
+clsparseStatus dia_bicg_dropin(cldenseVector* x, const clsparseCsrMatrix* A, const cldenseVector* b,
+                               clSParseSolverControl sc, clsparseControl c);
 
 // The distinct column offsets of a CSR matrix when there are at most
 // kMaxDiags and they hold at least half of the stored diagonal entries

@@ -957,6 +957,15 @@ clsparseStatus bicg_solve(cldenseVector* xv, const clsparseCsrMatrix* A, const c
     if (stt != clsparseSuccess) return stt;
     DeviceGuard guard(c->device);
     const size_t n = A->num_rows;
+    // loop mode 3 on a banded matrix: one cooperative launch (see cg_solve)
+    if (c->solver_loop_mode == 3 && std::is_same_v<V, T> && n > 0 && !c->extended_precision &&
+        sc->history == nullptr && dia_enabled()) {
+        stt = dia_bicg_dropin<T>(xv, A, bv, sc, c);
+        if (stt != clsparseNotImplemented) {
+            sc->printSummary(stt);
+            return stt;
+        }
+    }
     if (!c->solver_cache) c->solver_cache = std::make_unique<SolverCache>();
     SolverCache& cache = *c->solver_cache;
     const CsrView<V> Av = view_of<V>(A);

@@ -241,13 +241,15 @@ cldenseDdotNoAlloc(clsparseScalar* r, const cldenseVector* x, const cldenseVecto
  * iterates as 0); 2 = CG and factorized PCG as ONE persistent cooperative
  * kernel per solve (grid-wide exchanges between phases; needs a
  * CSR-Adaptive meta, otherwise and for BiCGStab the solve runs as in 0;
- * iterates equal up to reduction order); 3 = clsparse{S,D}csrcg on a banded
- * matrix (at most 16 distinct column offsets j - i, columns strictly
- * increasing per row) as ONE cooperative kernel over a private copy of A
- * stored by diagonal, rebuilt at every call (same stop test, nIters and
- * solver-control bookkeeping; iterates equal up to summation order); other
- * matrices, a zero or missing diagonal under Jacobi, residual history or
- * snapshots and extended precision run as in 0. */
+ * iterates equal up to reduction order); 3 = clsparse{S,D}csrcg and
+ * clsparse{S,D}csrbicgStab on a banded matrix with a CSR-Adaptive meta (at
+ * most 16 distinct column offsets j - i, columns strictly increasing per row)
+ * as ONE cooperative kernel over a private copy of A stored by diagonal,
+ * rebuilt at every call (the reference's row order and rounding, stop tests,
+ * nIters and solver-control bookkeeping; iterates equal up to the order of
+ * the dot-product sums); matrices without a meta or not banded, a zero or
+ * missing diagonal under Jacobi, residual history or snapshots, extended
+ * precision, and BiCGStab systems larger than L2 run as in 0. */
 CLSPARSE_EXPORT clsparseStatus
 clsparseB200SetSolverLoopMode(clsparseControl control, cl_int mode);
 

@@ -57,9 +57,16 @@ def reference(d, run):
 # (observed up to 1.5e-7 on the unpreconditioned lognormal diffusion
 # matrix), 1e-2 in FP32 (the reference test's own relative tolerance;
 # observed up to 2.1e-3).
-def iter_slack(method, t, n_ref):
+# The banded loop mode's BiCGStab sums its dot products in yet another order
+# and crosses the tolerance of that irregular history up to 3 iterations
+# from the reference's run (poisson20 tight FP64 Jacobi, adaptive: 47
+# against 44; the reference's own general-path run takes 46): its bar is
+# max(3, 7%). Its CG keeps the exact bar.
+def iter_slack(method, t, n_ref, banded=False):
     if method == "cg":
         return 0 if t == "d" else 1
+    if banded:
+        return max(3, int(0.07 * n_ref))
     return max(2, int(0.05 * n_ref))
 
 

@@ -1,6 +1,7 @@
-"""The drop-in clsparse{S,D}csrcg on the banded engine (solver loop mode 3)
-against the oracle restatement of the reference CG
-(src/library/solvers/conjugate-gradients.hpp:73-226).
+"""The drop-in clsparse{S,D}csrcg and clsparse{S,D}csrbicgStab on the banded
+engine (solver loop mode 3) against the oracle restatements of the
+reference CG and BiCGStab (src/library/solvers/conjugate-gradients.hpp:73-226,
+biconjugate-gradients-stabilized.hpp:61-266).
 
 Parity bar as for the other loop modes: the same stop decision (iteration
 counts within a small slack -- the banded kernel forms each row in the
@@ -59,7 +60,7 @@ PROBLEMS = {
 }
 
 
-def run(ctrl, rp, col, val, x0, b, dtype, precond, max_iters, rel, abs_, loop_mode=3, sc=None, norm=0):
+def run(ctrl, rp, col, val, x0, b, dtype, precond, max_iters, rel, abs_, loop_mode=3, sc=None, norm=0, kind="cg"):
     ctrl.set_solver_loop_mode(loop_mode)
     A = api.CsrMatrix.from_numpy(rp, col, val, dtype=dtype)
     A.create_meta(ctrl)
@@ -70,7 +71,7 @@ def run(ctrl, rp, col, val, x0, b, dtype, precond, max_iters, rel, abs_, loop_mo
         sc = api.SolverControl(precond, max_iters, rel, abs_)
         if norm:
             sc.set_norm(norm)
-    info = api.solve("cg", x, A, bt, sc, ctrl)
+    info = api.solve(kind, x, A, bt, sc, ctrl)
     status = sc.device_status()
     if own:
         sc.release()
@@ -277,3 +278,119 @@ def test_banded_cg_symmetric_form_is_bitwise_equal(ctrl, monkeypatch, prob, dtyp
                         rel, 0.0)
     assert out["0"][1] == out["1"][1]
     np.testing.assert_array_equal(out["0"][0], out["1"][0])
+
+
+# ---- BiCGStab (clsparse{S,D}csrbicgStab in loop mode 3)
+
+BICG_PROBLEMS = dict(PROBLEMS, convdiff5=lambda: convdiff5(48))
+
+
+def bicg_slack(n_ref):
+    # BiCGStab's convergence history is irregular and reacts to the order of
+    # the reduction sums (the bar of the other loop modes)
+    return max(8, int(0.12 * n_ref))
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+@pytest.mark.parametrize("precond", [L.DIAGONAL, L.NOPRECOND], ids=["jacobi", "none"])
+@pytest.mark.parametrize("prob", sorted(BICG_PROBLEMS))
+def test_banded_bicgstab_matches_oracle(ctrl, orc, prob, precond, dtype):
+    rp, col, val = BICG_PROBLEMS[prob]()
+    n = len(rp) - 1
+    b = np.random.default_rng(1).uniform(-1, 1, n)
+    rel = 1e-10 if dtype == torch.float64 else 1e-5
+    t = NP[dtype]
+    x, info, status = run(ctrl, rp, col, val, np.zeros(n), b, dtype, precond, 5000, rel, 0.0, kind="bicgstab")
+    _, oi = orc.solve("bicgstab", t, rp, col, val, np.zeros(n, t), np.asarray(b, t), precond, 5000, rel, 0.0)
+    assert abs(info["nIters"] - oi.nIters) <= bicg_slack(oi.nIters), (info, oi.nIters)
+    assert info["initialResidual"] == pytest.approx(oi.initialResidual, rel=1e-5)
+    assert info["currentResidual"] <= rel
+    assert status & ~8 == 0  # a breakdown flag is information, as in the other modes
+    r_true = l1_residual(rp, col, np.asarray(val, t).astype(np.float64), x, np.asarray(b, t).astype(np.float64))
+    assert r_true <= (10 * rel if dtype == torch.float64 else 50 * rel)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+def test_banded_bicgstab_agrees_with_graph_engine(ctrl, dtype):
+    rp, col, val = convdiff5(64)
+    n = len(rp) - 1
+    b = np.random.default_rng(5).uniform(-1, 1, n)
+    rel = 1e-10 if dtype == torch.float64 else 1e-5
+    xg, ig, _ = run(ctrl, rp, col, val, np.zeros(n), b, dtype, L.DIAGONAL, 5000, rel, 0.0, loop_mode=0,
+                    kind="bicgstab")
+    xb, ib, _ = run(ctrl, rp, col, val, np.zeros(n), b, dtype, L.DIAGONAL, 5000, rel, 0.0, loop_mode=3,
+                    kind="bicgstab")
+    assert abs(ig["nIters"] - ib["nIters"]) <= bicg_slack(ig["nIters"])
+    assert ib["initialResidual"] == pytest.approx(ig["initialResidual"], rel=1e-6)
+    A = sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64)), shape=(n, n))
+    tol = 1e-9 if dtype == torch.float64 else 1e-4
+    assert np.abs(b - A @ xb).sum() / np.abs(b).sum() <= tol
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+def test_banded_bicgstab_max_iters_bookkeeping(ctrl, orc, dtype):
+    rp, col, val = convdiff5(40)
+    n = len(rp) - 1
+    b = np.ones(n)
+    t = NP[dtype]
+    x, info, _ = run(ctrl, rp, col, val, np.zeros(n), b, dtype, L.DIAGONAL, 7, 1e-30, 0.0, kind="bicgstab")
+    xo, oi = orc.solve("bicgstab", t, rp, col, val, np.zeros(n, t), np.asarray(b, t), 1, 7, 1e-30, 0.0)
+    assert info["nIters"] == oi.nIters
+    tol = 1e-9 if dtype == torch.float64 else 2e-3
+    assert info["currentResidual"] == pytest.approx(oi.currentResidual, rel=tol)
+    np.testing.assert_allclose(x, xo.astype(np.float64), rtol=tol, atol=tol * np.abs(xo).max())
+
+
+def test_banded_bicgstab_previous_n_iters_enters_first_stop_tests(ctrl, orc):
+    rp, col, val = convdiff5(30)
+    n = len(rp) - 1
+    b = np.random.default_rng(2).uniform(-1, 1, n)
+    sc = api.SolverControl(L.DIAGONAL, 9, 1e-30, 0.0)
+    _, i1, _ = run(ctrl, rp, col, val, np.zeros(n), b, torch.float64, L.DIAGONAL, 0, 0, 0, sc=sc, kind="bicgstab")
+    x0 = np.random.default_rng(3).uniform(-1, 1, n)
+    x2, i2, _ = run(ctrl, rp, col, val, x0, b, torch.float64, L.DIAGONAL, 0, 0, 0, sc=sc, kind="bicgstab")
+    sc.release()
+    _, o1 = orc.solve("bicgstab", np.float64, rp, col, val, np.zeros(n), b, 1, 9, 1e-30, 0.0)
+    _, o2 = orc.solve("bicgstab", np.float64, rp, col, val, x0, b, 1, 9, 1e-30, 0.0, n_iters_in=o1.nIters)
+    assert (i1["nIters"], i2["nIters"]) == (o1.nIters, o2.nIters)
+    np.testing.assert_array_equal(x2, x0)
+
+
+def test_banded_bicgstab_exact_initial_guess(ctrl):
+    rp, col, val = convdiff5(16)
+    n = len(rp) - 1
+    xs = np.random.default_rng(2).uniform(-1, 1, n)
+    bx = sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64))) @ xs
+    x, info, _ = run(ctrl, rp, col, val, xs, bx, torch.float64, L.DIAGONAL, 100, 1e-8, 0.0, kind="bicgstab")
+    assert info["nIters"] == 0
+    np.testing.assert_array_equal(x, xs)
+
+
+def test_banded_bicgstab_zero_rhs_returns_b(ctrl):
+    rp, col, val = convdiff5(16)
+    n = len(rp) - 1
+    x, info, _ = run(ctrl, rp, col, val, np.full(n, 3.0), np.zeros(n), torch.float64, L.DIAGONAL, 100, 1e-6, 1e-8,
+                     kind="bicgstab")
+    assert info["nIters"] == 0
+    assert np.abs(x).sum() == 0.0
+
+
+def test_banded_bicgstab_barrier_timeout_is_reported_and_recovers(ctrl, orc, monkeypatch):
+    rp, col, val = convdiff5(48)
+    n = len(rp) - 1
+    b = np.random.default_rng(6).uniform(-1, 1, n)
+    monkeypatch.setenv("CLSPARSE_B200_TEST_BARRIER_NEVER_RELEASE", "1")
+    monkeypatch.setenv("CLSPARSE_B200_BARRIER_WAIT_NS", "2000000")
+    sc = api.SolverControl(L.DIAGONAL, 2000, 1e-10, 0.0)
+    with pytest.raises(api.ClsparseError) as e:
+        run(ctrl, rp, col, val, np.zeros(n), b, torch.float64, L.DIAGONAL, 0, 0, 0, sc=sc, kind="bicgstab")
+    ctrl.set_solver_loop_mode(0)
+    assert e.value.status == L.clsparseInvalidKernelExecution
+    assert sc.device_status() & 32
+    sc.release()
+    torch.cuda.synchronize()
+    monkeypatch.delenv("CLSPARSE_B200_TEST_BARRIER_NEVER_RELEASE")
+    monkeypatch.delenv("CLSPARSE_B200_BARRIER_WAIT_NS")
+    x, info, _ = run(ctrl, rp, col, val, np.zeros(n), b, torch.float64, L.DIAGONAL, 2000, 1e-10, 0.0,
+                     kind="bicgstab")
+    assert l1_residual(rp, col, val, x, b) <= 1e-9
