@@ -5,7 +5,9 @@ oracle.
   reference's L1 stop test at 1e-10 (clsparseDcsrcg), against the serial
   oracle restatement of the reference CG (conjugate-gradients.hpp:47-228):
   the same stop decision within 1% of the iterations, the same initial
-  residual, and the same solution.
+  residual, and the same solution -- on the default engine and on the banded
+  drop-in engine (solver loop mode 3), which also runs the FP64 Jacobi-CG of
+  C3 and C5.
 * C3 -- 3D 7-point log-normal diffusion 128^3 (2,097,152 rows, sigma 1.5)
   and C5 -- 2D Gaussian-random-field diffusion 1024^2 (1,048,576 rows,
   correlation length 0.05, sigma 2): FP64 Jacobi-CG, the mixed-precision
@@ -59,6 +61,13 @@ def fp64_oracle_solution(name):
     return x
 
 
+@functools.lru_cache(maxsize=None)
+def oracle_iterations_1e10(name):
+    import oracle
+    rp, col, val = config(name)
+    return oracle.reference_solution(rp, col, val, rhs(len(rp) - 1), rel_tol=1e-10)[1]
+
+
 def scipy_matrix(name):
     rp, col, val = config(name)
     n = len(rp) - 1
@@ -83,15 +92,26 @@ def device_problem(ctrl, name):
     return A, b, x
 
 
-def test_c1_poisson512_cg_matches_oracle(ctrl, orc):
+@functools.lru_cache(maxsize=None)
+def c1_oracle_cg():
+    import oracle
+    rp, col, val = config("C1")
+    n = len(rp) - 1
+    return oracle.solve("cg", np.float64, rp, col, val, np.zeros(n), rhs(n), L.DIAGONAL, 200000, 1e-10, 0.0)
+
+
+@pytest.mark.parametrize("loop_mode", [0, 3], ids=["graph", "banded"])
+def test_c1_poisson512_cg_matches_oracle(ctrl, orc, loop_mode):
     rp, col, val = config("C1")
     n = len(rp) - 1
     b = rhs(n)
     A, bt, x = device_problem(ctrl, "C1")
+    ctrl.set_solver_loop_mode(loop_mode)
     sc = api.SolverControl(L.DIAGONAL, 200000, 1e-10, 0.0)
     info = api.solve("cg", x, A, bt, sc, ctrl)
     sc.release()
-    xo, oi = orc.solve("cg", np.float64, rp, col, val, np.zeros(n), b, L.DIAGONAL, 200000, 1e-10, 0.0)
+    ctrl.set_solver_loop_mode(0)
+    xo, oi = c1_oracle_cg()
     assert oi.nIters > 1000
     assert abs(info["nIters"] - oi.nIters) <= max(3, int(0.01 * oi.nIters)), (info, oi.nIters)
     assert info["initialResidual"] == pytest.approx(oi.initialResidual, rel=1e-9)
@@ -102,23 +122,26 @@ def test_c1_poisson512_cg_matches_oracle(ctrl, orc):
     assert np.linalg.norm(xs - xo) / np.linalg.norm(xo) <= ERR_BAR
 
 
-def _fp64_cg(ctrl, name):
+def _fp64_cg(ctrl, name, loop_mode=0):
     A, b, x = device_problem(ctrl, name)
+    ctrl.set_solver_loop_mode(loop_mode)
     sc = api.SolverControl(L.DIAGONAL, 200000, 1e-10, 0.0)
     sc.set_norm(2)
     info = api.solve("cg", x, A, b, sc, ctrl)
     sc.release()
+    ctrl.set_solver_loop_mode(0)
     return x.cpu().numpy(), info
 
 
+@pytest.mark.parametrize("loop_mode", [0, 3], ids=["graph", "banded"])
 @pytest.mark.parametrize("name", ["C3", "C5"])
-def test_fp64_jacobi_cg_at_config_matches_oracle(ctrl, orc, name):
+def test_fp64_jacobi_cg_at_config_matches_oracle(ctrl, orc, name, loop_mode):
     import oracle
     rp, col, val = config(name)
-    xs, info = _fp64_cg(ctrl, name)
+    xs, info = _fp64_cg(ctrl, name, loop_mode)
     # the oracle's threaded CG to the same L2 tolerance: same iteration count
     # up to reduction order
-    _, it_o, _ = oracle.reference_solution(rp, col, val, rhs(len(rp) - 1), rel_tol=1e-10)
+    it_o = oracle_iterations_1e10(name)
     assert abs(info["nIters"] + 1 - it_o) <= max(3, int(0.02 * it_o)), (info, it_o)
     assert l2_residual(name, xs) <= 1.5e-10
     assert error_vs_oracle(name, xs) <= ERR_BAR
