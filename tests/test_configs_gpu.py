@@ -136,8 +136,6 @@ def _fp64_cg(ctrl, name, loop_mode=0):
 @pytest.mark.parametrize("loop_mode", [0, 3], ids=["graph", "banded"])
 @pytest.mark.parametrize("name", ["C3", "C5"])
 def test_fp64_jacobi_cg_at_config_matches_oracle(ctrl, orc, name, loop_mode):
-    import oracle
-    rp, col, val = config(name)
     xs, info = _fp64_cg(ctrl, name, loop_mode)
     # the oracle's threaded CG to the same L2 tolerance: same iteration count
     # up to reduction order
