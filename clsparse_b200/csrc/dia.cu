@@ -605,10 +605,10 @@ struct DiaCgArgs {
     const T* vals;
     LaneRange lanes[kMaxLaneRanges];
     int nlanes;
-    // A symmetric bit for bit with its offsets symmetric (the kernel's SYM
-    // form): the value of lower diagonal d at row i is read as A[j][i] from
-    // its upper partner nd_real - 1 - d at row j = i + off[d], and the lower
-    // diagonals are not read at all
+    // A symmetric bit for bit with its offsets symmetric and no padding
+    // diagonals (the kernel's SYM form): the value of lower diagonal d at row
+    // i is read as A[j][i] from its upper partner ND - 1 - d at row
+    // j = i + off[d], and the lower diagonals are not read at all
     int nd_real;
     int d0;         // index of the main diagonal (Jacobi)
     T* invD;        // Jacobi: 1 / a_ii, formed in the prologue; nullptr: no preconditioner
@@ -648,7 +648,7 @@ __device__ __forceinline__ typename Args::value_type dia_row_seq(const Args& a, 
         const uint32_t jc = in ? static_cast<uint32_t>(j) : i;
         T v;
         if (SYM && a.A.off[d] < 0)
-            v = __ldg(a.A.vals + static_cast<size_t>(a.nd_real - 1 - d) * n + jc);
+            v = __ldg(a.A.vals + static_cast<size_t>(ND - 1 - d) * n + jc);
         else
             v = __ldg(a.A.vals + static_cast<size_t>(d) * n + i);
         const T xj = xf(jc);
@@ -1334,13 +1334,19 @@ __global__ void dia_sym_check_kernel(const T* __restrict__ vals, uint32_t n, int
 // 1024^2 five-point FP64 matrix (96 MB) 30.0 -> 26.5 us; where the working
 // set stays in L2 the extra index arithmetic costs more than the bytes it
 // saves (512^2 FP64: 11.6 -> 12.0 us, 1024^2 FP32: 19.3 -> 21.9 us).
+// Diagonal classes the SYM form runs for. On the 128^3 seven-point matrix it
+// measured slower (FP64 74.8 vs 70.8 us per iteration, FP32 48.9 vs 42.8):
+// the mirrored reads at -16384 rows fall in another CTA's slice, L2 instead
+// of L1.
+constexpr int kSymMaxDiags = 5;
+
 template <typename T>
 clsparseStatus dia_symmetric(const DiaMat<T>& M, const DiaOffsets& offs, uint32_t n, int nd_pad, size_t l2_bytes,
                              DiaWork& w, cudaStream_t s, bool& sym) {
     sym = false;
     const char* env = std::getenv("CLSPARSE_B200_DIA_SYM");
     const int mode = env ? std::atoi(env) : -1;
-    if (mode == 0 || nd_pad > 5) return clsparseSuccess;
+    if (mode == 0 || nd_pad > kSymMaxDiags || offs.nd != nd_pad) return clsparseSuccess;
     const size_t working = static_cast<size_t>(nd_pad + 7) * n * sizeof(T);
     if (mode != 1 && (l2_bytes == 0 || 2 * working <= l2_bytes)) return clsparseSuccess;
     const int nd = offs.nd;
