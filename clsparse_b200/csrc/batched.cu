@@ -11,13 +11,22 @@
 // round trip. When the recursive FP32 residual meets the tolerance, the CTA
 // recomputes the true residual b - A x in FP64; if that check fails, CG
 // restarts from the current x with the FP64 residual (refinement) until the
-// check passes or the iteration budget is spent. Each system's SpMV uses the
-// lanes-per-row width the tuning table gives for its size class.
+// check passes or the iteration budget is spent. When every system is banded
+// (at most kBatchDiags column offsets, all inside its own rows), the products
+// come from a per-system diagonal-storage copy laid out at every call: one
+// thread per row, the values and the vector entries independent loads
+// instead of the row-pointer / column-index / vector chain of CSR (C4, 4096
+// stencil systems: 0.349 -> 0.312 s). Otherwise each system's SpMV uses the
+// lanes-per-row width the tuning table gives for its size class. The kernel
+// is held to two CTAs per SM (64 registers): the diagonal loop would
+// otherwise take 128 registers and halve the resident CTAs (0.51 s).
 //
 // The whole solve (queue reset, kernel) is captured once into a CUDA graph per
 // control and relaunched for repeated solves on the same operands.
 #include <algorithm>
+#include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <vector>
@@ -30,6 +39,9 @@ namespace {
 
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
+
+// Diagonals a system may have to be solved from diagonal storage.
+constexpr int kBatchDiags = 8;
 
 struct BatchArgs {
     const float* vals;
@@ -51,6 +63,13 @@ struct BatchArgs {
     uint32_t nsys;
     int max_iters;
     double tol;
+    // Diagonal storage (nullptr: every system's products come from CSR):
+    // system s's diagonal d at row r0 + i is dvals[dbase[s] + d * n_s + i],
+    // its column offsets doffs[s * kBatchDiags + d] increasing, dnd[s] of them.
+    const float* dvals;
+    const uint64_t* dbase;
+    const int32_t* doffs;
+    const uint8_t* dnd;
 };
 
 __device__ __forceinline__ double cta_sum(double v, double* red) {
@@ -88,6 +107,29 @@ __device__ __forceinline__ void spmv_dispatch(const BatchArgs& a, int g, uint32_
     }
 }
 
+// q = A v over the rows of one system from its diagonal storage: one thread
+// per row, products in increasing column order, columns outside the system
+// (the block diagonal) contribute nothing. The values and the v entries of
+// a row are independent loads (no row-pointer / column-index chain).
+__device__ __forceinline__ void sys_spmv_dia(const float* __restrict__ dv, uint32_t ns, uint32_t r0, uint32_t r1,
+                                             const int32_t* soff, int nd, const float* v, float* out) {
+    for (uint32_t row = r0 + threadIdx.x; row < r1; row += kThreads) {
+        const uint32_t i = row - r0;
+        float s = 0.f;
+#pragma unroll
+        for (int d = 0; d < kBatchDiags; ++d) {
+            if (d < nd) {
+                const int64_t j = static_cast<int64_t>(row) + soff[d];
+                const bool in = j >= r0 && j < r1;
+                const float av = __ldg(dv + static_cast<size_t>(d) * ns + i);
+                const float xv = v[in ? static_cast<uint32_t>(j) : row];
+                s = fmaf(av, in ? xv : 0.f, s);
+            }
+        }
+        out[row] = s;
+    }
+}
+
 // r = b - A x in FP64 (the check), written back to r in FP32; returns
 // sum r^2 and sum b^2 in every thread.
 __device__ __forceinline__ void true_residual(const BatchArgs& a, uint32_t r0, uint32_t r1, double* red,
@@ -107,9 +149,10 @@ __device__ __forceinline__ void true_residual(const BatchArgs& a, uint32_t r0, u
     bb = cta_sum(acc_b, red);
 }
 
-__global__ void __launch_bounds__(kThreads) batched_cg_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) batched_cg_kernel(BatchArgs a) {
     __shared__ double red[32];
     __shared__ uint32_t slot;
+    __shared__ int32_t soff[kBatchDiags];
     for (;;) {
         if (threadIdx.x == 0) slot = atomicAdd(a.counter, 1u);
         __syncthreads();
@@ -119,6 +162,9 @@ __global__ void __launch_bounds__(kThreads) batched_cg_kernel(BatchArgs a) {
         const uint32_t s = a.order[k];
         const uint32_t r0 = a.off[s], r1 = a.off[s + 1];
         const int g = a.lanes[s];
+        const float* dv = a.dvals ? a.dvals + a.dbase[s] : nullptr;
+        const int nd = a.dvals ? a.dnd[s] : 0;
+        if (a.dvals && threadIdx.x < kBatchDiags) soff[threadIdx.x] = a.doffs[s * kBatchDiags + threadIdx.x];
 
         // Jacobi: inverse diagonal (first diagonal entry of each row; 1 if absent)
         for (uint32_t row = r0 + threadIdx.x; row < r1; row += kThreads) {
@@ -150,7 +196,10 @@ __global__ void __launch_bounds__(kThreads) batched_cg_kernel(BatchArgs a) {
             __syncthreads();
             bool inner_done = false;
             while (!inner_done && it < a.max_iters) {
-                spmv_dispatch(a, g, r0, r1, a.p, a.q);
+                if (dv)
+                    sys_spmv_dia(dv, r1 - r0, r0, r1, soff, nd, a.p, a.q);
+                else
+                    spmv_dispatch(a, g, r0, r1, a.p, a.q);
                 __syncthreads();
                 acc = 0.0;
                 for (uint32_t row = r0 + threadIdx.x; row < r1; row += kThreads)
@@ -195,6 +244,83 @@ __global__ void __launch_bounds__(kThreads) batched_cg_kernel(BatchArgs a) {
             a.converged[s] = ok ? 1 : 0;
         }
         __syncthreads();
+    }
+}
+
+// One CTA per system: the distinct column offsets col - row of its rows,
+// increasing, into doffs[s * kBatchDiags ...] and their count into dnd[s]
+// (0 when the system does not qualify); bad[0] = 1 when a system has more
+// than kBatchDiags of them, a column outside its own rows, or columns not
+// strictly increasing in a row.
+__global__ void batch_dia_detect_kernel(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols,
+                                        const uint32_t* __restrict__ off, int32_t* doffs, uint8_t* dnd, int* bad) {
+    constexpr int32_t kEmptySlot = INT32_MIN;  // below any offset of a system of fewer than 2^31 rows
+    __shared__ int32_t set[kBatchDiags];
+    __shared__ int over;
+    const uint32_t s = blockIdx.x;
+    const uint32_t r0 = off[s], r1 = off[s + 1];
+    if (threadIdx.x < kBatchDiags) set[threadIdx.x] = kEmptySlot;
+    if (threadIdx.x == 0) over = 0;
+    __syncthreads();
+    int mine = 0;
+    for (uint32_t row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
+        for (uint32_t k = rp[row]; k < rp[row + 1]; ++k) {
+            const uint32_t c = cols[k];
+            if (c < r0 || c >= r1 || (k > rp[row] && c <= cols[k - 1])) {
+                mine = 1;
+                continue;
+            }
+            const int32_t o = static_cast<int32_t>(static_cast<int64_t>(c) - static_cast<int64_t>(row));
+            bool placed = false;
+            for (int t = 0; t < kBatchDiags && !placed; ++t) {
+                const int32_t cur = *reinterpret_cast<volatile int32_t*>(&set[t]);
+                if (cur == o) {
+                    placed = true;
+                } else if (cur == kEmptySlot) {
+                    const int32_t old = atomicCAS(&set[t], kEmptySlot, o);
+                    placed = old == kEmptySlot || old == o;
+                }
+            }
+            if (!placed) mine = 1;
+        }
+    }
+    if (mine) atomicExch(&over, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int32_t v[kBatchDiags];
+        int nd = 0;
+        for (int t = 0; t < kBatchDiags; ++t)
+            if (set[t] != kEmptySlot) v[nd++] = set[t];
+        if (over) nd = 0;
+        for (int t = 1; t < nd; ++t)  // insertion sort of at most kBatchDiags values
+            for (int u = t; u > 0 && v[u - 1] > v[u]; --u) {
+                const int32_t w = v[u];
+                v[u] = v[u - 1];
+                v[u - 1] = w;
+            }
+        for (int t = 0; t < kBatchDiags; ++t) doffs[s * kBatchDiags + t] = t < nd ? v[t] : 0;
+        dnd[s] = static_cast<uint8_t>(nd);
+        if (over) atomicExch(bad, 1);
+    }
+}
+
+// One CTA per system: its CSR values into diagonal storage (dv zeroed before).
+__global__ void batch_dia_fill_kernel(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cols,
+                                      const float* __restrict__ vals, const uint32_t* __restrict__ off,
+                                      const int32_t* __restrict__ doffs, const uint8_t* __restrict__ dnd,
+                                      const uint64_t* __restrict__ dbase, float* dv) {
+    const uint32_t s = blockIdx.x;
+    const uint32_t r0 = off[s], r1 = off[s + 1], ns = r1 - r0;
+    const int nd = dnd[s];
+    const int32_t* o = doffs + s * kBatchDiags;
+    float* out = dv + dbase[s];
+    for (uint32_t row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
+        int d = 0;
+        for (uint32_t k = rp[row]; k < rp[row + 1]; ++k) {
+            const int32_t c = static_cast<int32_t>(static_cast<int64_t>(cols[k]) - static_cast<int64_t>(row));
+            while (d < nd && o[d] < c) ++d;  // columns increase, so d only moves forward
+            if (d < nd && o[d] == c) out[static_cast<size_t>(d) * ns + (row - r0)] = vals[k];
+        }
     }
 }
 
@@ -277,6 +403,59 @@ clsparseStatus clsparseScsrcgBatched(cldenseVector* x, const clsparseCsrMatrix* 
     cudaMemcpyAsync(d_order, order.data(), nsys * 4, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d_lanes, lanes.data(), nsys, cudaMemcpyHostToDevice, s);
 
+    // Diagonal storage when every system is banded (at most kBatchDiags
+    // column offsets inside its own rows): offsets found on the device, the
+    // values laid out by diagonal at every call (so values changed in place
+    // are seen). CLSPARSE_B200_BATCH_DIA=0 keeps every system on CSR.
+    const float* dvals = nullptr;
+    const uint64_t* d_dbase = nullptr;
+    const int32_t* d_doffs = nullptr;
+    const uint8_t* d_dnd = nullptr;
+    const char* dia_env = std::getenv("CLSPARSE_B200_BATCH_DIA");
+    if (!(dia_env && std::atoi(dia_env) == 0)) {
+        const size_t offs_b = ((static_cast<size_t>(nsys) * kBatchDiags * 4 + 255) / 256) * 256;
+        const size_t base_b = ((static_cast<size_t>(nsys) * 8 + 255) / 256) * 256;
+        const size_t nd_b = ((static_cast<size_t>(nsys) + 255) / 256) * 256;
+        if (w.dia_meta.ensure(offs_b + base_b + nd_b + 256) != cudaSuccess) {
+            cudaGetLastError();
+            return clsparseOutOfResources;
+        }
+        char* dm = static_cast<char*>(w.dia_meta.ptr);
+        int32_t* doffs = reinterpret_cast<int32_t*>(dm);
+        uint64_t* dbase = reinterpret_cast<uint64_t*>(dm + offs_b);
+        uint8_t* dnd = reinterpret_cast<uint8_t*>(dm + offs_b + base_b);
+        int* bad = reinterpret_cast<int*>(dm + offs_b + base_b + nd_b);
+        const uint32_t* cols = dev_ptr<const uint32_t>(A->col_indices, A->off_col_indices);
+        cudaMemsetAsync(bad, 0, sizeof(int), s);
+        batch_dia_detect_kernel<<<nsys, 256, 0, s>>>(rp, cols, d_off, doffs, dnd, bad);
+        std::vector<uint8_t> hnd(nsys);
+        int hbad = 1;
+        cudaMemcpyAsync(hnd.data(), dnd, nsys, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) return clsparseInvalidKernelExecution;
+        if (hbad == 0) {
+            std::vector<uint64_t> hbase(nsys);
+            uint64_t total = 0;
+            for (uint32_t k = 0; k < nsys; ++k) {
+                hbase[k] = total;
+                total += static_cast<uint64_t>(hnd[k]) * (off[k + 1] - off[k]);
+            }
+            if (w.dia.ensure(total * sizeof(float) + 256) != cudaSuccess) {
+                cudaGetLastError();
+                return clsparseOutOfResources;
+            }
+            cudaMemcpyAsync(dbase, hbase.data(), nsys * 8, cudaMemcpyHostToDevice, s);
+            cudaMemsetAsync(w.dia.ptr, 0, total * sizeof(float), s);
+            batch_dia_fill_kernel<<<nsys, 256, 0, s>>>(rp, cols, dev_ptr<const float>(A->values, A->off_values), d_off,
+                                                      doffs, dnd, dbase, static_cast<float*>(w.dia.ptr));
+            if (cudaGetLastError() != cudaSuccess) return clsparseInvalidKernelExecution;
+            dvals = static_cast<const float*>(w.dia.ptr);
+            d_dbase = dbase;
+            d_doffs = doffs;
+            d_dnd = dnd;
+        }
+    }
+
     char* ob = static_cast<char*>(w.out.ptr);
     static_assert(sizeof(BatchArgs) <= sizeof(w.args), "argument record");
     BatchArgs a;
@@ -301,6 +480,10 @@ clsparseStatus clsparseScsrcgBatched(cldenseVector* x, const clsparseCsrMatrix* 
     a.nsys = nsys;
     a.max_iters = solverControl->maxIters;
     a.tol = solverControl->relativeTolerance;
+    a.dvals = dvals;
+    a.dbase = d_dbase;
+    a.doffs = d_doffs;
+    a.dnd = d_dnd;
 
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_cg_kernel, kThreads, 0);

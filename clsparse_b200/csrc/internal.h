@@ -62,6 +62,7 @@ struct MixedWork {
 // Work area and cached graph of the batched solver (batched.cu).
 struct BatchWork {
     DeviceBuffer vecs, meta, out;
+    DeviceBuffer dia, dia_meta;  // diagonal-storage copies of banded systems and their offsets
     cudaGraphExec_t exec = nullptr;
     unsigned char args[256] = {};  // kernel arguments the graph was captured with
     uint32_t grid = 0;

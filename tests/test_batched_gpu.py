@@ -1,6 +1,7 @@
 """Batched FP32 Jacobi-CG (clsparseScsrcgBatched) through the C ABI: every
 system's solution against an FP64 direct solve of that system, and the FP64
-residual each system reports against one recomputed here."""
+residual each system reports against one recomputed here -- from diagonal
+storage (banded systems, the default) and from CSR."""
 from __future__ import annotations
 
 import numpy as np
@@ -15,8 +16,13 @@ from clsparse_b200 import api, matgen
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("storage", ["diagonal", "csr"])
 @pytest.mark.parametrize("lanes", [None, 1, 4])
-def test_batched_cg_matches_direct_solves(ctrl, lanes):
+def test_batched_cg_matches_direct_solves(ctrl, lanes, storage, monkeypatch):
+    """Banded systems run from diagonal storage by default;
+    CLSPARSE_B200_BATCH_DIA=0 keeps them on CSR (the lanes-per-row path)."""
+    if storage == "csr":
+        monkeypatch.setenv("CLSPARSE_B200_BATCH_DIA", "0")
     rp, col, val, off, dims = matgen.batched_systems(48, 40, 4000, sigma=1.0, seed=3)
     n = len(rp) - 1
     A64 = sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64)), shape=(n, n))
@@ -68,3 +74,30 @@ def test_batched_rejects_bad_offsets(ctrl):
     with pytest.raises(api.ClsparseError):
         api.cg_batched(x, A, x, bad, sc, ctrl)
     sc.release()
+
+
+def test_batch_with_a_non_banded_system_runs_on_csr(ctrl):
+    """One system with more column offsets than diagonal storage takes: the
+    batch runs from CSR, and every system still meets the tolerance."""
+    rp, col, val, off, _ = matgen.batched_systems(12, 200, 3000, sigma=1.0, seed=4)
+    S = sp.csr_matrix((val, col.astype(np.int64), rp.astype(np.int64)), shape=(len(rp) - 1,) * 2)
+    rrp, rcol, rval = matgen.random_spd(1500, seed=8)
+    R = sp.csr_matrix((rval, rcol.astype(np.int64), rrp.astype(np.int64)), shape=(1500, 1500))
+    M = sp.block_diag([S, R], format="csr")
+    M.sort_indices()
+    offs = np.concatenate([off, [off[-1] + 1500]]).astype(np.uint32)
+    n = M.shape[0]
+    b = np.random.default_rng(6).uniform(-1, 1, n).astype(np.float32)
+    A = api.CsrMatrix.from_numpy(M.indptr.astype(np.uint32), M.indices.astype(np.uint32), M.data,
+                                 dtype=torch.float32)
+    x = torch.zeros(n, dtype=torch.float32, device="cuda")
+    sc = api.SolverControl(L.DIAGONAL, 20000, 1e-6, 0.0)
+    out = api.cg_batched(x, A, torch.tensor(b, device="cuda"), offs, sc, ctrl)
+    sc.release()
+    assert out["converged"] == 13, out
+    M32 = sp.csr_matrix((M.data.astype(np.float32).astype(np.float64), M.indices, M.indptr), shape=M.shape)
+    xs = x.cpu().numpy().astype(np.float64)
+    for s in range(13):
+        a, e = int(offs[s]), int(offs[s + 1])
+        bs = b[a:e].astype(np.float64)
+        assert np.linalg.norm(bs - M32[a:e, a:e] @ xs[a:e]) / np.linalg.norm(bs) <= 1.05e-6
