@@ -111,8 +111,9 @@ __device__ __forceinline__ void spmv_dispatch(const BatchArgs& a, int g, uint32_
 // per row, products in increasing column order, columns outside the system
 // (the block diagonal) contribute nothing. The values and the v entries of
 // a row are independent loads (no row-pointer / column-index chain).
-__device__ __forceinline__ void sys_spmv_dia(const float* __restrict__ dv, uint32_t ns, uint32_t r0, uint32_t r1,
-                                             const int32_t* soff, int nd, const float* v, float* out) {
+__device__ __forceinline__ double sys_spmv_dia(const float* __restrict__ dv, uint32_t ns, uint32_t r0, uint32_t r1,
+                                               const int32_t* soff, int nd, const float* v, float* out) {
+    double dot = 0.0;
     for (uint32_t row = r0 + threadIdx.x; row < r1; row += kThreads) {
         const uint32_t i = row - r0;
         float s = 0.f;
@@ -127,7 +128,9 @@ __device__ __forceinline__ void sys_spmv_dia(const float* __restrict__ dv, uint3
             }
         }
         out[row] = s;
+        dot += static_cast<double>(v[row]) * s;
     }
+    return dot;  // this thread's part of <v, A v>
 }
 
 // r = b - A x in FP64 (the check), written back to r in FP32; returns
@@ -196,15 +199,17 @@ __global__ void __launch_bounds__(kThreads, 2) batched_cg_kernel(BatchArgs a) {
             __syncthreads();
             bool inner_done = false;
             while (!inner_done && it < a.max_iters) {
-                if (dv)
-                    sys_spmv_dia(dv, r1 - r0, r0, r1, soff, nd, a.p, a.q);
-                else
+                if (dv) {
+                    // the row's thread also forms its part of <p, q>
+                    acc = sys_spmv_dia(dv, r1 - r0, r0, r1, soff, nd, a.p, a.q);
+                } else {
                     spmv_dispatch(a, g, r0, r1, a.p, a.q);
-                __syncthreads();
-                acc = 0.0;
-                for (uint32_t row = r0 + threadIdx.x; row < r1; row += kThreads)
-                    acc += static_cast<double>(a.p[row]) * a.q[row];
-                const double pq = cta_sum(acc, red);
+                    __syncthreads();
+                    acc = 0.0;
+                    for (uint32_t row = r0 + threadIdx.x; row < r1; row += kThreads)
+                        acc += static_cast<double>(a.p[row]) * a.q[row];
+                }
+                const double pq = cta_sum(acc, red);  // its barriers also order q's stores
                 const float alpha = static_cast<float>(rz / pq);
                 double acc_rz = 0.0, acc_rr = 0.0;
                 for (uint32_t row = r0 + threadIdx.x; row < r1; row += kThreads) {
