@@ -228,6 +228,30 @@ def dia_cg_profile(iters: int):
     ctrl.release()
 
 
+def batched_profile(nsys: int):
+    """Two batched FP32 Jacobi-CG solves (clsparseScsrcgBatched) over the
+    first `nsys` systems of the C4 family (same generator and seed), for a
+    profiler: per call the offset detection, the diagonal layout and one
+    persistent solver launch."""
+    import torch
+    from clsparse_b200 import _lib as L
+    from clsparse_b200 import api, matgen
+    api.setup()
+    ctrl = api.Control()
+    rp, col, val, off, _ = matgen.batched_systems(nsys, 500, 50_000, sigma=1.0, seed=11)
+    A = api.CsrMatrix.from_numpy(rp, col, val, dtype=torch.float32)
+    n = A.num_rows
+    b = torch.tensor(np.random.default_rng(1).uniform(-1, 1, n), dtype=torch.float32, device="cuda")
+    for _ in range(2):
+        x = torch.zeros(n, dtype=torch.float32, device="cuda")
+        sc = api.SolverControl(L.DIAGONAL, 20000, 1e-5, 0.0)
+        r = api.cg_batched(x, A, b, off, sc, ctrl)
+        sc.release()
+    torch.cuda.synchronize()
+    print(json.dumps({"batched_profile_systems": nsys, "converged": int(r["converged"])}), flush=True)
+    ctrl.release()
+
+
 def gnn_profile(builds: int):
     """BF16 factor builds of the learned preconditioner on the C5 matrix
     (1,048,576 rows): the network's forward pass with its dense layers on the
@@ -854,6 +878,8 @@ def main():
     ap.add_argument("--cg-profile", type=int, default=0, metavar="ITERS",
                     help="only run ITERS iterations of FP64 Jacobi-CG on the C5 matrix with directly launched "
                          "kernels (for a profiler's launch list), then exit")
+    ap.add_argument("--batched-profile", type=int, default=0, metavar="NSYS",
+                    help="only run two batched solves over the first NSYS systems of the C4 family, then exit")
     ap.add_argument("--dia-cg-profile", type=int, default=0, metavar="ITERS",
                     help="only run two FP64 Jacobi-CG calls of ITERS iterations on the C5 matrix through the "
                          "banded drop-in engine (loop mode 3), then exit")
@@ -861,6 +887,9 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.dia_cg_profile:
         dia_cg_profile(args.dia_cg_profile)
+        return
+    if args.batched_profile:
+        batched_profile(args.batched_profile)
         return
     if args.gnn_profile:
         gnn_profile(args.gnn_profile)
