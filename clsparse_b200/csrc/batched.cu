@@ -17,7 +17,8 @@
 // thread per row, the values and the vector entries independent loads
 // instead of the row-pointer / column-index / vector chain of CSR, and rows
 // whose whole stencil lies inside the system without clamps (C4, 4096 stencil
-// systems: 0.349 -> 0.312 -> 0.229 s). Otherwise each system's SpMV uses the
+// systems: 0.349 -> 0.312 -> 0.229 s; the update pass issuing each row's
+// loads before its stores: 0.198 s). Otherwise each system's SpMV uses the
 // lanes-per-row width the tuning table gives for its size class. The kernel
 // is held to two CTAs per SM (64 registers): the diagonal loop would
 // otherwise take 128 registers and halve the resident CTAs (0.51 s).
@@ -223,10 +224,13 @@ __global__ void __launch_bounds__(kThreads, 2) batched_cg_kernel(BatchArgs a) {
                 const float alpha = static_cast<float>(rz / pq);
                 double acc_rz = 0.0, acc_rr = 0.0;
                 for (uint32_t row = r0 + threadIdx.x; row < r1; row += kThreads) {
-                    a.x[row] = fmaf(alpha, a.p[row], a.x[row]);
+                    // the row's loads before its stores (the vectors are not
+                    // __restrict__: a store would hold back later loads)
+                    const float xi = fmaf(alpha, a.p[row], a.x[row]);
                     const float ri = fmaf(-alpha, a.q[row], a.r[row]);
-                    a.r[row] = ri;
                     const float z = ri * a.invd[row];
+                    a.x[row] = xi;
+                    a.r[row] = ri;
                     acc_rz += static_cast<double>(ri) * z;
                     acc_rr += static_cast<double>(ri) * ri;
                 }
