@@ -18,7 +18,8 @@
 // instead of the row-pointer / column-index / vector chain of CSR, and rows
 // whose whole stencil lies inside the system without clamps (C4, 4096 stencil
 // systems: 0.349 -> 0.312 -> 0.229 s; the update pass issuing each row's
-// loads before its stores: 0.198 s). Otherwise each system's SpMV uses the
+// loads before its stores: 0.198 s; the vector passes two rows at a time:
+// 0.169 s). Otherwise each system's SpMV uses the
 // lanes-per-row width the tuning table gives for its size class. The kernel
 // is held to two CTAs per SM (64 registers): the diagonal loop would
 // otherwise take 128 registers and halve the resident CTAs (0.51 s).
@@ -223,16 +224,29 @@ __global__ void __launch_bounds__(kThreads, 2) batched_cg_kernel(BatchArgs a) {
                 const double pq = cta_sum(acc, red);  // its barriers also order q's stores
                 const float alpha = static_cast<float>(rz / pq);
                 double acc_rz = 0.0, acc_rr = 0.0;
-                for (uint32_t row = r0 + threadIdx.x; row < r1; row += kThreads) {
-                    // the row's loads before its stores (the vectors are not
-                    // __restrict__: a store would hold back later loads)
+                // two rows per pass, all their loads before any store (the
+                // vectors are not __restrict__: a store holds back every later
+                // load, so one row per pass would wait out each row's loads)
+                for (uint32_t row = r0 + threadIdx.x; row < r1; row += 2 * kThreads) {
+                    const uint32_t row1 = row + kThreads;
+                    const bool has1 = row1 < r1;
+                    const uint32_t rb = has1 ? row1 : row;
                     const float xi = fmaf(alpha, a.p[row], a.x[row]);
                     const float ri = fmaf(-alpha, a.q[row], a.r[row]);
                     const float z = ri * a.invd[row];
+                    const float xj = fmaf(alpha, a.p[rb], a.x[rb]);
+                    const float rj = fmaf(-alpha, a.q[rb], a.r[rb]);
+                    const float zj = rj * a.invd[rb];
                     a.x[row] = xi;
                     a.r[row] = ri;
                     acc_rz += static_cast<double>(ri) * z;
                     acc_rr += static_cast<double>(ri) * ri;
+                    if (has1) {
+                        a.x[row1] = xj;
+                        a.r[row1] = rj;
+                        acc_rz += static_cast<double>(rj) * zj;
+                        acc_rr += static_cast<double>(rj) * rj;
+                    }
                 }
                 const double rz_new = cta_sum(acc_rz, red);
                 const double rr_new = cta_sum(acc_rr, red);
@@ -247,8 +261,15 @@ __global__ void __launch_bounds__(kThreads, 2) batched_cg_kernel(BatchArgs a) {
                 }
                 const float beta = static_cast<float>(rz_new / rz);
                 rz = rz_new;
-                for (uint32_t row = r0 + threadIdx.x; row < r1; row += kThreads)
-                    a.p[row] = fmaf(beta, a.p[row], a.r[row] * a.invd[row]);
+                for (uint32_t row = r0 + threadIdx.x; row < r1; row += 2 * kThreads) {
+                    const uint32_t row1 = row + kThreads;
+                    const bool has1 = row1 < r1;
+                    const uint32_t rb = has1 ? row1 : row;
+                    const float pi = fmaf(beta, a.p[row], a.r[row] * a.invd[row]);
+                    const float pj = fmaf(beta, a.p[rb], a.r[rb] * a.invd[rb]);
+                    a.p[row] = pi;
+                    if (has1) a.p[row1] = pj;
+                }
                 __syncthreads();
             }
             __syncthreads();
